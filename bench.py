@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""GTEPS per snapshot of the incremental streaming-graph engine on B200.
+
+Workload (the plain incremental SSSP/BFS/CC configuration): directed R-MAT
+scale 24 (16.7M vertices, edge factor 16, a/b/c/d = 0.57/0.19/0.19/0.05,
+seed 1, self-loops and duplicates removed), uint32 weights uniform in [1,64]
+from the seed, HBM edge budget 4 GB, queries SSSP(0), BFS(0) and CC kept up
+to date over snapshots of 1M updates (500k inserts of new edges + 500k
+deletes of existing edges).  Synthetic data generated on the device.
+
+One step = one snapshot: the batch is applied to the graph and the three
+queries are brought up to date incrementally.  GTEPS = edges traversed by the
+three queries (invalidation + re-push + convergence rounds) / step time.
+
+* value: batches already resident in HBM, time from CUDA events on the
+  engine's stream (summed over the K timed steps);
+* e2e:   the same through the C ABI with the batch in pinned host memory
+  (host->device copy inside the step) and a device->host read of each query's
+  summary (reached count, value sum, max, parent sum) after every step;
+  wall-clock per step.
+
+--impl reference times the reference's own CPU code for this path on the
+host cores (oracle/_ref, compiled from the reference sources) on a bounded
+sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "c-gpustreamgraph_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "GTEPS per snapshot (incremental SSSP+BFS+CC, R-MAT s24, 1M updates/snapshot)"
+UNIT = "GTEPS"
+L2_BYTES = 126 * 2**20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--edge-factor", type=int, default=16)
+    ap.add_argument("--updates", type=int, default=1_000_000)
+    ap.add_argument("--budget-gb", type=float, default=4.0)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- ranks
+class Ranks:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.dist, self.torch, self.pg = dist, torch, True
+
+    def _reduce(self, x, op):
+        if not self.pg:
+            return x
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64,
+                              device="cuda" if self.torch.cuda.is_available() else "cpu")
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max(self, x):
+        return self._reduce(x, self.dist.ReduceOp.MAX) if self.pg else x
+
+    def sum(self, x):
+        return self._reduce(x, self.dist.ReduceOp.SUM) if self.pg else x
+
+    def barrier(self):
+        if self.pg:
+            self.dist.barrier()
+
+    def close(self):
+        if self.pg:
+            self.dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        load = [s for s in sm if s > 0.5 * (max(mx) if mx else 0)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Bytes per slot / per entry of the dominant kernel from the committed ncu
+    summary (profiles/relax_traffic.json), if present."""
+    path = os.path.join(REPO, "profiles", "relax_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+# ----------------------------------------------------------------- engine arm
+def engine_arm(a, R):
+    import torch
+
+    import sgs
+
+    dev = torch.device("cuda", R.local)
+    torch.cuda.set_device(dev)
+    e = sgs.Engine(device=R.local, hbm_budget_gb=a.budget_gb, weight_mode=sgs.W_EXPLICIT)
+    t0 = time.time()
+    e.load_rmat(a.scale, a.edge_factor, a.seed, 0.57, 0.19, 0.19, wseed=a.seed)
+    t_gen = time.time() - t0
+    st0 = e.engine_stats()
+    nv = int(st0["nv"])
+    row, col, _ = e.export()
+    half = a.updates // 2
+    nbatch = a.warmup + a.steps * (1 if a.no_e2e else 2)
+    i_s, i_d, d_s, d_d = sgs.gen_update_stream(nv, row, col, a.seed * 1000003, nbatch * half,
+                                               nbatch * half)
+    i_w = sgs.hash_weights(a.seed, i_s, i_d)
+    del row, col
+    queries = [e.add_query(sgs.SSSP, 0), e.add_query(sgs.BFS, 0), e.add_query(sgs.CC, 0)]
+
+    def batch(k):
+        s = slice(k * half, (k + 1) * half)
+        return i_s[s], i_d[s], i_w[s], d_s[s], d_d[s]
+
+    def to_dev(arrs):
+        return [torch.from_numpy(x.view(np.int32)).to(dev) for x in arrs]
+
+    dev_batches = [to_dev(batch(k)) for k in range(a.warmup + a.steps)]
+
+    def run_dev(b):
+        isrc, idst, iw, dsrc, ddst = b
+        e.apply_batch_ptr(isrc.data_ptr(), idst.data_ptr(), iw.data_ptr(), half,
+                          dsrc.data_ptr(), ddst.data_ptr(), half, sgs.MEM_DEVICE)
+        return sum(q.stats()["edges_traversed"] for q in queries)
+
+    for k in range(a.warmup):
+        run_dev(dev_batches[k])
+    # ---------------- timed region (inputs resident in HBM)
+    e.kernel_timing(True)
+    clocks = Clocks(R.local)
+    R.barrier()
+    torch.cuda.synchronize()
+    e.synchronize()
+    clocks.start()
+    w0 = time.perf_counter()
+    edges = 0
+    dev_ms = 0.0
+    per_step = []
+    for k in range(a.steps):
+        ed = run_dev(dev_batches[a.warmup + k])
+        ms = e.engine_stats()["last_batch_ms"]
+        edges += ed
+        dev_ms += ms
+        per_step.append((ed, ms))
+    e.synchronize()
+    torch.cuda.synchronize()
+    R.barrier()
+    wall_ms = (time.perf_counter() - w0) * 1e3
+    clk = clocks.stop()
+    kst = e.kernel_stats()
+    e.kernel_timing(False)
+    del dev_batches
+    # ---------------- e2e (host pinned inputs, summaries read back)
+    e2e = None
+    if not a.no_e2e:
+        host = []
+        for k in range(a.steps):
+            arrs = batch(a.warmup + a.steps + k)
+            pinned = []
+            for x in arrs:
+                t = torch.empty(len(x), dtype=torch.int32, pin_memory=True)
+                t.numpy()[:] = x.view(np.int32)
+                pinned.append(t)
+            host.append(pinned)
+        R.barrier()
+        torch.cuda.synchronize()
+        e_edges, e_ms = 0, 0.0
+        out_bytes = 0
+        for k in range(a.steps):
+            isrc, idst, iw, dsrc, ddst = host[k]
+            t1 = time.perf_counter()
+            e.apply_batch_ptr(isrc.data_ptr(), idst.data_ptr(), iw.data_ptr(), half,
+                              dsrc.data_ptr(), ddst.data_ptr(), half, sgs.MEM_HOST)
+            sums = [q.summary() for q in queries]
+            e_ms += (time.perf_counter() - t1) * 1e3
+            out_bytes = sum(s.nbytes for s in sums)
+            e_edges += sum(q.stats()["edges_traversed"] for q in queries)
+        R.barrier()
+        e2e_ms = R.max(e_ms)
+        e2e = {"value": R.sum(e_edges) / (e2e_ms * 1e6), "unit": UNIT,
+               "h2d_bytes_per_step": half * 3 * 4 + half * 2 * 4,
+               "d2h_bytes_per_step": out_bytes,
+               "ms_per_step": e2e_ms / a.steps}
+    # ---------------- full-size self check: incremental == from-scratch
+    fresh = [e.add_query(sgs.SSSP, 0), e.add_query(sgs.BFS, 0), e.add_query(sgs.CC, 0)]
+    selfcheck = all(np.array_equal(q.summary(), f.summary()) for q, f in zip(queries, fresh))
+    static_gteps = {sgs.SSSP: None}
+    fs = fresh[0].stats()
+    static_gteps = fs["edges_traversed"] / (fs["ms"] * 1e6) if fs["ms"] > 0 else None
+    st = e.engine_stats()
+    # ---------------- aggregate over ranks (replicas)
+    T = R.max(dev_ms)
+    tot_edges = R.sum(edges)
+    value = tot_edges / (T * 1e6)
+    # roofline of the dominant kernel class
+    dom = max(kst, key=lambda k: kst[k]["ms"])
+    kd = kst[dom]
+    peak, peak_src = measured_peak_hbm()
+    achieved = kd["bytes_alg"] / (kd["ms"] * 1e-3) / 1e9 if kd["ms"] > 0 else 0.0
+    tr = profile_traffic()
+    traffic = None
+    if tr and dom in tr.get("per_kind", {}):
+        pk = tr["per_kind"][dom]
+        traffic = (pk["bytes_per_slot"] * kd["slots"] + pk["bytes_per_entry"] * kd["entries"]) / max(kd["launches"], 1)
+    roof = {"bound": "hbm", "kernel": f"seg_map<{dom}>", "achieved": round(achieved, 1),
+            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "peak_source": peak_src, "traffic": traffic,
+            "launches": kd["launches"], "avg_launch_ms": kd["ms"] / max(kd["launches"], 1),
+            "alg_bytes_per_launch": kd["bytes_alg"] / max(kd["launches"], 1)}
+    launches = int(sum(k["launches"] for k in kst.values()))
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": R.world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(T / a.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (device R-MAT, seeded weights and update stream)",
+        "config": {"workload": f"incremental SSSP/BFS/CC, R-MAT scale {a.scale} ef {a.edge_factor} seed {a.seed}, "
+                               f"{a.updates} updates/snapshot (50/50), source 0, HBM budget {a.budget_gb} GB",
+                   "nv": nv, "ne_initial": int(st0["ne"]), "ne_final": int(st["ne"]),
+                   "hbm_resident_fraction": st["hbm_resident_vertices"] / max(nv, 1),
+                   "arena_bytes_hbm": int(st["arena_bytes_hbm"]),
+                   "arena_bytes_host": int(st["arena_bytes_host"]),
+                   "l2": "inputs larger than L2 (edge arena %.1f GB vs %d MB L2)" % (
+                       st["arena_bytes_hbm"] / 1e9, L2_BYTES // 2**20),
+                   "parallelism": "replicas" if R.world > 1 else "single GPU",
+                   "queries": ["sssp:0", "bfs:0", "cc"]},
+        "e2e": e2e,
+        "gpu_launches": None,
+        "roofline": roof,
+        "clocks": clk,
+        "wall_ms_timed": round(wall_ms, 2),
+        "edges_per_step": round(edges / a.steps),
+        "selfcheck_incremental_eq_static": bool(selfcheck),
+        "static_sssp_gteps": round(static_gteps, 3) if static_gteps else None,
+        "gen_s": round(t_gen, 2),
+        "kernel_stats": {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in v.items()}
+                         for k, v in kst.items()},
+    }
+    out["gpu_launches_relax"] = launches
+    if R.rank == 0 and R.world == 1 and not a.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(e, a)
+    e.close()
+    return out
+
+
+def cpu_baseline(e, a):
+    """The oracle's restatements of the reference's serial host oracles
+    (SSSPHostNaive FIFO Bellman-Ford with the explicit weights, BFSHost, and
+    the directed min-label CC), from scratch on the final graph, each stopped
+    after an edge budget sized for about a third of --cpu-seconds; 1 thread."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+
+    row, col, w = e.export(weights=True)
+    nv = len(row) - 1
+    parts = {}
+    per = a.cpu_seconds / 3.0
+    # calibrate the relax rate on a small budget, then size each run
+    t = time.perf_counter()
+    _, e0 = O.sssp_fifo(nv, row, col, w, 0, max_edges=20_000_000)
+    rate = e0 / max(time.perf_counter() - t, 1e-6)
+    budget = int(rate * per)
+    t = time.perf_counter()
+    _, es = O.sssp_fifo(nv, row, col, w, 0, max_edges=budget)
+    ts = time.perf_counter() - t
+    parts["sssp_fifo"] = (es, ts)
+    t = time.perf_counter()
+    _, eb = O.bfs_fifo(nv, row, col, 0, max_edges=budget)
+    tb = time.perf_counter() - t
+    parts["bfs_fifo"] = (eb, tb)
+    t = time.perf_counter()
+    O.cc(nv, row, col)
+    tc = time.perf_counter() - t
+    parts["cc"] = (int(row[-1]), tc)
+    tot_e = sum(p[0] for p in parts.values())
+    tot_t = sum(p[1] for p in parts.values())
+    return {"value": round(tot_e / tot_t / 1e9, 4), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "from-scratch SSSP (FIFO, restating SSSPHostNaive) and BFS (restating BFSHost) "
+                      "from source 0, each stopped after %d relaxations, plus full directed CC, on the "
+                      "final scale-%d graph; single thread" % (budget, a.scale),
+            "parts": {k: {"edges": int(v[0]), "s": round(v[1], 3)} for k, v in parts.items()}}
+
+
+# ----------------------------------------------------------------- reference arm
+def reference_arm(a, R):
+    if R.rank != 0:
+        return None
+    return {"impl": "reference", "metric": METRIC, "unit": UNIT,
+            "unavailable": "reference CPU arm not wired yet"}
+
+
+def main():
+    a = parse()
+    R = Ranks()
+    try:
+        if a.impl == "reference":
+            out = reference_arm(a, R)
+        else:
+            out = engine_arm(a, R)
+        if R.rank == 0 and out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        R.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1313 @@
+// engine.cu -- host side of the B200 streaming-graph engine and the C ABI
+// declared in include/sgs.h.
+//
+// One engine = one dynamic graph in HBM (optionally part of it in pinned host
+// memory under an HBM budget) plus registered queries (BFS, SSSP, CC, PR),
+// all kept up to date snapshot by snapshot.  Everything runs on one CUDA
+// stream; the host only reads a handful of counters per convergence (a
+// batch of rounds is queued back to back and their frontier counters are read
+// once), instead of the reference's blocking count read per segment per round
+// (groute/device/queue.cuh:315-321 called from algo_variants.cuh:628 and
+// framework.cuh:1460).
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/sgs.h"
+#include "sgs_kernels.cuh"
+
+using namespace sgs;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct SgsError {
+  int code;
+  std::string msg;
+};
+
+[[noreturn]] void fail(int code, const std::string &msg) { throw SgsError{code, msg}; }
+
+void ck(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return;
+  cudaGetLastError();
+  fail(e == cudaErrorMemoryAllocation ? SGS_ERR_OOM : SGS_ERR_CUDA,
+       std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(x) ck((x), #x)
+
+template <class T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  void ensure(size_t want) {
+    if (want <= n && p) return;
+    release();
+    size_t bytes = std::max<size_t>(want, 1) * sizeof(T);
+    CK(cudaMalloc((void **)&p, bytes));
+    n = std::max<size_t>(want, 1);
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { release(); }
+};
+
+template <class T>
+struct HBuf {  // pinned, mapped host memory
+  T *p = nullptr;
+  size_t n = 0;
+  void ensure(size_t want) {
+    if (want <= n && p) return;
+    release();
+    CK(cudaHostAlloc((void **)&p, std::max<size_t>(want, 1) * sizeof(T),
+                     cudaHostAllocMapped | cudaHostAllocPortable));
+    n = std::max<size_t>(want, 1);
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~HBuf() { release(); }
+};
+
+struct Frontier {
+  DBuf<uint32_t> vtx;
+  DBuf<uint64_t> ebase;
+  DBuf<uint32_t> ustart;
+};
+
+struct Query {
+  int id = 0;
+  int algo = 0;
+  uint32_t source = 0;
+  DBuf<unsigned long long> st;
+  DBuf<uint32_t> mark;
+  uint32_t stamp = 1;
+  DBuf<double> x, r, pv;
+  sgs_query_stats stats{};
+};
+
+struct Events {
+  cudaEvent_t a = nullptr, b = nullptr;
+  void init() {
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+  }
+  ~Events() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
+inline uint32_t blocks_for(uint64_t n, uint32_t cap) {
+  uint64_t b = (n + 255) / 256;
+  return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(b, cap));
+}
+
+}  // namespace
+
+struct sgs_engine {
+  sgs_config cfg{};
+  int dev = 0;
+  int nsm = 148;
+  cudaStream_t s = nullptr;
+  bool loaded = false;
+
+  // graph
+  uint32_t nv = 0;
+  uint64_t ne = 0;  // live edges (host mirror)
+  uint64_t slots_total = 0;  // used slots (host mirror)
+  DBuf<uint64_t> off;
+  DBuf<uint32_t> slots, live, cap;
+  DBuf<uint32_t> adj_d, wgt_d;
+  HBuf<uint32_t> adj_h, wgt_h;
+  uint64_t arena_cap[2] = {0, 0};
+  DBuf<unsigned long long> arena_top;  // [2]
+  uint32_t split = 0;                   // vertices [0,split) start in HBM
+  uint64_t repacks = 0;
+
+  // frontier scratch
+  Frontier fb[2];
+  uint32_t ucap = 0;
+  static constexpr uint32_t kSpecial = 8;  // extra counter slots at the end
+  DBuf<unsigned long long> cnt;            // [max_rounds + 2 + kSpecial]
+  unsigned long long *h_cnt = nullptr;     // pinned mirror
+  DBuf<uint32_t> emark;                    // engine-level marks (touched sets)
+  uint32_t estamp = 1;
+  DBuf<double> l1;                         // PR per-round L1
+
+  // batch scratch
+  DBuf<uint32_t> b_isrc, b_idst, b_iw, b_dsrc, b_ddst;
+  DBuf<uint64_t> b_ikeys, b_ikeys_s, b_ikept, b_dkeys, b_dkeys_s;
+  DBuf<uint32_t> b_iw_s, b_iw_kept, b_gstart;
+  DBuf<unsigned char> b_flag;
+  DBuf<uint32_t> b_nkept;
+  DBuf<unsigned int> b_err;
+  DBuf<unsigned long long> b_stat;  // [0] demand d, [1] demand h, [2] tombs, [3] inval
+  DBuf<uint64_t> wbase;
+  DBuf<uint32_t> rl_vtx, rl_len;
+  DBuf<uint64_t> rl_from, rl_to;
+  DBuf<unsigned int> rl_count;
+  DBuf<unsigned char> cub_tmp;
+
+  // per-kernel-class timing
+  bool ktiming = false;
+  std::vector<cudaEvent_t> kev;  // 2 per queued launch
+  sgs_kernel_stats kst[SGS_K_COUNT]{};
+
+  std::vector<std::unique_ptr<Query>> queries;
+  int next_qid = 1;
+  sgs_engine_stats est{};
+  Events ev_batch, ev_apply, ev_q;
+
+  ~sgs_engine() {
+    for (auto ev : kev) cudaEventDestroy(ev);
+    if (h_cnt) cudaFreeHost(h_cnt);
+    if (s) cudaStreamDestroy(s);
+  }
+
+  GraphView view() {
+    GraphView g;
+    g.nv = nv;
+    g.off = off.p;
+    g.slots = slots.p;
+    g.live = live.p;
+    g.cap = cap.p;
+    g.adj_d = adj_d.p;
+    g.wgt_d = wgt_d.p;
+    g.adj_h = adj_h.p;
+    g.wgt_h = wgt_h.p;
+    g.wmode = cfg.weight_mode;
+    return g;
+  }
+  FrontierView fview(uint32_t buf, unsigned long long *counter) {
+    FrontierView f;
+    f.vtx = fb[buf & 1].vtx.p;
+    f.ebase = fb[buf & 1].ebase.p;
+    f.ustart = fb[buf & 1].ustart.p;
+    f.counter = (uint64_t *)counter;
+    f.ucap = ucap;
+    return f;
+  }
+  unsigned long long *special(uint32_t k) { return cnt.p + cfg.max_rounds + 2 + k; }
+  uint32_t grid_map() const { return (uint32_t)nsm * 8; }
+  uint32_t grid_elem(uint64_t n) const { return blocks_for(n, (uint32_t)nsm * 8); }
+  size_t wbytes() const { return cfg.weight_mode == SGS_W_EXPLICIT ? 8 : 4; }
+
+  void cub_ensure(size_t bytes) { cub_tmp.ensure(bytes); }
+
+  void sync() { CK(cudaStreamSynchronize(s)); }
+
+  // ------------------------------------------------------------------ setup
+  void init(const sgs_config &c) {
+    cfg = c;
+    if (cfg.max_rounds == 0) cfg.max_rounds = 1000;
+    if (cfg.pr_alpha <= 0 || cfg.pr_alpha >= 1) fail(SGS_ERR_INVALID, "pr_alpha must be in (0,1)");
+    if (cfg.weight_mode < 0 || cfg.weight_mode > 2) fail(SGS_ERR_INVALID, "bad weight_mode");
+    dev = cfg.device;
+    CK(cudaSetDevice(dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    cnt.ensure(cfg.max_rounds + 2 + kSpecial);
+    CK(cudaHostAlloc((void **)&h_cnt, (cfg.max_rounds + 2 + kSpecial) * sizeof(unsigned long long),
+                     cudaHostAllocDefault));
+    arena_top.ensure(2);
+    b_err.ensure(1);
+    b_stat.ensure(8);
+    b_nkept.ensure(1);
+    rl_count.ensure(1);
+    l1.ensure(cfg.max_rounds + 2);
+    ev_batch.init();
+    ev_apply.init();
+    ev_q.init();
+  }
+
+  // ------------------------------------------------------------- graph load
+  // Lays the graph out in arenas from a device CSR: per-vertex capacity with
+  // slack, offsets by an exclusive scan, the first `split` vertices in HBM
+  // (as many whole segments as the HBM budget allows), the rest pinned host.
+  void load_device_csr(uint32_t n, const uint64_t *d_row, const uint32_t *d_col,
+                       const uint32_t *d_w) {
+    if (n == 0) fail(SGS_ERR_INVALID, "empty graph");
+    if (n >= (1u << 27)) fail(SGS_ERR_INVALID, "more than 2^27-1 vertices is not supported");
+    queries.clear();
+    est = sgs_engine_stats{};
+    nv = n;
+    uint64_t ne_in = 0;
+    CK(cudaMemcpyAsync(&ne_in, d_row + nv, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    sync();
+    if (ne_in >= (1ull << CNT_SHIFT)) fail(SGS_ERR_INVALID, "too many edges");
+    if (cfg.weight_mode == SGS_W_EXPLICIT && ne_in && !d_w)
+      fail(SGS_ERR_INVALID, "explicit weight mode needs weights");
+    off.ensure(nv);
+    slots.ensure(nv);
+    live.ensure(nv);
+    cap.ensure(nv);
+    k_row_degrees<<<grid_elem(nv), 256, 0, s>>>(d_row, nv, slots.p);
+    CK(cudaGetLastError());
+    layout_from(slots.p, /*extra=*/0);
+    CK(cudaMemcpyAsync(live.p, slots.p, sizeof(uint32_t) * nv, cudaMemcpyDeviceToDevice, s));
+    // copy lists
+    reset_counters(1);
+    FrontierView f0 = fview(0, special(0));
+    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), nullptr, 2, f0);
+    LoadCsrOp op{view(), d_row, d_col, cfg.weight_mode == SGS_W_EXPLICIT ? d_w : nullptr};
+    seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(f0, fview(1, special(1)), op, nullptr);
+    CK(cudaGetLastError());
+    sync();
+    ne = ne_in;
+    slots_total = ne_in;
+    loaded = true;
+  }
+
+  // New arena layout for blocks whose sizes are in `sz` (slots): capacities
+  // with slack, offsets, tier split, arena allocation.  Leaves off/cap set and
+  // the arenas allocated but empty; returns nothing (fills members).
+  void layout_from(const uint32_t *sz, uint64_t extra) {
+    DBuf<uint64_t> scan;
+    scan.ensure((size_t)nv + 1);
+    k_layout_caps<<<grid_elem(nv), 256, 0, s>>>(sz, nv, cfg.slack_div, cap.p);
+    k_u32_to_u64<<<grid_elem(nv), 256, 0, s>>>(cap.p, nv, scan.p);
+    CK(cudaMemsetAsync(scan.p + nv, 0, sizeof(uint64_t), s));
+    size_t tb = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, scan.p, scan.p, (int)(nv + 1), s));
+    cub_ensure(tb);
+    CK(cub::DeviceScan::ExclusiveSum(cub_tmp.p, tb, scan.p, scan.p, (int)(nv + 1), s));
+    std::vector<uint64_t> hs((size_t)nv + 1);
+    CK(cudaMemcpyAsync(hs.data(), scan.p, sizeof(uint64_t) * (nv + 1), cudaMemcpyDeviceToHost, s));
+    sync();
+    const uint64_t total = hs[nv];
+    // tier split on segment boundaries
+    uint32_t sp = nv;
+    if (cfg.hbm_budget_gb > 0) {
+      const double budget_slots = cfg.hbm_budget_gb * 1e9 / (double)wbytes();
+      const double usable = budget_slots / (1.0 + std::max(0.0, cfg.arena_headroom));
+      const uint32_t nseg = std::max<uint32_t>(1, cfg.segments);
+      // segment s = vertices [b_s, b_{s+1}) with ~total/nseg slots each
+      sp = 0;
+      for (uint32_t sg = 1; sg <= nseg; ++sg) {
+        uint64_t target = (uint64_t)((double)total * sg / nseg);
+        uint32_t b = (uint32_t)(std::lower_bound(hs.begin(), hs.end(), target) - hs.begin());
+        b = std::min(b, nv);
+        if ((double)hs[b] <= usable) sp = b;
+        else break;
+      }
+    }
+    split = sp;
+    const double hr = std::max(0.0, cfg.arena_headroom);
+    uint64_t need_d = hs[sp], need_h = total - hs[sp];
+    uint64_t cap_d = need_d + (uint64_t)(need_d * hr) + 4096 + (sp == nv ? extra : 0);
+    uint64_t cap_h = need_h ? need_h + (uint64_t)(need_h * hr) + 4096 + extra : 0;
+    if (cfg.hbm_budget_gb > 0) {
+      const uint64_t budget_slots = (uint64_t)(cfg.hbm_budget_gb * 1e9 / (double)wbytes());
+      cap_d = std::min(cap_d, std::max(budget_slots, need_d));
+      if (sp < nv && cap_h < need_h + extra) cap_h = need_h + extra + 4096;
+    }
+    adj_d.ensure(cap_d);
+    if (cfg.weight_mode == SGS_W_EXPLICIT) wgt_d.ensure(cap_d);
+    if (cap_h) {
+      adj_h.ensure(cap_h);
+      if (cfg.weight_mode == SGS_W_EXPLICIT) wgt_h.ensure(cap_h);
+    }
+    arena_cap[0] = cap_d;
+    arena_cap[1] = cap_h;
+    k_assign_off<<<grid_elem(nv), 256, 0, s>>>(scan.p, nv, sp, hs[sp], off.p);
+    unsigned long long tops[2] = {need_d, need_h};
+    CK(cudaMemcpyAsync(arena_top.p, tops, sizeof(tops), cudaMemcpyHostToDevice, s));
+    ensure_frontier(cap_d + cap_h);
+    est.arena_bytes_hbm = cap_d * wbytes();
+    est.arena_bytes_host = cap_h * wbytes();
+    est.hbm_resident_vertices = sp;
+    sync();
+  }
+
+  void ensure_frontier(uint64_t max_slots) {
+    const uint32_t need_u = (uint32_t)std::min<uint64_t>(max_slots / UNIT + 2, 0xFFFFFFF0ull);
+    for (int i = 0; i < 2; ++i) {
+      fb[i].vtx.ensure((size_t)nv + 1);
+      fb[i].ebase.ensure((size_t)nv + 1);
+      if (need_u > ucap) fb[i].ustart.ensure(need_u);
+    }
+    if (need_u > ucap) ucap = need_u;
+    emark.ensure(nv);
+    CK(cudaMemsetAsync(emark.p, 0, sizeof(uint32_t) * nv, s));
+    estamp = 1;
+  }
+
+  // Repack: fresh arenas sized from the current slot counts (+extra room),
+  // every block copied (tombstones included).
+  void repack(uint64_t extra) {
+    DBuf<uint64_t> old_off;
+    old_off.ensure(nv);
+    CK(cudaMemcpyAsync(old_off.p, off.p, sizeof(uint64_t) * nv, cudaMemcpyDeviceToDevice, s));
+    DBuf<uint32_t> od, ow;
+    HBuf<uint32_t> oh, ohw;
+    std::swap(od.p, adj_d.p); std::swap(od.n, adj_d.n);
+    std::swap(ow.p, wgt_d.p); std::swap(ow.n, wgt_d.n);
+    std::swap(oh.p, adj_h.p); std::swap(oh.n, adj_h.n);
+    std::swap(ohw.p, wgt_h.p); std::swap(ohw.n, wgt_h.n);
+    layout_from(slots.p, extra);
+    reset_counters(1);
+    FrontierView f0 = fview(0, special(0));
+    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), nullptr, 2, f0);
+    CopyBlockOp op{view(), old_off.p, off.p, od.p, ow.p, oh.p, ohw.p};
+    seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(f0, fview(1, special(1)), op, nullptr);
+    CK(cudaGetLastError());
+    sync();
+    ++repacks;
+  }
+
+  void reset_counters(uint32_t) {
+    CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long) * (cfg.max_rounds + 2 + kSpecial), s));
+  }
+
+  // ----------------------------------------------------------- convergence
+  // Runs relaxation rounds from the frontier in buffer 0 / cnt[0] until a
+  // round produces an empty frontier.  Rounds are queued in batches; the
+  // host reads the batch's counters once.
+  void ensure_kev(size_t n) {
+    while (kev.size() < n) {
+      cudaEvent_t ev;
+      CK(cudaEventCreate(&ev));
+      kev.push_back(ev);
+    }
+  }
+
+  // Accounts one timed launch: in = packed input counter of the launch.
+  void account(int kind, unsigned long long in, cudaEvent_t a, cudaEvent_t b) {
+    const uint64_t n = in >> CNT_SHIFT, T = in & EDGE_MASK;
+    if (!n) return;
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    static const double per_slot[SGS_K_COUNT] = {16, 12, 12, 12, 20};
+    sgs_kernel_stats &k = kst[kind];
+    k.launches += 1;
+    k.slots += T;
+    k.entries += n;
+    k.bytes_alg += per_slot[kind] * (double)T + 20.0 * (double)n;
+    k.ms += ms;
+  }
+
+  template <class MakeOp>
+  uint32_t run_rounds(MakeOp make_op, unsigned long long *edge_stat, bool &converged,
+                      int kind) {
+    const uint32_t maxr = cfg.max_rounds;
+    uint32_t r = 0;
+    uint32_t rb = 2;
+    converged = false;
+    // empty initial frontier?
+    CK(cudaMemcpyAsync(h_cnt, cnt.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    sync();
+    if (h_cnt[0] == 0) { converged = true; return 0; }
+    while (r < maxr) {
+      const uint32_t nb = std::min(rb, maxr - r);
+      if (ktiming) ensure_kev(2 * nb);
+      for (uint32_t k = 0; k < nb; ++k) {
+        const uint32_t rr = r + k;
+        auto op = make_op(rr);
+        if (ktiming) CK(cudaEventRecord(kev[2 * k], s));
+        seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(rr, cnt.p + rr), fview(rr + 1, cnt.p + rr + 1),
+                                                     op, edge_stat);
+        if (ktiming) CK(cudaEventRecord(kev[2 * k + 1], s));
+      }
+      CK(cudaGetLastError());
+      // counters r .. r+nb: inputs of the queued rounds and the last output
+      CK(cudaMemcpyAsync(h_cnt, cnt.p + r, sizeof(unsigned long long) * (nb + 1),
+                         cudaMemcpyDeviceToHost, s));
+      sync();
+      if (ktiming)
+        for (uint32_t k = 0; k < nb; ++k) account(kind, h_cnt[k], kev[2 * k], kev[2 * k + 1]);
+      for (uint32_t k = 0; k < nb; ++k)
+        if (h_cnt[k + 1] == 0) { converged = true; return r + k + 1; }
+      r += nb;
+      rb = std::min<uint32_t>(rb * 2, 16);
+    }
+    return r;
+  }
+
+  uint32_t next_stamps(Query &q, uint32_t n) {
+    if ((uint64_t)q.stamp + n + 2 >= 0xFFFFFFF0ull) {
+      CK(cudaMemsetAsync(q.mark.p, 0, sizeof(uint32_t) * nv, s));
+      q.stamp = 1;
+    }
+    uint32_t base = q.stamp;
+    q.stamp += n;
+    return base;
+  }
+
+  // Relax from the frontier already in buffer 0 until convergence.
+  uint32_t converge_query(Query &q, unsigned long long *edge_stat, bool &conv) {
+    const uint32_t base = next_stamps(q, cfg.max_rounds + 2);
+    GraphView g = view();
+    if (q.algo == SGS_CC) {
+      return run_rounds([&](uint32_t rr) { return RelaxLabelOp{g, q.st.p, q.mark.p, base + rr + 1}; },
+                        edge_stat, conv, SGS_K_CC);
+    }
+    const int unit = q.algo == SGS_BFS;
+    return run_rounds(
+        [&](uint32_t rr) { return RelaxMinOp{g, q.st.p, q.mark.p, base + rr + 1, unit}; },
+        edge_stat, conv, unit ? SGS_K_BFS : SGS_K_SSSP);
+  }
+
+  // PageRank rounds over the static frontier of all non-empty blocks:
+  // absorb (value += residual) then push alpha*res/outdeg; stop after the
+  // first round whose absorbed residual L1 is below pr_tol.
+  uint32_t pr_rounds(Query &q, unsigned long long *edge_stat, bool &conv, double &last_l1) {
+    GraphView g = view();
+    reset_counters(0);
+    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(g, nullptr, 2, fview(0, cnt.p));
+    const uint32_t maxr = cfg.max_rounds;
+    CK(cudaMemsetAsync(l1.p, 0, sizeof(double) * (maxr + 2), s));
+    std::vector<double> hl(maxr + 2);
+    uint32_t r = 0, rb = 8;
+    conv = false;
+    last_l1 = 0;
+    PrPushOp op{g, q.pv.p, q.r.p};
+    unsigned long long pr_in = 0;
+    if (ktiming) {
+      CK(cudaMemcpyAsync(&pr_in, cnt.p, sizeof(pr_in), cudaMemcpyDeviceToHost, s));
+      sync();
+    }
+    while (r < maxr) {
+      const uint32_t nb = std::min(rb, maxr - r);
+      if (ktiming) ensure_kev(2 * nb);
+      for (uint32_t k = 0; k < nb; ++k) {
+        k_pr_absorb<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(g, q.x.p, q.r.p, q.pv.p, cfg.pr_alpha,
+                                                           l1.p + r + k);
+        if (ktiming) CK(cudaEventRecord(kev[2 * k], s));
+        seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, cnt.p), fview(1, cnt.p + 1), op,
+                                                     edge_stat);
+        if (ktiming) CK(cudaEventRecord(kev[2 * k + 1], s));
+      }
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(hl.data(), l1.p + r, sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
+      sync();
+      if (ktiming)
+        for (uint32_t k = 0; k < nb; ++k) account(SGS_K_PR_PUSH, pr_in, kev[2 * k], kev[2 * k + 1]);
+      for (uint32_t k = 0; k < nb; ++k) {
+        last_l1 = hl[k];
+        if (hl[k] < cfg.pr_tol) { conv = true; return r + k + 1; }
+      }
+      r += nb;
+      rb = std::min<uint32_t>(rb * 2, 32);
+    }
+    return r;
+  }
+
+  // ---------------------------------------------------------------- queries
+  Query &find(int qid) {
+    for (auto &q : queries)
+      if (q->id == qid) return *q;
+    fail(SGS_ERR_INVALID, "unknown query id");
+  }
+
+  void start_query(Query &q) {
+    GraphView g = view();
+    CK(cudaEventRecord(ev_q.a, s));
+    CK(cudaMemsetAsync(b_stat.p, 0, sizeof(unsigned long long) * 8, s));
+    unsigned long long *es = b_stat.p + 4;
+    bool conv = false;
+    uint32_t rounds = 0;
+    double l1v = 0;
+    if (q.algo == SGS_PR) {
+      k_pr_init<<<grid_elem(nv), 256, 0, s>>>(q.x.p, q.r.p, nv, 1.0 - cfg.pr_alpha);
+      rounds = pr_rounds(q, es, conv, l1v);
+    } else {
+      k_init_state<<<grid_elem(nv), 256, 0, s>>>(q.st.p, nv, q.algo, q.source);
+      reset_counters(0);
+      if (q.algo == SGS_CC) {
+        k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(g, q.st.p, 1, fview(0, cnt.p));
+      } else {
+        uint32_t d = 0;
+        CK(cudaMemcpyAsync(&d, slots.p + q.source, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        sync();
+        k_append_one<<<1, 32, 0, s>>>(fview(0, cnt.p), q.source, d);
+      }
+      CK(cudaGetLastError());
+      rounds = converge_query(q, es, conv);
+    }
+    CK(cudaEventRecord(ev_q.b, s));
+    finish_stats(q, rounds, conv, l1v, 0);
+  }
+
+  void finish_stats(Query &q, uint32_t rounds, bool conv, double l1v, uint64_t inval) {
+    unsigned long long e = 0;
+    CK(cudaMemcpyAsync(&e, b_stat.p + 4, sizeof(e), cudaMemcpyDeviceToHost, s));
+    sync();
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ev_q.a, ev_q.b));
+    q.stats.edges_traversed = e;
+    q.stats.edges_total += e;
+    q.stats.rounds = rounds;
+    q.stats.converged = conv ? 1 : 0;
+    q.stats.ms = ms;
+    q.stats.pr_residual_l1 = l1v;
+    q.stats.invalidated = inval;
+  }
+
+  int add_query(int algo, uint32_t source) {
+    if (!loaded) fail(SGS_ERR_STATE, "no graph loaded");
+    if (algo < 0 || algo > 3) fail(SGS_ERR_INVALID, "unknown algorithm");
+    auto q = std::make_unique<Query>();
+    q->id = next_qid++;
+    q->algo = algo;
+    q->source = std::min(source, nv - 1);
+    if (algo == SGS_PR) {
+      q->x.ensure(nv);
+      q->r.ensure(nv);
+      q->pv.ensure(nv);
+    } else {
+      q->st.ensure(nv);
+      q->mark.ensure(nv);
+      CK(cudaMemsetAsync(q->mark.p, 0, sizeof(uint32_t) * nv, s));
+    }
+    Query &ref = *q;
+    queries.push_back(std::move(q));
+    start_query(ref);
+    return ref.id;
+  }
+
+  // ------------------------------------------------------------ snapshots
+  void upload(DBuf<uint32_t> &dst, const uint32_t *src, uint64_t n, int mem) {
+    dst.ensure(n);
+    if (n)
+      CK(cudaMemcpyAsync(dst.p, src, n * sizeof(uint32_t),
+                         mem == SGS_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+  }
+
+  int sort_bits() const {
+    int b = 1;
+    while (b < 32 && (1ull << b) < nv) ++b;
+    return 32 + b;
+  }
+
+  void apply_batch(const uint32_t *is, const uint32_t *id, const uint32_t *iw, uint64_t ni,
+                   const uint32_t *ds, const uint32_t *dd, uint64_t nd, int mem) {
+    if (!loaded) fail(SGS_ERR_STATE, "no graph loaded");
+    if (ni >= (1ull << 31) || nd >= (1ull << 31)) fail(SGS_ERR_INVALID, "batch too large");
+    if ((ni && (!is || !id)) || (nd && (!ds || !dd))) fail(SGS_ERR_INVALID, "null batch array");
+    const bool explicit_w = cfg.weight_mode == SGS_W_EXPLICIT;
+    if (ni && explicit_w && !iw) fail(SGS_ERR_INVALID, "explicit weight mode needs insert weights");
+    GraphView g = view();
+    CK(cudaEventRecord(ev_batch.a, s));
+    // ---- upload + keys + sort
+    upload(b_isrc, is, ni, mem);
+    upload(b_idst, id, ni, mem);
+    if (explicit_w) upload(b_iw, iw, ni, mem);
+    upload(b_dsrc, ds, nd, mem);
+    upload(b_ddst, dd, nd, mem);
+    b_ikeys.ensure(ni); b_ikeys_s.ensure(ni); b_ikept.ensure(ni);
+    b_iw_s.ensure(ni); b_iw_kept.ensure(ni); b_flag.ensure(ni);
+    b_dkeys.ensure(nd); b_dkeys_s.ensure(nd);
+    CK(cudaMemsetAsync(b_err.p, 0, sizeof(unsigned int), s));
+    CK(cudaMemsetAsync(b_stat.p, 0, sizeof(unsigned long long) * 8, s));
+    if (ni)
+      k_make_keys<<<grid_elem(ni), 256, 0, s>>>(b_isrc.p, b_idst.p, ni, nv, b_ikeys.p,
+                                                explicit_w ? b_iw.p : nullptr, explicit_w, b_err.p);
+    if (nd)
+      k_make_keys<<<grid_elem(nd), 256, 0, s>>>(b_dsrc.p, b_ddst.p, nd, nv, b_dkeys.p, nullptr, 0,
+                                                b_err.p);
+    const int eb = sort_bits();
+    size_t tb = 0, t2 = 0, t3 = 0;
+    if (nd) CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, b_dkeys.p, b_dkeys_s.p, (int)nd, 0, eb, s));
+    if (ni) {
+      CK(cub::DeviceRadixSort::SortPairs(nullptr, t2, b_ikeys.p, b_ikeys_s.p,
+                                         explicit_w ? b_iw.p : b_isrc.p, b_iw_s.p, (int)ni, 0, eb, s));
+      CK(cub::DeviceSelect::Flagged(nullptr, t3, b_ikeys_s.p, b_flag.p, b_ikept.p, b_nkept.p, (int)ni, s));
+    }
+    cub_ensure(std::max(tb, std::max(t2, t3)));
+    if (nd) CK(cub::DeviceRadixSort::SortKeys(cub_tmp.p, tb, b_dkeys.p, b_dkeys_s.p, (int)nd, 0, eb, s));
+    CK(cudaMemsetAsync(b_nkept.p, 0, sizeof(uint32_t), s));
+    if (ni) {
+      CK(cub::DeviceRadixSort::SortPairs(cub_tmp.p, t2, b_ikeys.p, b_ikeys_s.p,
+                                         explicit_w ? b_iw.p : b_isrc.p, b_iw_s.p, (int)ni, 0, eb, s));
+      k_filter_inserts<<<grid_elem(ni), 256, 0, s>>>(b_ikeys_s.p, (uint32_t)ni, b_dkeys_s.p,
+                                                     (uint32_t)nd, b_flag.p);
+      CK(cub::DeviceSelect::Flagged(cub_tmp.p, t3, b_ikeys_s.p, b_flag.p, b_ikept.p, b_nkept.p,
+                                    (int)ni, s));
+      if (explicit_w)
+        CK(cub::DeviceSelect::Flagged(cub_tmp.p, t3, b_iw_s.p, b_flag.p, b_iw_kept.p, b_nkept.p,
+                                      (int)ni, s));
+    }
+    CK(cudaGetLastError());
+    unsigned int herr = 0;
+    CK(cudaMemcpyAsync(&herr, b_err.p, sizeof(herr), cudaMemcpyDeviceToHost, s));
+    sync();
+    if (herr & 1u) fail(SGS_ERR_INVALID, "batch vertex id out of range");
+    if (herr & 2u) fail(SGS_ERR_INVALID, "insert weight 0 (weights must be >= 1)");
+
+    bool any_pr = false;
+    for (auto &q : queries) any_pr |= q->algo == SGS_PR;
+    // per-query timing accumulators
+    std::vector<float> qms(queries.size(), 0.f);
+    std::vector<unsigned long long> qedges(queries.size(), 0);
+    std::vector<uint64_t> qinval(queries.size(), 0);
+
+    // ---- PR cancel over the old out-lists of touched sources
+    if (any_pr) {
+      build_touched(g, ni, nd);
+      for (size_t i = 0; i < queries.size(); ++i) {
+        Query &q = *queries[i];
+        if (q.algo != SGS_PR) continue;
+        PrAmendOp op{g, q.x.p, q.r.p, -cfg.pr_alpha};
+        seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(2)), fview(1, special(3)), op,
+                                                     nullptr);
+      }
+    }
+    // ---- deletion phase: parent-tree invalidation on the old graph
+    for (size_t i = 0; i < queries.size() && nd; ++i) {
+      Query &q = *queries[i];
+      if (q.algo == SGS_PR) continue;
+      CK(cudaEventRecord(ev_q.a, s));
+      CK(cudaMemsetAsync(b_stat.p + 3, 0, sizeof(unsigned long long) * 2, s));
+      reset_counters(0);
+      k_seed_deleted<<<grid_elem(nd), 256, 0, s>>>(g, q.st.p, q.algo == SGS_CC, b_dkeys_s.p,
+                                                   (uint32_t)nd, b_stat.p + 3, fview(0, cnt.p));
+      bool conv = false;
+      InvalidateOp base{g, q.st.p, q.algo == SGS_CC, b_stat.p + 3};
+      run_rounds([&](uint32_t) { return base; }, b_stat.p + 4, conv, SGS_K_INVALIDATE);
+      if (!conv) fail(SGS_ERR_NOCONV, "invalidation did not converge");
+      CK(cudaEventRecord(ev_q.b, s));
+      unsigned long long hv[2];
+      CK(cudaMemcpyAsync(hv, b_stat.p + 3, sizeof(hv), cudaMemcpyDeviceToHost, s));
+      sync();
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, ev_q.a, ev_q.b));
+      qms[i] += ms;
+      qinval[i] = hv[0];
+      qedges[i] += hv[1];
+    }
+
+    // ---- graph update
+    CK(cudaEventRecord(ev_apply.a, s));
+    apply_graph(ni, nd);
+    CK(cudaEventRecord(ev_apply.b, s));
+    g = view();
+
+    // ---- PR compensate over the new out-lists
+    if (any_pr) {
+      build_touched(g, ni, nd);
+      for (size_t i = 0; i < queries.size(); ++i) {
+        Query &q = *queries[i];
+        if (q.algo != SGS_PR) continue;
+        PrAmendOp op{g, q.x.p, q.r.p, cfg.pr_alpha};
+        seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(2)), fview(1, special(3)), op,
+                                                     nullptr);
+      }
+    }
+    // ---- add phase + convergence per query
+    for (size_t i = 0; i < queries.size(); ++i) {
+      Query &q = *queries[i];
+      CK(cudaEventRecord(ev_q.a, s));
+      CK(cudaMemsetAsync(b_stat.p + 4, 0, sizeof(unsigned long long), s));
+      bool conv = false;
+      uint32_t rounds = 0;
+      double l1v = 0;
+      if (q.algo == SGS_PR) {
+        rounds = pr_rounds(q, b_stat.p + 4, conv, l1v);
+      } else {
+        reset_counters(0);
+        const uint32_t st0 = next_stamps(q, 1);
+        if (qinval[i] > 0) {
+          // re-push from every reached vertex (SyncPushDDBAll)
+          k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(g, q.st.p, q.algo == SGS_CC ? 1 : 0,
+                                                         fview(0, cnt.p));
+        } else if (ni) {
+          k_relax_inserted<<<grid_elem(ni), 256, 0, s>>>(g, q.st.p, q.algo, b_ikept.p,
+                                                         explicit_w ? b_iw_kept.p : nullptr,
+                                                         b_nkept.p, q.mark.p, st0, fview(0, cnt.p),
+                                                         b_stat.p + 4);
+        }
+        CK(cudaGetLastError());
+        rounds = converge_query(q, b_stat.p + 4, conv);
+      }
+      CK(cudaEventRecord(ev_q.b, s));
+      unsigned long long e = 0;
+      CK(cudaMemcpyAsync(&e, b_stat.p + 4, sizeof(e), cudaMemcpyDeviceToHost, s));
+      sync();
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, ev_q.a, ev_q.b));
+      q.stats.edges_traversed = qedges[i] + e;
+      q.stats.edges_total += qedges[i] + e;
+      q.stats.rounds = rounds;
+      q.stats.converged = conv;
+      q.stats.ms = qms[i] + ms;
+      q.stats.pr_residual_l1 = l1v;
+      q.stats.invalidated = qinval[i];
+      if (!conv) fail(SGS_ERR_NOCONV, "round limit reached before convergence");
+    }
+    CK(cudaEventRecord(ev_batch.b, s));
+    sync();
+    float ams = 0, bms = 0;
+    CK(cudaEventElapsedTime(&ams, ev_apply.a, ev_apply.b));
+    CK(cudaEventElapsedTime(&bms, ev_batch.a, ev_batch.b));
+    est.last_apply_ms = ams;
+    est.last_batch_ms = bms;
+  }
+
+  // Union of the distinct sources of the sorted deletes and kept inserts, with
+  // their current block sizes, as a frontier in buffer 0 / special(2).
+  void build_touched(const GraphView &g, uint64_t ni, uint64_t nd) {
+    if (estamp >= 0xFFFFFFF0u) {
+      CK(cudaMemsetAsync(emark.p, 0, sizeof(uint32_t) * nv, s));
+      estamp = 1;
+    }
+    const uint32_t st = ++estamp;
+    CK(cudaMemsetAsync(special(2), 0, sizeof(unsigned long long), s));
+    if (nd)
+      k_group_heads<<<grid_elem(nd), 256, 0, s>>>(g, b_dkeys_s.p, nullptr, (uint32_t)nd, nullptr,
+                                                  emark.p, st, fview(0, special(2)));
+    if (ni)
+      k_group_heads<<<grid_elem(ni), 256, 0, s>>>(g, b_ikept.p, b_nkept.p, 0, nullptr, emark.p, st,
+                                                  fview(0, special(2)));
+    CK(cudaGetLastError());
+  }
+
+  // Deletes become tombstones; kept inserts are appended in place or their
+  // block is relocated (capacity x1.5) within its tier; the arena is repacked
+  // first when the relocations would not fit.
+  void apply_graph(uint64_t ni, uint64_t nd) {
+    GraphView g = view();
+    unsigned long long *tombs = b_stat.p + 2;
+    CK(cudaMemsetAsync(tombs, 0, sizeof(unsigned long long), s));
+    if (nd) {
+      b_gstart.ensure((size_t)nv + 1);
+      CK(cudaMemsetAsync(special(4), 0, sizeof(unsigned long long), s));
+      k_group_heads<<<grid_elem(nd), 256, 0, s>>>(g, b_dkeys_s.p, nullptr, (uint32_t)nd, b_gstart.p,
+                                                  nullptr, 0, fview(0, special(4)));
+      TombOp op{g, b_dkeys_s.p, b_gstart.p, (uint32_t)nd};
+      seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(4)), fview(1, special(5)), op,
+                                                   tombs);
+      CK(cudaGetLastError());
+    }
+    uint32_t nkept = 0;
+    uint64_t nreloc = 0;
+    if (ni) {
+      wbase.ensure(nv);
+      InsertCtx c{};
+      c.arena_top = arena_top.p;
+      c.arena_cap[0] = arena_cap[0];
+      c.arena_cap[1] = arena_cap[1];
+      c.err = b_err.p;
+      c.wbase = wbase.p;
+      // dry run: relocation demand per tier
+      CK(cudaMemsetAsync(b_stat.p, 0, sizeof(unsigned long long) * 2, s));
+      k_insert_plan<<<grid_elem(ni), 256, 0, s>>>(g, b_ikept.p, b_nkept.p, c, 1, b_stat.p);
+      unsigned long long h[2], tops[2];
+      CK(cudaMemcpyAsync(h, b_stat.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(tops, arena_top.p, sizeof(tops), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(&nkept, b_nkept.p, sizeof(nkept), cudaMemcpyDeviceToHost, s));
+      sync();
+      if (tops[0] + h[0] > arena_cap[0] || tops[1] + h[1] > arena_cap[1]) {
+        repack(h[0] + h[1] + 4096);
+        g = view();
+        c.arena_cap[0] = arena_cap[0];
+        c.arena_cap[1] = arena_cap[1];
+      }
+      rl_vtx.ensure(nkept + 1);
+      rl_len.ensure(nkept + 1);
+      rl_from.ensure(nkept + 1);
+      rl_to.ensure(nkept + 1);
+      c.rl_vtx = rl_vtx.p;
+      c.rl_from = rl_from.p;
+      c.rl_to = rl_to.p;
+      c.rl_len = rl_len.p;
+      c.rl_count = rl_count.p;
+      CK(cudaMemsetAsync(rl_count.p, 0, sizeof(unsigned int), s));
+      CK(cudaMemsetAsync(b_err.p, 0, sizeof(unsigned int), s));
+      k_insert_plan<<<grid_elem(ni), 256, 0, s>>>(g, b_ikept.p, b_nkept.p, c, 0, nullptr);
+      k_insert_write<<<grid_elem(ni), 256, 0, s>>>(
+          g, b_ikept.p, cfg.weight_mode == SGS_W_EXPLICIT ? b_iw_kept.p : nullptr, b_nkept.p, wbase.p);
+      CK(cudaMemsetAsync(special(6), 0, sizeof(unsigned long long), s));
+      k_reloc_frontier<<<grid_elem(nkept), 256, 0, s>>>(rl_count.p, rl_len.p, fview(0, special(6)));
+      RelocCopyOp op{g, rl_from.p, rl_to.p};
+      seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(6)), fview(1, special(7)), op,
+                                                   nullptr);
+      CK(cudaGetLastError());
+      unsigned int herr = 0, hrl = 0;
+      CK(cudaMemcpyAsync(&herr, b_err.p, sizeof(herr), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(&hrl, rl_count.p, sizeof(hrl), cudaMemcpyDeviceToHost, s));
+      sync();
+      if (herr) fail(SGS_ERR_OOM, "edge arena exhausted while inserting");
+      nreloc = hrl;
+    }
+    unsigned long long ht = 0;
+    CK(cudaMemcpyAsync(&ht, tombs, sizeof(ht), cudaMemcpyDeviceToHost, s));
+    sync();
+    ne = ne + nkept - ht;
+    slots_total += nkept;
+    est.last_inserted = nkept;
+    est.last_deleted = ht;
+    est.last_relocated = nreloc;
+  }
+
+  // --------------------------------------------------------------- output
+  void gather(Query &q, int field, void *out, int mem) {
+    const cudaMemcpyKind kind = mem == SGS_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (q.algo == SGS_PR) {
+      if (field == SGS_FIELD_PARENT) fail(SGS_ERR_INVALID, "PageRank has no parent field");
+      const double *src = field == SGS_FIELD_VALUE ? q.x.p : q.r.p;
+      CK(cudaMemcpyAsync(out, src, sizeof(double) * nv, kind, s));
+      sync();
+      return;
+    }
+    DBuf<uint32_t> tmp;
+    tmp.ensure(nv);
+    if (field == SGS_FIELD_PARENT)
+      k_split_state<<<grid_elem(nv), 256, 0, s>>>(q.st.p, nv, nullptr, tmp.p);
+    else if (field == SGS_FIELD_VALUE || field == SGS_FIELD_BUFFER)
+      k_split_state<<<grid_elem(nv), 256, 0, s>>>(q.st.p, nv, tmp.p, nullptr);
+    else
+      fail(SGS_ERR_INVALID, "unknown field");
+    CK(cudaMemcpyAsync(out, tmp.p, sizeof(uint32_t) * nv, kind, s));
+    sync();
+  }
+
+  void summary(Query &q, uint64_t out[4]) {
+    b_stat.ensure(8);
+    CK(cudaMemsetAsync(b_stat.p, 0, sizeof(unsigned long long) * 4, s));
+    if (q.algo == SGS_PR) {
+      k_summary_pr<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.x.p, nv, (double *)b_stat.p + 1);
+    } else {
+      k_summary<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.st.p, nv, b_stat.p);
+    }
+    CK(cudaGetLastError());
+    unsigned long long h[4];
+    CK(cudaMemcpyAsync(h, b_stat.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    sync();
+    if (q.algo == SGS_PR) h[0] = nv;
+    for (int i = 0; i < 4; ++i) out[i] = h[i];
+  }
+
+  void export_graph(uint64_t *row, uint32_t *col, uint32_t *w, int mem) {
+    DBuf<uint64_t> drow;
+    drow.ensure((size_t)nv + 1);
+    k_u32_to_u64<<<grid_elem(nv), 256, 0, s>>>(live.p, nv, drow.p);
+    CK(cudaMemsetAsync(drow.p + nv, 0, sizeof(uint64_t), s));
+    size_t tb = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, drow.p, drow.p, (int)(nv + 1), s));
+    cub_ensure(tb);
+    CK(cub::DeviceScan::ExclusiveSum(cub_tmp.p, tb, drow.p, drow.p, (int)(nv + 1), s));
+    DBuf<uint32_t> dcol, dw, fill;
+    dcol.ensure(ne + 1);
+    if (w) dw.ensure(ne + 1);
+    fill.ensure(nv);
+    CK(cudaMemsetAsync(fill.p, 0, sizeof(uint32_t) * nv, s));
+    reset_counters(0);
+    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), nullptr, 2, fview(0, special(0)));
+    ExportOp op{view(), drow.p, dcol.p, w ? dw.p : nullptr, fill.p};
+    seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(0)), fview(1, special(1)), op,
+                                                 nullptr);
+    CK(cudaGetLastError());
+    const cudaMemcpyKind kind = mem == SGS_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    CK(cudaMemcpyAsync(row, drow.p, sizeof(uint64_t) * (nv + 1), kind, s));
+    if (ne) CK(cudaMemcpyAsync(col, dcol.p, sizeof(uint32_t) * ne, kind, s));
+    if (w && ne) CK(cudaMemcpyAsync(w, dw.p, sizeof(uint32_t) * ne, kind, s));
+    sync();
+  }
+
+  // ------------------------------------------------------------- generator
+  void load_rmat(uint32_t scale, uint32_t ef, uint64_t seed, double a, double b, double c,
+                 uint64_t wseed) {
+    if (scale < 1 || scale > 26) fail(SGS_ERR_INVALID, "scale must be in [1,26]");
+    if (a < 0 || b < 0 || c < 0 || a + b + c > 1) fail(SGS_ERR_INVALID, "bad R-MAT probabilities");
+    const uint32_t n = 1u << scale;
+    const uint64_t m = (uint64_t)n * ef;
+    if (m >= (1ull << 31)) fail(SGS_ERR_INVALID, "too many edges for the generator");
+    const double S = (double)(1ull << 53);
+    const uint64_t tA = (uint64_t)(a * S), tAB = (uint64_t)((a + b) * S),
+                   tABC = (uint64_t)((a + b + c) * S);
+    const uint64_t key = fin64_host(seed ^ 0x524D4154ull);
+    DBuf<uint64_t> k1, k2;
+    k1.ensure(m);
+    k2.ensure(m);
+    k_rmat<<<grid_elem(m), 256, 0, s>>>(scale, m, key, tA, tAB, tABC, 1, k1.p);
+    size_t tb = 0, tu = 0;
+    DBuf<uint32_t> nsel;
+    nsel.ensure(1);
+    CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, k1.p, k2.p, (int)m, 0, 64, s));
+    CK(cub::DeviceSelect::Unique(nullptr, tu, k2.p, k1.p, nsel.p, (int)m, s));
+    cub_ensure(std::max(tb, tu));
+    CK(cub::DeviceRadixSort::SortKeys(cub_tmp.p, tb, k1.p, k2.p, (int)m, 0, 64, s));
+    CK(cub::DeviceSelect::Unique(cub_tmp.p, tu, k2.p, k1.p, nsel.p, (int)m, s));
+    uint32_t hn = 0;
+    CK(cudaMemcpyAsync(&hn, nsel.p, sizeof(hn), cudaMemcpyDeviceToHost, s));
+    sync();
+    // the self-loop marker ~0 sorts last
+    uint64_t lastk = 0;
+    if (hn) CK(cudaMemcpyAsync(&lastk, k1.p + hn - 1, sizeof(lastk), cudaMemcpyDeviceToHost, s));
+    sync();
+    if (hn && lastk == ~0ull) --hn;
+    CK(cudaMemcpyAsync(nsel.p, &hn, sizeof(hn), cudaMemcpyHostToDevice, s));
+    k2.release();
+    DBuf<uint64_t> row;
+    DBuf<uint32_t> col, w;
+    row.ensure((size_t)n + 1);
+    col.ensure(hn + 1);
+    k_row_from_sorted<<<grid_elem(n + 1), 256, 0, s>>>(k1.p, nsel.p, n, row.p);
+    k_keys_low<<<grid_elem(hn), 256, 0, s>>>(k1.p, nsel.p, col.p);
+    if (cfg.weight_mode == SGS_W_EXPLICIT) {
+      w.ensure(hn + 1);
+      const uint64_t wkey = fin64_host(wseed ^ 0x57454947ull);
+      k_hash_weights<<<grid_elem(hn), 256, 0, s>>>(k1.p, nsel.p, wkey, w.p);
+    }
+    CK(cudaGetLastError());
+    k1.release();
+    load_device_csr(n, row.p, col.p, cfg.weight_mode == SGS_W_EXPLICIT ? w.p : nullptr);
+  }
+
+  static uint64_t fin64_host(uint64_t x) {
+    uint64_t z = x + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+template <class F>
+static int guarded(F &&f) {
+  try {
+    f();
+    return SGS_OK;
+  } catch (const SgsError &e) {
+    g_last_error = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    g_last_error = "host allocation failed";
+    return SGS_ERR_OOM;
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return SGS_ERR_CUDA;
+  }
+}
+
+extern "C" {
+
+SGS_API const char *sgs_version(void) { return "sgs-b200 0.1"; }
+SGS_API const char *sgs_last_error(void) { return g_last_error.c_str(); }
+
+SGS_API void sgs_config_default(sgs_config *c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->device = 0;
+  c->segments = 512;
+  c->n_stream = 3;
+  c->block_size = 512;
+  c->cache_gb = 0;
+  c->hbm_budget_gb = 0;
+  c->weight_mode = SGS_W_EXPLICIT;
+  c->max_rounds = 1000;
+  c->pr_alpha = 0.85;
+  c->pr_tol = 1e-6 * 0.15;
+  c->slack_div = 8;
+  c->arena_headroom = 0.10;
+}
+
+SGS_API int sgs_create(const sgs_config *cfg, sgs_engine **out) {
+  if (!out) { g_last_error = "null out"; return SGS_ERR_INVALID; }
+  *out = nullptr;
+  return guarded([&] {
+    sgs_config c;
+    if (cfg) c = *cfg;
+    else sgs_config_default(&c);
+    auto e = std::make_unique<sgs_engine>();
+    e->init(c);
+    *out = e.release();
+  });
+}
+
+SGS_API int sgs_destroy(sgs_engine *e) {
+  if (!e) return SGS_OK;
+  return guarded([&] {
+    cudaSetDevice(e->dev);
+    cudaStreamSynchronize(e->s);
+    delete e;
+  });
+}
+
+SGS_API int sgs_load_csr(sgs_engine *e, uint32_t nv, const uint64_t *row, const uint32_t *col,
+                         const uint32_t *w, int mem) {
+  if (!e || !row) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    if (mem == SGS_MEM_DEVICE) {
+      e->load_device_csr(nv, row, col, w);
+      return;
+    }
+    const uint64_t ne = row[nv];
+    for (uint32_t v = 0; v < nv; ++v)
+      if (row[v + 1] < row[v]) fail(SGS_ERR_INVALID, "row offsets must be non-decreasing");
+    if (row[0] != 0) fail(SGS_ERR_INVALID, "row[0] must be 0");
+    for (uint64_t i = 0; i < ne; ++i)
+      if (col[i] >= nv) fail(SGS_ERR_INVALID, "edge destination out of range");
+    const bool ew = e->cfg.weight_mode == SGS_W_EXPLICIT;
+    if (ew && ne && !w) fail(SGS_ERR_INVALID, "explicit weight mode needs weights");
+    if (ew)
+      for (uint64_t i = 0; i < ne; ++i)
+        if (w[i] == 0) fail(SGS_ERR_INVALID, "edge weight 0 (weights must be >= 1)");
+    DBuf<uint64_t> drow;
+    DBuf<uint32_t> dcol, dw;
+    drow.ensure((size_t)nv + 1);
+    dcol.ensure(ne + 1);
+    CK(cudaMemcpyAsync(drow.p, row, sizeof(uint64_t) * (nv + 1), cudaMemcpyHostToDevice, e->s));
+    if (ne) CK(cudaMemcpyAsync(dcol.p, col, sizeof(uint32_t) * ne, cudaMemcpyHostToDevice, e->s));
+    if (ew) {
+      dw.ensure(ne + 1);
+      if (ne) CK(cudaMemcpyAsync(dw.p, w, sizeof(uint32_t) * ne, cudaMemcpyHostToDevice, e->s));
+    }
+    e->load_device_csr(nv, drow.p, dcol.p, ew ? dw.p : nullptr);
+  });
+}
+
+SGS_API int sgs_load_edge_list(sgs_engine *e, uint32_t nv, uint64_t ne, const uint32_t *src,
+                               const uint32_t *dst, const uint32_t *w, int mem) {
+  if (!e || (ne && (!src || !dst))) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    std::vector<uint32_t> hs, hd, hw;
+    const uint32_t *S = src, *D = dst, *W = w;
+    if (mem == SGS_MEM_DEVICE) {
+      hs.resize(ne); hd.resize(ne);
+      if (ne) {
+        CK(cudaMemcpy(hs.data(), src, ne * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hd.data(), dst, ne * 4, cudaMemcpyDeviceToHost));
+      }
+      S = hs.data(); D = hd.data();
+      if (w) {
+        hw.resize(ne);
+        if (ne) CK(cudaMemcpy(hw.data(), w, ne * 4, cudaMemcpyDeviceToHost));
+        W = hw.data();
+      }
+    }
+    uint64_t mx = 0;
+    for (uint64_t i = 0; i < ne; ++i) mx = std::max<uint64_t>(mx, std::max(S[i], D[i]));
+    uint64_t n = nv ? nv : (ne ? mx + 1 : 0);
+    if (n == 0 || n > 0xFFFFFFFFull) fail(SGS_ERR_INVALID, "bad vertex count");
+    if (ne && mx >= n) fail(SGS_ERR_INVALID, "edge endpoint out of range");
+    // counting sort by source, stable (file order within a source)
+    std::vector<uint64_t> row(n + 1, 0);
+    for (uint64_t i = 0; i < ne; ++i) row[S[i] + 1]++;
+    for (uint64_t v = 0; v < n; ++v) row[v + 1] += row[v];
+    std::vector<uint64_t> fill(row.begin(), row.end() - 1);
+    std::vector<uint32_t> col(ne), ww(W ? ne : 0);
+    for (uint64_t i = 0; i < ne; ++i) {
+      const uint64_t p = fill[S[i]]++;
+      col[p] = D[i];
+      if (W) ww[p] = W[i];
+    }
+    // weights: explicit mode without weights falls back to the reference's
+    // synthesized (u+v)%128+1 so that market_big files without weights load
+    if (e->cfg.weight_mode == SGS_W_EXPLICIT && !W) {
+      ww.resize(ne);
+      for (uint32_t u = 0; u < n; ++u)
+        for (uint64_t p = row[u]; p < row[u + 1]; ++p) ww[p] = (u + col[p]) % 128u + 1u;
+    }
+    const int rc = sgs_load_csr(e, (uint32_t)n, row.data(), col.data(),
+                                ww.empty() ? nullptr : ww.data(), SGS_MEM_HOST);
+    if (rc != SGS_OK) fail(rc, g_last_error);
+  });
+}
+
+SGS_API int sgs_load_rmat(sgs_engine *e, uint32_t scale, uint32_t edge_factor, uint64_t seed,
+                          double a, double b, double c, uint64_t wseed) {
+  if (!e) { g_last_error = "null engine"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    e->load_rmat(scale, edge_factor, seed, a, b, c, wseed);
+  });
+}
+
+SGS_API int sgs_query_add(sgs_engine *e, int algo, uint32_t source, int *qid) {
+  if (!e || !qid) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    *qid = e->add_query(algo, source);
+    if (!e->find(*qid).stats.converged) fail(SGS_ERR_NOCONV, "round limit reached before convergence");
+  });
+}
+
+SGS_API int sgs_query_remove(sgs_engine *e, int qid) {
+  if (!e) { g_last_error = "null engine"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    for (size_t i = 0; i < e->queries.size(); ++i)
+      if (e->queries[i]->id == qid) {
+        CK(cudaStreamSynchronize(e->s));
+        e->queries.erase(e->queries.begin() + i);
+        return;
+      }
+    fail(SGS_ERR_INVALID, "unknown query id");
+  });
+}
+
+SGS_API int sgs_apply_batch(sgs_engine *e, const uint32_t *ins_src, const uint32_t *ins_dst,
+                            const uint32_t *ins_w, uint64_t n_ins, const uint32_t *del_src,
+                            const uint32_t *del_dst, uint64_t n_del, int mem) {
+  if (!e) { g_last_error = "null engine"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    e->apply_batch(ins_src, ins_dst, ins_w, n_ins, del_src, del_dst, n_del, mem);
+  });
+}
+
+SGS_API int sgs_gather(sgs_engine *e, int qid, int field, void *out, int mem) {
+  if (!e || !out) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    e->gather(e->find(qid), field, out, mem);
+  });
+}
+
+SGS_API int sgs_get_query_stats(sgs_engine *e, int qid, sgs_query_stats *out) {
+  if (!e || !out) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  return guarded([&] { *out = e->find(qid).stats; });
+}
+
+SGS_API int sgs_get_engine_stats(sgs_engine *e, sgs_engine_stats *out) {
+  if (!e || !out) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    e->est.nv = e->nv;
+    e->est.ne = e->ne;
+    e->est.repacks = e->repacks;
+    unsigned long long tops[2] = {0, 0};
+    if (e->loaded) {
+      CK(cudaMemcpyAsync(tops, e->arena_top.p, sizeof(tops), cudaMemcpyDeviceToHost, e->s));
+      CK(cudaStreamSynchronize(e->s));
+    }
+    e->est.slots = e->slots_total;
+    *out = e->est;
+  });
+}
+
+SGS_API int sgs_graph_export(sgs_engine *e, uint64_t *row, uint32_t *col, uint32_t *w, int mem) {
+  if (!e || !row || !col) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    if (!e->loaded) fail(SGS_ERR_STATE, "no graph loaded");
+    CK(cudaSetDevice(e->dev));
+    e->export_graph(row, col, w, mem);
+  });
+}
+
+SGS_API int sgs_query_summary(sgs_engine *e, int qid, uint64_t out[4]) {
+  if (!e || !out) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    e->summary(e->find(qid), out);
+  });
+}
+
+// splitmix64 output function and stream (same definitions as the device
+// generator in sgs_kernels.cuh).
+static inline uint64_t h_fin64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+static inline uint64_t h_mix64(uint64_t x) { return h_fin64(x + 0x9E3779B97F4A7C15ull); }
+static inline uint64_t h_stream(uint64_t key, uint64_t i) {
+  return h_fin64(key + (i + 1) * 0x9E3779B97F4A7C15ull);
+}
+
+SGS_API int sgs_gen_update_stream(uint32_t nv, const uint64_t *row, const uint32_t *col,
+                                  uint64_t seed, uint64_t n_ins, uint64_t n_del, uint32_t *ins_src,
+                                  uint32_t *ins_dst, uint32_t *del_src, uint32_t *del_dst) {
+  if (!row || (row[nv] && !col) || (n_ins && (!ins_src || !ins_dst)) ||
+      (n_del && (!del_src || !del_dst))) {
+    g_last_error = "null argument";
+    return SGS_ERR_INVALID;
+  }
+  return guarded([&] {
+    const uint64_t ne = row[nv];
+    if (n_del > ne) fail(SGS_ERR_INVALID, "more deletes than edges");
+    if (n_del) {
+      std::vector<uint64_t> bits(ne / 64 + 1, 0);
+      const uint64_t key = h_mix64(seed ^ 0x44454C45ull);
+      uint64_t got = 0, i = 0;
+      while (got < n_del) {
+        const uint64_t idx =
+            (uint64_t)(((unsigned __int128)h_stream(key, i++) * (unsigned __int128)ne) >> 64);
+        if (bits[idx >> 6] >> (idx & 63) & 1) continue;
+        bits[idx >> 6] |= 1ull << (idx & 63);
+        const uint32_t u = (uint32_t)(std::upper_bound(row, row + nv + 1, idx) - row) - 1;
+        del_src[got] = u;
+        del_dst[got] = col[idx];
+        ++got;
+      }
+    }
+    if (n_ins) {
+      if (nv < 2) fail(SGS_ERR_INVALID, "graph too small for inserts");
+      uint64_t tsz = 1;
+      while (tsz < 2 * n_ins + 16) tsz <<= 1;
+      std::vector<uint64_t> tab(tsz, ~0ull);
+      const uint64_t key = h_mix64(seed ^ 0x494E5345ull);
+      uint64_t got = 0, i = 0;
+      const uint64_t limit = 64 * n_ins + 1000000;
+      while (got < n_ins) {
+        if (i > limit) fail(SGS_ERR_INVALID, "graph too dense for the requested inserts");
+        const uint64_t h = h_stream(key, i++);
+        const uint32_t u = (uint32_t)(((h >> 32) * (uint64_t)nv) >> 32);
+        const uint32_t v = (uint32_t)(((h & 0xFFFFFFFFull) * (uint64_t)nv) >> 32);
+        if (u == v) continue;
+        if (std::binary_search(col + row[u], col + row[u + 1], v)) continue;
+        const uint64_t k = ((uint64_t)u << 32) | v;
+        uint64_t s = h_mix64(k) & (tsz - 1);
+        bool dup = false;
+        while (tab[s] != ~0ull) {
+          if (tab[s] == k) { dup = true; break; }
+          s = (s + 1) & (tsz - 1);
+        }
+        if (dup) continue;
+        tab[s] = k;
+        ins_src[got] = u;
+        ins_dst[got] = v;
+        ++got;
+      }
+    }
+  });
+}
+
+SGS_API void sgs_hash_weights(uint64_t wseed, uint64_t n, const uint32_t *src, const uint32_t *dst,
+                              uint32_t *w) {
+  if (!src || !dst || !w) return;
+  const uint64_t key = h_mix64(wseed ^ 0x57454947ull);
+  for (uint64_t i = 0; i < n; ++i)
+    w[i] = 1u + (uint32_t)(h_fin64(key ^ (((uint64_t)src[i] << 32) | dst[i])) >> 58);
+}
+
+SGS_API int sgs_kernel_timing(sgs_engine *e, int enable) {
+  if (!e) { g_last_error = "null engine"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    e->ktiming = enable != 0;
+    for (auto &k : e->kst) k = sgs_kernel_stats{};
+  });
+}
+
+SGS_API int sgs_get_kernel_stats(sgs_engine *e, int kind, sgs_kernel_stats *out) {
+  if (!e || !out) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  if (kind < 0 || kind >= SGS_K_COUNT) { g_last_error = "bad kernel kind"; return SGS_ERR_INVALID; }
+  *out = e->kst[kind];
+  return SGS_OK;
+}
+
+SGS_API int sgs_synchronize(sgs_engine *e) {
+  if (!e) { g_last_error = "null engine"; return SGS_ERR_INVALID; }
+  return guarded([&] { CK(cudaStreamSynchronize(e->s)); });
+}
+
+}  // extern "C"

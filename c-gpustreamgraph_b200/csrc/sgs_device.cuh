@@ -1,0 +1,140 @@
+// sgs_device.cuh -- device-side data layout and shared helpers of the
+// B200 streaming-graph engine.
+//
+// Layout in HBM (one engine = one dynamic graph + N registered queries):
+//
+//   per vertex (struct-of-arrays, 20 B/vertex):
+//     off[v]   u64  start of v's edge block in an arena; bit 63 selects the
+//                   pinned-host arena (out-of-HBM tier) instead of HBM
+//     slots[v] u32  used slots of the block (live edges + tombstones)
+//     live[v]  u32  live out-degree (what PageRank divides by)
+//     cap[v]   u32  capacity of the block (multiple of 4, block 16-B aligned)
+//   arenas (per tier): adj[] u32 destination ids, wgt[] u32 weights (only
+//     when weights are stored explicitly); a deleted edge becomes a tombstone
+//     (adj == SGS_TOMB) until its block is relocated or compacted.
+//
+//   per query: st[v] u64 packed (value << 32 | parent) for BFS/SSSP/CC; a
+//     single 64-bit atomic keeps value and parent consistent, which is what
+//     makes parent-tree invalidation after deletions exact.  PageRank keeps
+//     x[v], r[v] in FP64.
+//
+//   frontier (shared scratch): entries (vertex, edge-prefix) appended with
+//     one packed 64-bit atomicAdd per warp: count in the high 27 bits, the
+//     running sum of block sizes in the low 37 bits.  So the append itself
+//     produces the exclusive prefix sum of degrees, and it also writes, for
+//     every unit of UNIT edges, the first entry covering it.  The next round
+//     splits its edges into equal units with no scan kernel and no host sync.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sgs {
+
+constexpr uint32_t INF32 = 0xFFFFFFFFu;
+constexpr uint32_t SGS_TOMB = 0xFFFFFFFFu;   // tombstoned edge slot
+constexpr uint64_t HOST_BIT = 1ull << 63;
+constexpr uint64_t OFF_MASK = HOST_BIT - 1;
+constexpr int CNT_SHIFT = 37;                 // packed frontier counter
+constexpr uint64_t EDGE_MASK = (1ull << CNT_SHIFT) - 1;
+constexpr uint32_t UNIT = 2048;               // edges per load-balanced unit
+constexpr int RELAX_THREADS = 256;
+
+enum Algo : int { A_BFS = 0, A_SSSP = 1, A_CC = 2, A_PR = 3 };
+enum WMode : int { W_EXPLICIT = 0, W_SYNTH = 1, W_UNIT = 2 };
+
+struct GraphView {
+  uint32_t nv;
+  uint64_t *off;
+  uint32_t *slots;
+  uint32_t *live;
+  uint32_t *cap;
+  uint32_t *adj_d;   // HBM arena
+  uint32_t *wgt_d;
+  uint32_t *adj_h;   // pinned, mapped host arena (may be null)
+  uint32_t *wgt_h;
+  int wmode;
+};
+
+struct FrontierView {
+  uint32_t *vtx;       // [cap] vertex of each entry
+  uint64_t *ebase;     // [cap] exclusive prefix of block sizes
+  uint32_t *ustart;    // [ucap] first entry of each UNIT-edge unit
+  uint64_t *counter;   // packed (count << 37 | edges)
+  uint32_t ucap;
+};
+
+__device__ __forceinline__ uint64_t pack(uint32_t val, uint32_t par) {
+  return ((uint64_t)val << 32) | par;
+}
+__device__ __forceinline__ uint32_t val_of(uint64_t s) { return (uint32_t)(s >> 32); }
+__device__ __forceinline__ uint32_t par_of(uint64_t s) { return (uint32_t)s; }
+
+__device__ __forceinline__ const uint32_t *adj_ptr(const GraphView &g, uint64_t o) {
+  return ((o & HOST_BIT) ? g.adj_h : g.adj_d) + (o & OFF_MASK);
+}
+__device__ __forceinline__ const uint32_t *wgt_ptr(const GraphView &g, uint64_t o) {
+  return ((o & HOST_BIT) ? g.wgt_h : g.wgt_d) + (o & OFF_MASK);
+}
+__device__ __forceinline__ uint32_t *adj_wptr(const GraphView &g, uint64_t o) {
+  return ((o & HOST_BIT) ? g.adj_h : g.adj_d) + (o & OFF_MASK);
+}
+__device__ __forceinline__ uint32_t *wgt_wptr(const GraphView &g, uint64_t o) {
+  return ((o & HOST_BIT) ? g.wgt_h : g.wgt_d) + (o & OFF_MASK);
+}
+
+// Weight of slot j of u's block.  Synthesized mode reproduces the
+// reference's per-edge (src+dst)%128+1 (push_functor.h:306).
+__device__ __forceinline__ uint32_t edge_weight(const GraphView &g, uint64_t o,
+                                                uint32_t j, uint32_t u,
+                                                uint32_t dst) {
+  if (g.wmode == W_EXPLICIT) return wgt_ptr(g, o)[j];
+  if (g.wmode == W_SYNTH) return (u + dst) % 128u + 1u;
+  return 1u;
+}
+
+// Warp-aggregated append of (v, d) into a frontier.  Must be called by all 32
+// lanes of a converged warp; `want` selects the lanes that append.  One packed
+// 64-bit atomicAdd per warp reserves the slots and the edge range together.
+__device__ __forceinline__ void frontier_append(const FrontierView &f, bool want,
+                                                uint32_t v, uint32_t d,
+                                                uint32_t *aux = nullptr,
+                                                uint32_t aux_val = 0) {
+  const unsigned full = 0xFFFFFFFFu;
+  unsigned m = __ballot_sync(full, want);
+  if (!m) return;
+  const int lane = threadIdx.x & 31;
+  uint64_t inc = want ? ((1ull << CNT_SHIFT) | (uint64_t)d) : 0ull;
+  // inclusive warp scan of inc
+  uint64_t x = inc;
+#pragma unroll
+  for (int s = 1; s < 32; s <<= 1) {
+    uint64_t y = __shfl_up_sync(full, x, s);
+    if (lane >= s) x += y;
+  }
+  uint64_t total = __shfl_sync(full, x, 31);
+  uint64_t base = 0;
+  if (lane == 31) base = atomicAdd((unsigned long long *)f.counter, (unsigned long long)total);
+  base = __shfl_sync(full, base, 31);
+  if (want) {
+    uint64_t excl = x - inc;
+    uint32_t slot = (uint32_t)((base >> CNT_SHIFT) + (excl >> CNT_SHIFT));
+    uint64_t eb = (base & EDGE_MASK) + (excl & EDGE_MASK);
+    f.vtx[slot] = v;
+    f.ebase[slot] = eb;
+    if (aux) aux[slot] = aux_val;
+    if (d) {
+      uint64_t u0 = (eb + UNIT - 1) / UNIT, u1 = (eb + d - 1) / UNIT;
+      for (uint64_t u = u0; u <= u1 && u < f.ucap; ++u) f.ustart[u] = slot;
+    }
+  }
+}
+
+// Block-wide helpers --------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, s);
+  return v;
+}
+
+}  // namespace sgs

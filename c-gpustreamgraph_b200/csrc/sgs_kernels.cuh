@@ -1,0 +1,916 @@
+// sgs_kernels.cuh -- sm_100a kernels of the streaming-graph engine.
+//
+// Reference behaviour each kernel re-implements (paths relative to the
+// reference project):
+//   seg_map + RelaxOp     <- kernel::SyncPushDDBDelta / RelaxCTADB /
+//                            CTAWorkSchedulerNew / PushFunctorDB
+//                            (variants/driver.cuh:1893-1935,
+//                             variants/sync_push_dd.cuh:170-268,
+//                             groute/device/cta_scheduler_hybrid.cuh:59-245,
+//                             variants/push_functor.h:252-321)
+//   frontier_append       <- RebuildWorklist* + dev::Queue::append
+//                            (driver.cuh:654-909, groute/device/queue.cuh:84-88)
+//   InvalidateOp, k_seed_deleted
+//                         <- reset_del_edges + SyncPushDDB_del
+//                            (driver.cuh:398-430, :1985-2031,
+//                             hybrid_sssp.cu:154-167)
+//   k_dense_frontier      <- RebuildWorklist_AllVertices + SyncPushDDBAll
+//                            (driver.cuh:704-720, :1727-1761)
+//   PR absorb/push/amend  <- hybrid_pr.cu:66-122 CombineValueBuffer /
+//                            CombineValueBufferAmend / AccumulateBuffer and
+//                            SyncPushDDBAmend (driver.cuh:1770-1804)
+//   batch-apply kernels   <- host::PMAGraph::insert / del_edge
+//                            (groute/graphs/csr_graph.cuh:658-811), done on
+//                            the device as sort + tombstone + append/relocate
+#pragma once
+#include <cub/block/block_reduce.cuh>
+
+#include "sgs_device.cuh"
+
+namespace sgs {
+
+// ---------------------------------------------------------------------------
+// Generic load-balanced segmented map.
+//
+// The input frontier is a list of entries (vertex v, ebase) whose ranges
+// [ebase_s, ebase_{s+1}) tile [0, T).  Units of UNIT consecutive positions are
+// spread over a fixed grid; a CTA stages up to CHUNK entries of its unit in
+// shared memory (the per-entry payload is loaded once, coalesced) and then
+// its threads walk consecutive positions, so consecutive lanes touch
+// consecutive slots of the same block (coalesced 128-B lines).  Every thread
+// of a CTA runs the same trip count, so warp-aggregated appends always see
+// full warps.
+// ---------------------------------------------------------------------------
+constexpr int CHUNK = 256;
+
+template <class Op>
+__global__ void __launch_bounds__(RELAX_THREADS)
+    seg_map(FrontierView in, FrontierView out, Op op, unsigned long long *edge_stat) {
+  using P = typename Op::Payload;
+  __shared__ uint64_t s_eb[CHUNK + 1];
+  __shared__ P s_pay[CHUNK];
+  __shared__ uint32_t s_vtx[CHUNK];
+  const uint64_t packed = __ldcg((const unsigned long long *)in.counter);
+  const uint32_t n = (uint32_t)(packed >> CNT_SHIFT);
+  const uint64_t T = packed & EDGE_MASK;
+  if (n == 0 || T == 0) return;
+  const uint64_t nunits = (T + UNIT - 1) / UNIT;
+  uint64_t counted = 0;
+  for (uint64_t unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
+    const uint64_t E0 = unit * UNIT;
+    const uint64_t E1 = min(E0 + (uint64_t)UNIT, T);
+    uint32_t s = __ldcg(&in.ustart[unit]);
+    for (;;) {
+      __syncthreads();  // previous chunk fully consumed
+      {
+        const uint32_t t = threadIdx.x;
+        const uint32_t idx = s + t;
+        uint64_t eb = idx < n ? __ldcg((const unsigned long long *)&in.ebase[idx]) : T;
+        s_eb[t] = eb;
+        if (t == 0) {
+          const uint32_t j = s + CHUNK;
+          s_eb[CHUNK] = j < n ? __ldcg((const unsigned long long *)&in.ebase[j]) : T;
+        }
+        if (idx < n && eb < E1) {
+          const uint32_t v = __ldcg(&in.vtx[idx]);
+          s_vtx[t] = v;
+          s_pay[t] = op.load(idx, v);
+        }
+      }
+      __syncthreads();
+      const uint64_t lo = max(E0, s_eb[0]);
+      const uint64_t hi = min(E1, s_eb[CHUNK]);
+      for (uint64_t base = lo; base < hi; base += RELAX_THREADS) {
+        const uint64_t e = base + threadIdx.x;
+        const bool valid = e < hi;
+        bool app = false;
+        uint32_t av = 0, ad = 0;
+        if (valid) {
+          // largest i with s_eb[i] <= e
+          int l = 0, r = CHUNK - 1;
+          while (l < r) {
+            int m = (l + r + 1) >> 1;
+            if (s_eb[m] <= e) l = m;
+            else r = m - 1;
+          }
+          const uint32_t j = (uint32_t)(e - s_eb[l]);
+          counted += op.visit(s_vtx[l], s_pay[l], j, app, av, ad);
+        }
+        if (Op::kAppends) frontier_append(out, app, av, ad);
+      }
+      if (s_eb[CHUNK] >= E1 || s + CHUNK >= n) break;
+      s += CHUNK;
+    }
+  }
+  if (edge_stat) {
+    typedef cub::BlockReduce<unsigned long long, RELAX_THREADS> BR;
+    __shared__ typename BR::TempStorage tmp;
+    unsigned long long tot = BR(tmp).Sum((unsigned long long)counted);
+    if (threadIdx.x == 0 && tot) atomicAdd(edge_stat, tot);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Ops
+// ---------------------------------------------------------------------------
+struct SrcPay {
+  uint64_t off;
+  uint32_t val;
+  uint32_t pad;
+};
+
+// BFS / SSSP relaxation on packed (value,parent): atomicMin keeps value and
+// parent consistent; the parent is the smallest-id tight predecessor at the
+// fixed point (deterministic).  A vertex is re-activated only when its value
+// strictly drops (hybrid_sssp.cu:97-118 semantics).
+struct RelaxMinOp {
+  static constexpr bool kAppends = true;
+  using Payload = SrcPay;
+  GraphView g;
+  unsigned long long *st;
+  uint32_t *mark;
+  uint32_t stamp;
+  int unit_weight;  // BFS
+  __device__ __forceinline__ Payload load(uint32_t, uint32_t v) const {
+    SrcPay p;
+    p.off = g.off[v];
+    p.val = (uint32_t)(__ldcg(&st[v]) >> 32);
+    p.pad = 0;
+    return p;
+  }
+  __device__ __forceinline__ uint32_t visit(uint32_t u, const Payload &p, uint32_t j,
+                                            bool &app, uint32_t &av,
+                                            uint32_t &ad) const {
+    const uint32_t dst = adj_ptr(g, p.off)[j];
+    if (dst == SGS_TOMB) return 0;
+    if (p.val == INF32) return 1;
+    const uint32_t w = unit_weight ? 1u : edge_weight(g, p.off, j, u, dst);
+    const uint64_t nd = (uint64_t)p.val + w;
+    if (nd >= INF32) return 1;
+    const unsigned long long np = ((unsigned long long)nd << 32) | u;
+    if (np >= __ldcg(&st[dst])) return 1;
+    const unsigned long long old = atomicMin(&st[dst], np);
+    if (nd < (old >> 32)) {
+      if (__ldcg(&mark[dst]) != stamp && atomicExch(&mark[dst], stamp) != stamp) {
+        const uint32_t d = g.slots[dst];
+        if (d) { app = true; av = dst; ad = d; }
+      }
+    }
+    return 1;
+  }
+};
+
+// Directed min-label propagation (hybrid_cc.cu:96-110).  Only a strictly
+// smaller label is accepted (CAS), so the parent of v is the vertex that
+// delivered v's current label first; parent chains are then acyclic.
+struct RelaxLabelOp {
+  static constexpr bool kAppends = true;
+  using Payload = SrcPay;
+  GraphView g;
+  unsigned long long *st;
+  uint32_t *mark;
+  uint32_t stamp;
+  __device__ __forceinline__ Payload load(uint32_t, uint32_t v) const {
+    SrcPay p;
+    p.off = g.off[v];
+    p.val = (uint32_t)(__ldcg(&st[v]) >> 32);
+    p.pad = 0;
+    return p;
+  }
+  __device__ __forceinline__ uint32_t visit(uint32_t u, const Payload &p, uint32_t j,
+                                            bool &app, uint32_t &av,
+                                            uint32_t &ad) const {
+    const uint32_t dst = adj_ptr(g, p.off)[j];
+    if (dst == SGS_TOMB) return 0;
+    const uint32_t L = p.val;
+    unsigned long long cur = __ldcg(&st[dst]);
+    while ((uint32_t)(cur >> 32) > L) {
+      const unsigned long long nw = ((unsigned long long)L << 32) | u;
+      const unsigned long long old = atomicCAS(&st[dst], cur, nw);
+      if (old == cur) {
+        if (__ldcg(&mark[dst]) != stamp && atomicExch(&mark[dst], stamp) != stamp) {
+          const uint32_t d = g.slots[dst];
+          if (d) { app = true; av = dst; ad = d; }
+        }
+        break;
+      }
+      cur = old;
+    }
+    return 1;
+  }
+};
+
+// Parent-tree invalidation: a child whose parent is an invalidated vertex is
+// reset (to INF, or to its own id for CC) exactly once (CAS on the packed
+// word), which also makes the appended frontier duplicate-free.
+struct InvalidateOp {
+  static constexpr bool kAppends = true;
+  using Payload = SrcPay;
+  GraphView g;
+  unsigned long long *st;
+  int cc;
+  unsigned long long *n_inval;
+  __device__ __forceinline__ Payload load(uint32_t, uint32_t v) const {
+    SrcPay p;
+    p.off = g.off[v];
+    p.val = 0;
+    p.pad = 0;
+    return p;
+  }
+  __device__ __forceinline__ uint32_t visit(uint32_t u, const Payload &p, uint32_t j,
+                                            bool &app, uint32_t &av,
+                                            uint32_t &ad) const {
+    const uint32_t dst = adj_ptr(g, p.off)[j];
+    if (dst == SGS_TOMB) return 0;
+    const unsigned long long cur = __ldcg(&st[dst]);
+    if ((uint32_t)cur != u) return 1;
+    const unsigned long long rst =
+        cc ? (((unsigned long long)dst << 32) | INF32) : ~0ull;
+    if (atomicCAS(&st[dst], cur, rst) == cur) {
+      atomicAdd(n_inval, 1ull);
+      const uint32_t d = g.slots[dst];
+      if (d) { app = true; av = dst; ad = d; }
+    }
+    return 1;
+  }
+};
+
+// PageRank push of a per-source scalar (absorbed residual or +-alpha*x/deg).
+struct PrPay {
+  uint64_t off;
+  double c;
+};
+struct PrPushOp {
+  static constexpr bool kAppends = false;
+  using Payload = PrPay;
+  GraphView g;
+  const double *pv;   // per-vertex push value (alpha * r / outdeg)
+  double *r;
+  __device__ __forceinline__ Payload load(uint32_t, uint32_t v) const {
+    PrPay p;
+    p.off = g.off[v];
+    p.c = pv[v];
+    return p;
+  }
+  __device__ __forceinline__ uint32_t visit(uint32_t, const Payload &p, uint32_t j,
+                                            bool &, uint32_t &, uint32_t &) const {
+    const uint32_t dst = adj_ptr(g, p.off)[j];
+    if (dst == SGS_TOMB) return 0;
+    if (p.c != 0.0) atomicAdd(&r[dst], p.c);
+    return 1;
+  }
+};
+// Cancel (sign=-1, old graph) / compensate (sign=+1, new graph) of
+// hybrid_pr.cu:88-106, restricted to sources whose out-edges changed.
+struct PrAmendOp {
+  static constexpr bool kAppends = false;
+  using Payload = PrPay;
+  GraphView g;
+  const double *x;
+  double *r;
+  double scale;  // sign * alpha
+  __device__ __forceinline__ Payload load(uint32_t, uint32_t v) const {
+    PrPay p;
+    p.off = g.off[v];
+    const uint32_t l = g.live[v];
+    p.c = l ? scale * x[v] / (double)l : 0.0;
+    return p;
+  }
+  __device__ __forceinline__ uint32_t visit(uint32_t, const Payload &p, uint32_t j,
+                                            bool &, uint32_t &, uint32_t &) const {
+    const uint32_t dst = adj_ptr(g, p.off)[j];
+    if (dst == SGS_TOMB) return 0;
+    if (p.c != 0.0) atomicAdd(&r[dst], p.c);
+    return 1;
+  }
+};
+
+// Tombstone every slot of u whose destination is in u's sorted delete group
+// (PMAGraph::del_edge removes every matching entry).
+struct GroupPay {
+  uint64_t off;
+  uint32_t gs, ge;
+};
+struct TombOp {
+  static constexpr bool kAppends = false;
+  using Payload = GroupPay;
+  GraphView g;
+  const uint64_t *keys;   // sorted delete keys (src<<32|dst)
+  const uint32_t *gstart; // per entry
+  uint32_t nkeys;
+  __device__ __forceinline__ Payload load(uint32_t slot, uint32_t v) const {
+    GroupPay p;
+    p.off = g.off[v];
+    p.gs = gstart[slot];
+    // end of the group: first key with a larger source
+    const uint64_t lim = ((uint64_t)v + 1) << 32;
+    uint32_t l = p.gs, r = nkeys;
+    while (l < r) {
+      uint32_t m = (l + r) >> 1;
+      if (keys[m] < lim) l = m + 1;
+      else r = m;
+    }
+    p.ge = l;
+    return p;
+  }
+  __device__ __forceinline__ uint32_t visit(uint32_t u, const Payload &p, uint32_t j,
+                                            bool &, uint32_t &, uint32_t &) const {
+    uint32_t *a = adj_wptr(g, p.off);
+    const uint32_t dst = a[j];
+    if (dst == SGS_TOMB) return 0;
+    const uint64_t k = ((uint64_t)u << 32) | dst;
+    uint32_t l = p.gs, r = p.ge;
+    while (l < r) {
+      uint32_t m = (l + r) >> 1;
+      if (keys[m] < k) l = m + 1;
+      else r = m;
+    }
+    if (l < p.ge && keys[l] == k) {
+      a[j] = SGS_TOMB;
+      atomicSub(&g.live[u], 1u);
+      return 1;
+    }
+    return 0;
+  }
+};
+
+// Copy of a whole block (slots as they are, tombstones included) from an old
+// location to the vertex's current block; used by relocation and repacking.
+struct CopyPay {
+  uint64_t from;
+  uint64_t to;
+};
+struct CopyBlockOp {
+  static constexpr bool kAppends = false;
+  using Payload = CopyPay;
+  GraphView g;
+  const uint64_t *from_off;  // per vertex: old offset (tier bit included)
+  const uint64_t *to_off;    // per vertex: new offset
+  uint32_t *src_adj_d, *src_wgt_d, *src_adj_h, *src_wgt_h;  // source arenas
+  __device__ __forceinline__ Payload load(uint32_t, uint32_t v) const {
+    CopyPay p;
+    p.from = from_off[v];
+    p.to = to_off[v];
+    return p;
+  }
+  __device__ __forceinline__ uint32_t visit(uint32_t, const Payload &p, uint32_t j,
+                                            bool &, uint32_t &, uint32_t &) const {
+    const uint64_t fo = p.from & OFF_MASK;
+    const bool fh = (p.from & HOST_BIT) != 0;
+    const uint32_t a = (fh ? src_adj_h : src_adj_d)[fo + j];
+    adj_wptr(g, p.to)[j] = a;
+    if (g.wmode == W_EXPLICIT) wgt_wptr(g, p.to)[j] = (fh ? src_wgt_h : src_wgt_d)[fo + j];
+    return 0;
+  }
+};
+
+// Copy an input CSR (device arrays) into the arena blocks.
+struct LoadCsrOp {
+  static constexpr bool kAppends = false;
+  using Payload = CopyPay;
+  GraphView g;
+  const uint64_t *row;
+  const uint32_t *col;
+  const uint32_t *w;   // null unless weights are explicit
+  __device__ __forceinline__ Payload load(uint32_t, uint32_t v) const {
+    CopyPay p;
+    p.from = row[v];
+    p.to = g.off[v];
+    return p;
+  }
+  __device__ __forceinline__ uint32_t visit(uint32_t, const Payload &p, uint32_t j,
+                                            bool &, uint32_t &, uint32_t &) const {
+    adj_wptr(g, p.to)[j] = col[p.from + j];
+    if (w) wgt_wptr(g, p.to)[j] = w[p.from + j];
+    return 0;
+  }
+};
+
+// Export blocks (live edges only) into a CSR whose row offsets are given.  A
+// block without tombstones keeps its order; otherwise live slots are placed
+// through a per-vertex counter (order not kept).
+struct ExportPay {
+  uint64_t from;
+  uint64_t to;
+  uint32_t dense;
+  uint32_t pad;
+};
+struct ExportOp {
+  static constexpr bool kAppends = false;
+  using Payload = ExportPay;
+  GraphView g;
+  const uint64_t *row_out;
+  uint32_t *col_out;
+  uint32_t *w_out;
+  uint32_t *fill;  // per-vertex fill counter (zeroed)
+  __device__ __forceinline__ Payload load(uint32_t, uint32_t v) const {
+    ExportPay p;
+    p.from = g.off[v];
+    p.to = row_out[v];
+    p.dense = g.slots[v] == g.live[v];
+    p.pad = 0;
+    return p;
+  }
+  __device__ __forceinline__ uint32_t visit(uint32_t u, const Payload &p, uint32_t j,
+                                            bool &, uint32_t &, uint32_t &) const {
+    const uint32_t dst = adj_ptr(g, p.from)[j];
+    if (dst == SGS_TOMB) return 0;
+    const uint32_t k = p.dense ? j : atomicAdd(&fill[u], 1u);
+    col_out[p.to + k] = dst;
+    if (w_out) w_out[p.to + k] = edge_weight(g, p.from, j, u, dst);
+    return 1;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Frontier builders (all lanes of every warp reach frontier_append)
+// ---------------------------------------------------------------------------
+__global__ void k_append_one(FrontierView out, uint32_t v, uint32_t d) {
+  if (threadIdx.x >= 32) return;
+  frontier_append(out, threadIdx.x == 0 && d > 0, v, d);
+}
+
+// Every vertex whose value is finite (all vertices for CC) and whose block is
+// non-empty: the all-vertices re-push after a batch (SyncPushDDBAll).
+__global__ void k_dense_frontier(GraphView g, const unsigned long long *st,
+                                 int mode /*0: st finite, 1: all, 2: slots only*/,
+                                 FrontierView out) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < g.nv; b += stride) {
+    const uint64_t v = b + threadIdx.x;
+    bool want = false;
+    uint32_t d = 0;
+    if (v < g.nv) {
+      d = g.slots[v];
+      want = d > 0;
+      if (want && mode == 0) want = (uint32_t)(__ldcg(&st[v]) >> 32) != INF32;
+    }
+    frontier_append(out, want, (uint32_t)v, d);
+  }
+}
+
+// Seeds of the deletion phase: deleted (u,v) with parent[v]==u resets v
+// (reset_del_edges, driver.cuh:398-430).
+__global__ void k_seed_deleted(GraphView g, unsigned long long *st, int cc,
+                               const uint64_t *keys, uint32_t n,
+                               unsigned long long *n_inval, FrontierView out) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < n; b += stride) {
+    const uint64_t i = b + threadIdx.x;
+    bool want = false;
+    uint32_t v = 0, d = 0;
+    if (i < n) {
+      const uint64_t k = keys[i];
+      const uint32_t u = (uint32_t)(k >> 32);
+      v = (uint32_t)k;
+      const unsigned long long cur = __ldcg(&st[v]);
+      if ((uint32_t)cur == u) {
+        const unsigned long long rst = cc ? (((unsigned long long)v << 32) | INF32) : ~0ull;
+        if (atomicCAS(&st[v], cur, rst) == cur) {
+          atomicAdd(n_inval, 1ull);
+          d = g.slots[v];
+          want = d > 0;
+        }
+      }
+    }
+    frontier_append(out, want, v, d);
+  }
+}
+
+// Relax only the inserted edges (no invalidation happened): the insert-only
+// fast path of the add phase.
+__global__ void k_relax_inserted(GraphView g, unsigned long long *st, int algo,
+                                 const uint64_t *keys, const uint32_t *w,
+                                 const uint32_t *n_ptr, uint32_t *mark,
+                                 uint32_t stamp, FrontierView out,
+                                 unsigned long long *edge_stat) {
+  const uint32_t n = *n_ptr;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t counted = 0;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < n; b += stride) {
+    const uint64_t i = b + threadIdx.x;
+    bool want = false;
+    uint32_t v = 0, d = 0;
+    if (i < n) {
+      const uint64_t k = keys[i];
+      const uint32_t u = (uint32_t)(k >> 32);
+      v = (uint32_t)k;
+      ++counted;
+      const unsigned long long su = __ldcg(&st[u]);
+      const uint32_t du = (uint32_t)(su >> 32);
+      bool improved = false;
+      if (algo == A_CC) {
+        unsigned long long cur = __ldcg(&st[v]);
+        while ((uint32_t)(cur >> 32) > du) {
+          const unsigned long long nw = ((unsigned long long)du << 32) | u;
+          const unsigned long long old = atomicCAS(&st[v], cur, nw);
+          if (old == cur) { improved = true; break; }
+          cur = old;
+        }
+      } else if (du != INF32) {
+        uint32_t wt = 1;
+        if (algo == A_SSSP)
+          wt = g.wmode == W_EXPLICIT ? w[i] : g.wmode == W_SYNTH ? (u + v) % 128u + 1u : 1u;
+        const uint64_t nd = (uint64_t)du + wt;
+        if (nd < INF32) {
+          const unsigned long long np = (nd << 32) | u;
+          const unsigned long long old = atomicMin(&st[v], np);
+          improved = nd < (old >> 32);
+        }
+      }
+      if (improved && __ldcg(&mark[v]) != stamp && atomicExch(&mark[v], stamp) != stamp) {
+        d = g.slots[v];
+        want = d > 0;
+      }
+    }
+    frontier_append(out, want, v, d);
+  }
+  if (edge_stat && counted) atomicAdd(edge_stat, (unsigned long long)counted);
+}
+
+// ---------------------------------------------------------------------------
+// Per-query state init (InitGraph, driver.cuh:200-229)
+// ---------------------------------------------------------------------------
+__global__ void k_init_state(unsigned long long *st, uint32_t nv, int algo,
+                             uint32_t source) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride) {
+    unsigned long long s;
+    if (algo == A_CC) s = ((unsigned long long)v << 32) | INF32;
+    else s = (v == source) ? (unsigned long long)INF32 : ~0ull;
+    st[v] = s;
+  }
+}
+
+__global__ void k_split_state(const unsigned long long *st, uint32_t nv,
+                              uint32_t *val, uint32_t *par) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride) {
+    const unsigned long long s = st[v];
+    if (val) val[v] = (uint32_t)(s >> 32);
+    if (par) par[v] = (uint32_t)s;
+  }
+}
+
+// PageRank: value 0, buffer (residual) 1-alpha (hybrid_pr.cu:43-52).
+__global__ void k_pr_init(double *x, double *r, uint32_t nv, double r0) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride) {
+    x[v] = 0.0;
+    r[v] = r0;
+  }
+}
+
+// Absorb: value += residual, residual = 0, push value alpha*res/outdeg
+// (CombineValueBuffer, hybrid_pr.cu:66-85).  Accumulates the L1 norm of the
+// absorbed residual into *l1.
+__global__ void k_pr_absorb(GraphView g, double *x, double *r, double *pv,
+                            double alpha, double *l1) {
+  double acc = 0.0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < g.nv; v += stride) {
+    const double rv = r[v];
+    double p = 0.0;
+    if (rv != 0.0) {
+      r[v] = 0.0;
+      x[v] += rv;
+      acc += fabs(rv);
+      const uint32_t l = g.live[v];
+      if (l) p = alpha * rv / (double)l;
+    }
+    pv[v] = p;
+  }
+  typedef cub::BlockReduce<double, RELAX_THREADS> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const double tot = BR(tmp).Sum(acc);
+  if (threadIdx.x == 0 && tot != 0.0) atomicAdd(l1, tot);
+}
+
+// ---------------------------------------------------------------------------
+// Batch apply
+// ---------------------------------------------------------------------------
+__global__ void k_make_keys(const uint32_t *src, const uint32_t *dst, uint64_t n,
+                            uint32_t nv, uint64_t *keys, const uint32_t *w,
+                            int check_w, unsigned int *err) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t u = src[i], v = dst[i];
+    if (u >= nv || v >= nv) atomicOr(err, 1u);
+    if (check_w && w && w[i] == 0) atomicOr(err, 2u);
+    keys[i] = ((uint64_t)u << 32) | v;
+  }
+}
+
+__device__ __forceinline__ bool sorted_has(const uint64_t *a, uint32_t n, uint64_t k) {
+  uint32_t l = 0, r = n;
+  while (l < r) {
+    uint32_t m = (l + r) >> 1;
+    if (a[m] < k) l = m + 1;
+    else r = m;
+  }
+  return l < n && a[l] == k;
+}
+
+// flag[i] = insert i survives the batch's deletes (insert-then-delete order of
+// framework.cuh:1011-1012).
+__global__ void k_filter_inserts(const uint64_t *ins, uint32_t n_ins,
+                                 const uint64_t *del, uint32_t n_del,
+                                 unsigned char *flag) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_ins; i += stride)
+    flag[i] = n_del ? !sorted_has(del, n_del, ins[i]) : 1;
+}
+
+// One entry per distinct source of a sorted key list (group heads); aux =
+// group start.  With `mark`, sources already marked with `stamp` are skipped,
+// which builds the union of the sources of several lists.
+__global__ void k_group_heads(GraphView g, const uint64_t *keys,
+                              const uint32_t *n_ptr, uint32_t n_fixed,
+                              uint32_t *gstart, uint32_t *mark, uint32_t stamp,
+                              FrontierView out) {
+  const uint32_t n = n_ptr ? *n_ptr : n_fixed;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < n; b += stride) {
+    const uint64_t i = b + threadIdx.x;
+    bool want = false;
+    uint32_t u = 0, d = 0;
+    if (i < n) {
+      u = (uint32_t)(keys[i] >> 32);
+      const bool head = i == 0 || (uint32_t)(keys[i - 1] >> 32) != u;
+      if (head) {
+        d = g.slots[u];
+        want = d > 0;
+        if (want && mark) want = atomicExch(&mark[u], stamp) != stamp;
+      }
+    }
+    frontier_append(out, want, u, d, gstart, (uint32_t)i);
+  }
+}
+
+// Insert phase 1 (one thread per distinct source of the kept, sorted inserts):
+// append in place when the block has room, else relocate the block to a new
+// region of the same tier (capacity grows 1.5x) and queue the copy of the old
+// slots.  Mirrors PMAGraph::insert's "append at index+degree" and its
+// resize-on-overflow, without shifting neighbours.
+struct InsertCtx {
+  unsigned long long *arena_top;   // [2] per tier
+  uint64_t arena_cap[2];
+  unsigned int *err;
+  uint64_t *wbase;                 // per vertex: write position of its inserts
+  // relocation list
+  uint32_t *rl_vtx;
+  uint64_t *rl_from;
+  uint64_t *rl_to;
+  uint32_t *rl_len;
+  unsigned int *rl_count;
+};
+
+__device__ __forceinline__ uint32_t grow_cap(uint32_t need) {
+  uint64_t c = (uint64_t)need + (need >> 1) + 4;
+  c = (c + 3) & ~3ull;
+  return (uint32_t)min(c, (uint64_t)0xFFFFFFF0u);
+}
+
+__global__ void k_insert_plan(GraphView g, const uint64_t *keys, const uint32_t *n_ptr,
+                              InsertCtx c, int dry, unsigned long long *demand) {
+  const uint32_t n = *n_ptr;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t u = (uint32_t)(keys[i] >> 32);
+    if (i > 0 && (uint32_t)(keys[i - 1] >> 32) == u) continue;
+    // group end
+    const uint64_t lim = ((uint64_t)u + 1) << 32;
+    uint32_t l = (uint32_t)i, r = n;
+    while (l < r) {
+      uint32_t m = (l + r) >> 1;
+      if (keys[m] < lim) l = m + 1;
+      else r = m;
+    }
+    const uint32_t k = l - (uint32_t)i;
+    const uint32_t sl = g.slots[u], cp = g.cap[u];
+    const uint64_t need = (uint64_t)sl + k;
+    const uint64_t o = g.off[u];
+    const int tier = (o & HOST_BIT) ? 1 : 0;
+    if (need <= cp) {
+      if (!dry) {
+        c.wbase[u] = o + sl;
+        g.slots[u] = (uint32_t)need;
+        g.live[u] += k;
+      }
+      continue;
+    }
+    if (need > 0xFFFFFFF0ull) { atomicOr(c.err, 4u); continue; }
+    const uint32_t nc = grow_cap((uint32_t)need);
+    if (dry) { atomicAdd(&demand[tier], (unsigned long long)nc); continue; }
+    const unsigned long long pos = atomicAdd(&c.arena_top[tier], (unsigned long long)nc);
+    if (pos + nc > c.arena_cap[tier]) { atomicOr(c.err, 8u); continue; }
+    const uint64_t no = pos | (tier ? HOST_BIT : 0);
+    if (sl) {
+      const unsigned int q = atomicAdd(c.rl_count, 1u);
+      c.rl_vtx[q] = u;
+      c.rl_from[q] = o;
+      c.rl_to[q] = no;
+      c.rl_len[q] = sl;
+    }
+    c.wbase[u] = no + sl;
+    g.off[u] = no;
+    g.cap[u] = nc;
+    g.slots[u] = (uint32_t)need;
+    g.live[u] += k;
+  }
+}
+
+// Insert phase 2: one thread per kept insert writes (dst, w) at its rank
+// within its source's group.
+__global__ void k_insert_write(GraphView g, const uint64_t *keys, const uint32_t *w,
+                               const uint32_t *n_ptr, const uint64_t *wbase) {
+  const uint32_t n = *n_ptr;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint64_t k = keys[i];
+    const uint32_t u = (uint32_t)(k >> 32), v = (uint32_t)k;
+    const uint64_t lo_key = (uint64_t)u << 32;
+    uint32_t l = 0, r = (uint32_t)i;
+    while (l < r) {
+      uint32_t m = (l + r) >> 1;
+      if (keys[m] < lo_key) l = m + 1;
+      else r = m;
+    }
+    const uint64_t pos = wbase[u] + (i - l);
+    adj_wptr(g, pos)[0] = v;
+    if (g.wmode == W_EXPLICIT) wgt_wptr(g, pos)[0] = w[i];
+  }
+}
+
+// Relocation list -> frontier of copy entries; the entry's vertex field holds
+// the relocation list index.
+__global__ void k_reloc_frontier(const unsigned int *rl_count, const uint32_t *rl_len,
+                                 FrontierView out) {
+  const uint32_t n = *rl_count;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < n; b += stride) {
+    const uint64_t i = b + threadIdx.x;
+    const uint32_t d = i < n ? rl_len[i] : 0u;
+    frontier_append(out, d > 0, (uint32_t)i, d);
+  }
+}
+
+// Copy op over relocation entries: vertex field = relocation list index.
+struct RelocCopyOp {
+  static constexpr bool kAppends = false;
+  using Payload = CopyPay;
+  GraphView g;
+  const uint64_t *rl_from;
+  const uint64_t *rl_to;
+  __device__ __forceinline__ Payload load(uint32_t, uint32_t q) const {
+    CopyPay p;
+    p.from = rl_from[q];
+    p.to = rl_to[q];
+    return p;
+  }
+  __device__ __forceinline__ uint32_t visit(uint32_t, const Payload &p, uint32_t j,
+                                            bool &, uint32_t &, uint32_t &) const {
+    adj_wptr(g, p.to)[j] = adj_ptr(g, p.from)[j];
+    if (g.wmode == W_EXPLICIT) wgt_wptr(g, p.to)[j] = wgt_ptr(g, p.from)[j];
+    return 0;
+  }
+};
+
+// Per-vertex block layout for a fresh arena: capacity with slack.
+__global__ void k_layout_caps(const uint32_t *deg, uint32_t nv, uint32_t slack_div,
+                              uint32_t *cap) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride) {
+    const uint32_t d = deg[v];
+    uint64_t c = d ? (uint64_t)d + (slack_div ? d / slack_div : 0) + 2 : 0;
+    c = (c + 3) & ~3ull;
+    cap[v] = (uint32_t)min(c, (uint64_t)0xFFFFFFF0u);
+  }
+}
+
+__global__ void k_row_degrees(const uint64_t *row, uint32_t nv, uint32_t *deg) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride)
+    deg[v] = (uint32_t)(row[v + 1] - row[v]);
+}
+
+// Assign tiers: vertices [0, split) in HBM, the rest in the host arena; the
+// offsets come from an exclusive scan of capacities per tier.
+__global__ void k_assign_off(const uint64_t *scan, uint32_t nv, uint32_t split,
+                             uint64_t host_base_scan, uint64_t *off) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride)
+    off[v] = v < split ? scan[v] : ((scan[v] - host_base_scan) | HOST_BIT);
+}
+
+__global__ void k_u32_to_u64(const uint32_t *a, uint32_t n, uint64_t *b) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    b[i] = a[i];
+}
+
+// ---------------------------------------------------------------------------
+// Device R-MAT generator: bit-identical to the oracle's sgso_rmat_edge.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t fin64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+constexpr uint64_t GAMMA = 0x9E3779B97F4A7C15ull;
+
+__global__ void k_rmat(uint32_t scale, uint64_t ne, uint64_t key, uint64_t tA,
+                       uint64_t tAB, uint64_t tABC, int drop_self, uint64_t *keys) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < ne; k += stride) {
+    uint32_t uu = 0, vv = 0;
+    for (uint32_t l = 0; l < scale; ++l) {
+      const uint64_t r = fin64(key + (k * 64u + l + 1) * GAMMA) >> 11;
+      uint32_t bu, bv;
+      if (r < tA) { bu = 0; bv = 0; }
+      else if (r < tAB) { bu = 0; bv = 1; }
+      else if (r < tABC) { bu = 1; bv = 0; }
+      else { bu = 1; bv = 1; }
+      uu = (uu << 1) | bu;
+      vv = (vv << 1) | bv;
+    }
+    keys[k] = (drop_self && uu == vv) ? ~0ull : (((uint64_t)uu << 32) | vv);
+  }
+}
+
+// Weight of edge (u,v) = 1 + top 6 bits of fin64(wkey ^ (u<<32|v)): uniform in
+// [1,64]; identical to the oracle's sgso_weight_of.
+__global__ void k_hash_weights(const uint64_t *keys, const uint32_t *n_ptr, uint64_t wkey,
+                               uint32_t *w) {
+  const uint32_t n = *n_ptr;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    w[i] = 1u + (uint32_t)(fin64(wkey ^ keys[i]) >> 58);
+}
+
+// row[v] = first index of a key with source >= v in a sorted key list.
+__global__ void k_row_from_sorted(const uint64_t *keys, const uint32_t *n_ptr, uint32_t nv,
+                                  uint64_t *row) {
+  const uint32_t n = *n_ptr;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v <= nv; v += stride) {
+    const uint64_t k = v << 32;
+    uint32_t l = 0, r = n;
+    while (l < r) {
+      uint32_t m = (l + r) >> 1;
+      if (keys[m] < k) l = m + 1;
+      else r = m;
+    }
+    row[v] = l;
+  }
+}
+
+__global__ void k_keys_low(const uint64_t *keys, const uint32_t *n_ptr, uint32_t *col) {
+  const uint32_t n = *n_ptr;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    col[i] = (uint32_t)keys[i];
+}
+
+// Per-query summary: reached count, sum / max of finite values, sum of the
+// parents of reached vertices.
+__global__ void k_summary(const unsigned long long *st, uint32_t nv, unsigned long long *out) {
+  unsigned long long reached = 0, sum = 0, mx = 0, psum = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride) {
+    const unsigned long long s = st[v];
+    const uint32_t val = (uint32_t)(s >> 32);
+    if (val == INF32) continue;
+    reached += 1;
+    sum += val;
+    mx = val > mx ? val : mx;
+    if ((uint32_t)s != INF32) psum += (uint32_t)s;
+  }
+  typedef cub::BlockReduce<unsigned long long, RELAX_THREADS> BR;
+  __shared__ typename BR::TempStorage tmp;
+  unsigned long long r = BR(tmp).Sum(reached);
+  __syncthreads();
+  unsigned long long sm = BR(tmp).Sum(sum);
+  __syncthreads();
+  unsigned long long m = BR(tmp).Reduce(mx, cub::Max());
+  __syncthreads();
+  unsigned long long ps = BR(tmp).Sum(psum);
+  if (threadIdx.x == 0) {
+    atomicAdd(&out[0], r);
+    atomicAdd(&out[1], sm);
+    atomicMax(&out[2], m);
+    atomicAdd(&out[3], ps);
+  }
+}
+
+__global__ void k_summary_pr(const double *x, uint32_t nv, double *out) {
+  double sum = 0.0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride) sum += x[v];
+  typedef cub::BlockReduce<double, RELAX_THREADS> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const double s = BR(tmp).Sum(sum);
+  if (threadIdx.x == 0) atomicAdd(out, s);
+}
+
+}  // namespace sgs

@@ -1,0 +1,414 @@
+"""Python binding of the B200 streaming-graph engine (``include/sgs.h``).
+
+Thin ctypes layer over ``lib/libsgs.so``; every call goes through the C ABI.
+There is no fallback: importing works without a GPU (so CPU tests can check
+that the library loads and exports its symbols), but every compute call
+needs the CUDA library and a B200, and raises if either is missing.
+
+Two spellings are offered:
+
+* :class:`Engine` -- the C ABI in Python form (load / add_query /
+  apply_batch / gather);
+* :class:`HybridEngine` -- the call sequence of the reference's sample
+  drivers (``samples/hybrid_sssp/hybrid_sssp.cu:204-296``,
+  ``samples/hybrid_pr/hybrid_pr.cu:154-200``): ``LoadGraph``, ``InitGraph``,
+  ``Start``, per snapshot ``del_edge`` + ``add_edge`` (or ``Cancelation`` +
+  ``Compensate`` for PageRank), then ``GatherValue`` / ``GatherParent`` /
+  ``GatherBuffer``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "lib", "libsgs.so")
+
+BFS, SSSP, CC, PR = 0, 1, 2, 3
+ALGOS = {"bfs": BFS, "sssp": SSSP, "cc": CC, "pr": PR}
+MEM_HOST, MEM_DEVICE = 0, 1
+W_EXPLICIT, W_SYNTH, W_UNIT = 0, 1, 2
+FIELD_VALUE, FIELD_PARENT, FIELD_BUFFER = 0, 1, 2
+INF = 0xFFFFFFFF
+
+OK = 0
+ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of memory",
+          -4: "bad state", -5: "not converged"}
+
+EXPORTS = [
+    "sgs_version", "sgs_last_error", "sgs_config_default", "sgs_create",
+    "sgs_destroy", "sgs_load_csr", "sgs_load_edge_list", "sgs_load_rmat",
+    "sgs_query_add", "sgs_query_remove", "sgs_apply_batch", "sgs_gather",
+    "sgs_get_query_stats", "sgs_get_engine_stats", "sgs_graph_export",
+    "sgs_synchronize", "sgs_kernel_timing", "sgs_get_kernel_stats",
+    "sgs_query_summary", "sgs_gen_update_stream", "sgs_hash_weights",
+]
+
+K_SSSP, K_BFS, K_CC, K_INVALIDATE, K_PR_PUSH = range(5)
+KERNEL_KINDS = {"sssp": K_SSSP, "bfs": K_BFS, "cc": K_CC, "invalidate": K_INVALIDATE,
+                "pr_push": K_PR_PUSH}
+
+
+class SgsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, 'error')} ({code}): {msg}")
+        self.code = code
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("device", C.c_int),
+        ("segments", C.c_uint32),
+        ("n_stream", C.c_uint32),
+        ("block_size", C.c_uint32),
+        ("cache_gb", C.c_double),
+        ("hbm_budget_gb", C.c_double),
+        ("weight_mode", C.c_int),
+        ("max_rounds", C.c_uint32),
+        ("pr_alpha", C.c_double),
+        ("pr_tol", C.c_double),
+        ("slack_div", C.c_uint32),
+        ("arena_headroom", C.c_double),
+    ]
+
+
+class QueryStats(C.Structure):
+    _fields_ = [
+        ("edges_traversed", C.c_uint64),
+        ("edges_total", C.c_uint64),
+        ("invalidated", C.c_uint64),
+        ("rounds", C.c_uint32),
+        ("converged", C.c_uint32),
+        ("ms", C.c_double),
+        ("pr_residual_l1", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class EngineStats(C.Structure):
+    _fields_ = [
+        ("nv", C.c_uint64),
+        ("ne", C.c_uint64),
+        ("slots", C.c_uint64),
+        ("arena_bytes_hbm", C.c_uint64),
+        ("arena_bytes_host", C.c_uint64),
+        ("hbm_resident_vertices", C.c_uint64),
+        ("last_inserted", C.c_uint64),
+        ("last_deleted", C.c_uint64),
+        ("last_relocated", C.c_uint64),
+        ("repacks", C.c_uint64),
+        ("last_apply_ms", C.c_double),
+        ("last_batch_ms", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class KernelStats(C.Structure):
+    _fields_ = [
+        ("launches", C.c_uint64),
+        ("slots", C.c_uint64),
+        ("entries", C.c_uint64),
+        ("bytes_alg", C.c_double),
+        ("ms", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    """Loads lib/libsgs.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {PKG}`")
+    L = C.CDLL(LIB_PATH)
+    vp, u32, u64, i32, dbl = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_double
+    L.sgs_version.restype = C.c_char_p
+    L.sgs_last_error.restype = C.c_char_p
+    L.sgs_config_default.argtypes = [C.POINTER(Config)]
+    L.sgs_config_default.restype = None
+    L.sgs_create.argtypes = [C.POINTER(Config), C.POINTER(vp)]
+    L.sgs_destroy.argtypes = [vp]
+    L.sgs_load_csr.argtypes = [vp, u32, vp, vp, vp, i32]
+    L.sgs_load_edge_list.argtypes = [vp, u32, u64, vp, vp, vp, i32]
+    L.sgs_load_rmat.argtypes = [vp, u32, u32, u64, dbl, dbl, dbl, u64]
+    L.sgs_query_add.argtypes = [vp, i32, u32, C.POINTER(i32)]
+    L.sgs_query_remove.argtypes = [vp, i32]
+    L.sgs_apply_batch.argtypes = [vp, vp, vp, vp, u64, vp, vp, u64, i32]
+    L.sgs_gather.argtypes = [vp, i32, i32, vp, i32]
+    L.sgs_get_query_stats.argtypes = [vp, i32, C.POINTER(QueryStats)]
+    L.sgs_get_engine_stats.argtypes = [vp, C.POINTER(EngineStats)]
+    L.sgs_graph_export.argtypes = [vp, vp, vp, vp, i32]
+    L.sgs_synchronize.argtypes = [vp]
+    L.sgs_kernel_timing.argtypes = [vp, i32]
+    L.sgs_get_kernel_stats.argtypes = [vp, i32, C.POINTER(KernelStats)]
+    L.sgs_query_summary.argtypes = [vp, i32, vp]
+    L.sgs_gen_update_stream.argtypes = [u32, vp, vp, u64, u64, u64, vp, vp, vp, vp]
+    L.sgs_hash_weights.argtypes = [u64, u64, vp, vp, vp]
+    L.sgs_hash_weights.restype = None
+    for name in EXPORTS:
+        if name not in ("sgs_version", "sgs_last_error", "sgs_config_default",
+                        "sgs_hash_weights"):
+            getattr(L, name).restype = i32
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != OK:
+        raise SgsError(rc, lib().sgs_last_error().decode())
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, int):  # device pointer
+        return C.c_void_p(a)
+    return C.c_void_p(a.ctypes.data)
+
+
+def _u32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def default_config(**overrides) -> Config:
+    c = Config()
+    lib().sgs_config_default(C.byref(c))
+    for k, v in overrides.items():
+        if not hasattr(c, k):
+            raise TypeError(f"unknown config field {k}")
+        setattr(c, k, v)
+    return c
+
+
+def gen_update_stream(nv, row, col, seed, n_ins, n_del):
+    """Deterministic synthetic update stream w.r.t. a CSR with sorted rows:
+    (ins_src, ins_dst, del_src, del_dst)."""
+    row = np.ascontiguousarray(row, np.uint64)
+    col = np.ascontiguousarray(col, np.uint32)
+    out = [np.empty(max(n, 1), np.uint32) for n in (n_ins, n_ins, n_del, n_del)]
+    _check(lib().sgs_gen_update_stream(nv, _ptr(row), _ptr(col), seed, n_ins, n_del,
+                                       *[_ptr(a) for a in out]))
+    return out[0][:n_ins], out[1][:n_ins], out[2][:n_del], out[3][:n_del]
+
+
+def hash_weights(wseed, src, dst):
+    src, dst = _u32(src), _u32(dst)
+    w = np.empty(max(len(src), 1), np.uint32)
+    lib().sgs_hash_weights(wseed, len(src), _ptr(src), _ptr(dst), _ptr(w))
+    return w[: len(src)]
+
+
+class Query:
+    def __init__(self, engine, qid, algo, source):
+        self.engine, self.qid, self.algo, self.source = engine, qid, algo, source
+
+    def value(self):
+        return self.engine.gather(self.qid, FIELD_VALUE)
+
+    def parent(self):
+        return self.engine.gather(self.qid, FIELD_PARENT)
+
+    def buffer(self):
+        return self.engine.gather(self.qid, FIELD_BUFFER)
+
+    def stats(self):
+        return self.engine.query_stats(self.qid)
+
+    def summary(self):
+        return self.engine.summary(self.qid)
+
+
+class Engine:
+    """One dynamic graph plus registered queries on one GPU."""
+
+    def __init__(self, config: Config | None = None, **overrides):
+        self.cfg = config if config is not None else default_config(**overrides)
+        h = C.c_void_p()
+        _check(lib().sgs_create(C.byref(self.cfg), C.byref(h)))
+        self.h = h
+        self.nv = 0
+        self._queries = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sgs_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- load
+    def load_csr(self, nv, row, col, w=None):
+        row = np.ascontiguousarray(row, dtype=np.uint64)
+        col, w = _u32(col), _u32(w)
+        _check(lib().sgs_load_csr(self.h, nv, _ptr(row), _ptr(col), _ptr(w), MEM_HOST))
+        self.nv = nv
+        self._queries.clear()
+
+    def load_edge_list(self, src, dst, w=None, nv=0):
+        src, dst, w = _u32(src), _u32(dst), _u32(w)
+        _check(lib().sgs_load_edge_list(self.h, nv, len(src), _ptr(src), _ptr(dst), _ptr(w), MEM_HOST))
+        self.nv = int(self.engine_stats()["nv"])
+        self._queries.clear()
+
+    def load_rmat(self, scale, edge_factor=16, seed=1, a=0.57, b=0.19, c=0.19, wseed=1):
+        _check(lib().sgs_load_rmat(self.h, scale, edge_factor, seed, a, b, c, wseed))
+        self.nv = 1 << scale
+        self._queries.clear()
+
+    # -- queries
+    def add_query(self, algo, source=0) -> Query:
+        if isinstance(algo, str):
+            algo = ALGOS[algo]
+        qid = C.c_int()
+        _check(lib().sgs_query_add(self.h, algo, source, C.byref(qid)))
+        q = Query(self, qid.value, algo, source)
+        self._queries[qid.value] = q
+        return q
+
+    def remove_query(self, q):
+        _check(lib().sgs_query_remove(self.h, q.qid if isinstance(q, Query) else q))
+
+    def apply_batch_ptr(self, isp, idp, iwp, ni, dsp, ddp, nd, mem):
+        """Raw-pointer form (host pinned or device memory, as ints)."""
+        _check(lib().sgs_apply_batch(self.h, _ptr(isp), _ptr(idp), _ptr(iwp), ni,
+                                     _ptr(dsp), _ptr(ddp), nd, mem))
+
+    def apply_batch(self, ins_src=(), ins_dst=(), ins_w=None, del_src=(), del_dst=(), mem=MEM_HOST):
+        if mem == MEM_DEVICE:
+            # device pointers (ints) with explicit counts: (ptr, n) tuples
+            (isp, ni), (idp, _), (dsp, nd), (ddp, _) = ins_src, ins_dst, del_src, del_dst
+            iwp = ins_w[0] if ins_w is not None else None
+            _check(lib().sgs_apply_batch(self.h, _ptr(isp), _ptr(idp), _ptr(iwp), ni,
+                                         _ptr(dsp), _ptr(ddp), nd, MEM_DEVICE))
+            return
+        isrc, idst, iw = _u32(ins_src), _u32(ins_dst), _u32(ins_w)
+        dsrc, ddst = _u32(del_src), _u32(del_dst)
+        _check(lib().sgs_apply_batch(self.h, _ptr(isrc), _ptr(idst), _ptr(iw), len(isrc),
+                                     _ptr(dsrc), _ptr(ddst), len(dsrc), MEM_HOST))
+
+    def gather(self, qid, field=FIELD_VALUE):
+        q = self._queries.get(qid)
+        pr = q is not None and q.algo == PR
+        out = np.empty(self.nv, np.float64 if pr else np.uint32)
+        _check(lib().sgs_gather(self.h, qid, field, _ptr(out), MEM_HOST))
+        return out
+
+    def query_stats(self, qid):
+        s = QueryStats()
+        _check(lib().sgs_get_query_stats(self.h, qid, C.byref(s)))
+        return s.as_dict()
+
+    def summary(self, qid):
+        out = np.zeros(4, np.uint64)
+        _check(lib().sgs_query_summary(self.h, qid, _ptr(out)))
+        return out
+
+    def engine_stats(self):
+        s = EngineStats()
+        _check(lib().sgs_get_engine_stats(self.h, C.byref(s)))
+        return s.as_dict()
+
+    def export(self, weights=False):
+        st = self.engine_stats()
+        nv, ne = int(st["nv"]), int(st["ne"])
+        row = np.empty(nv + 1, np.uint64)
+        col = np.empty(max(ne, 1), np.uint32)
+        w = np.empty(max(ne, 1), np.uint32) if weights else None
+        _check(lib().sgs_graph_export(self.h, _ptr(row), _ptr(col), _ptr(w), MEM_HOST))
+        return row, col[:ne], (None if w is None else w[:ne])
+
+    def synchronize(self):
+        _check(lib().sgs_synchronize(self.h))
+
+    def kernel_timing(self, enable=True):
+        _check(lib().sgs_kernel_timing(self.h, int(enable)))
+
+    def kernel_stats(self):
+        out = {}
+        for name, k in KERNEL_KINDS.items():
+            s = KernelStats()
+            _check(lib().sgs_get_kernel_stats(self.h, k, C.byref(s)))
+            out[name] = s.as_dict()
+        return out
+
+
+class HybridEngine:
+    """The reference sample drivers' call sequence over :class:`Engine`.
+
+    ``algo`` is one of "pr", "sssp", "bfs", "cc" (the HybridPageRank /
+    HybridSSSP / HybridBFS / HybridCC drivers).  Snapshots come from the
+    reference's update-file format (see :mod:`sgs.io`).
+    """
+
+    def __init__(self, algo, **cfg):
+        self.algo = ALGOS[algo] if isinstance(algo, str) else algo
+        self.engine = Engine(**cfg)
+        self.q = None
+        self._source = 0
+        self._pending = None
+
+    # Engine::LoadGraph
+    def LoadGraph(self, src=None, dst=None, w=None, nv=0, csr=None):
+        if csr is not None:
+            self.engine.load_csr(*csr)
+        else:
+            self.engine.load_edge_list(src, dst, w, nv)
+
+    # Engine::InitGraph(args...): the source node (SSSP/BFS), error (PR)
+    def InitGraph(self, arg=0):
+        if self.algo in (SSSP, BFS):
+            self._source = int(arg)
+
+    # Engine::Start: static convergence
+    def Start(self):
+        self.q = self.engine.add_query(self.algo, self._source)
+        return self.q.stats()
+
+    # SSSP/BFS/CC snapshot: del_edge(...) then add_edge(...)
+    def del_edge(self, del_src, del_dst):
+        self._pending = (np.asarray(del_src, np.uint32), np.asarray(del_dst, np.uint32))
+
+    def add_edge(self, ins_src, ins_dst, ins_w=None):
+        d = self._pending or (np.empty(0, np.uint32), np.empty(0, np.uint32))
+        self._pending = None
+        self.engine.apply_batch(ins_src, ins_dst, ins_w, d[0], d[1])
+        return self.q.stats()
+
+    # PR snapshot: Cancelation(...) then Compensate(...)
+    Cancelation = del_edge
+    Compensate = add_edge
+
+    def GatherValue(self):
+        return self.q.value()
+
+    def GatherParent(self):
+        return self.q.parent()
+
+    def GatherBuffer(self):
+        return self.q.buffer()
+
+    def GetNodeNum(self):
+        return self.engine.nv

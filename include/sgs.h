@@ -1,0 +1,218 @@
+/*
+ * sgs.h -- C ABI of the B200-native incremental streaming-graph engine
+ * (drop-in for the hot path of C-GpuStreamGraph).
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes
+ * (0 = ok, < 0 = error; sgs_last_error() gives a thread-local message).  No
+ * entry point exits the process (the reference exits through
+ * GROUTE_CUDA_CHECK -> HandleError, groute/internal/cuda_utils.h:59-65).
+ *
+ * Mapping to the reference (paths relative to the reference project):
+ *   sgs_create / sgs_config       <- Engine ctor + flags
+ *                                    (include/framework/framework.cuh:124-140,
+ *                                     include/utils/app_skeleton.h:42-100)
+ *   sgs_load_csr / sgs_load_edge_list
+ *                                 <- Engine::LoadGraph + Context graph load
+ *                                    (framework.cuh:310-384,
+ *                                     include/utils/graphs/traversal.h:149-170,
+ *                                     src/utils/parser.cpp:296-406)
+ *   sgs_query_add                 <- Engine::InitGraph(args...) + Engine::Start
+ *                                    (framework.cuh:389-439, :549-584) for the
+ *                                    AppBase functors of samples/hybrid_{bfs,
+ *                                    sssp,cc,pr}
+ *   sgs_apply_batch               <- one snapshot of the sample drivers:
+ *                                    del_edge + add_edge (SSSP/BFS/CC,
+ *                                    framework.cuh:975-1038, :1507-1655) or
+ *                                    Cancelation + Compensate (PR,
+ *                                    framework.cuh:1110-1301), with the PMA
+ *                                    updates of csr_graph.cuh:658-811
+ *   sgs_gather                    <- Engine::GatherValue/GatherParent/
+ *                                    GatherBuffer (framework.cuh:1657-1679)
+ *   sgs_get_query_stats           <- RunningInfo counters
+ *                                    (framework/hybrid_policy.h:38-136)
+ */
+#ifndef SGS_H
+#define SGS_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define SGS_API __attribute__((visibility("default")))
+#else
+#define SGS_API
+#endif
+
+/* status codes */
+#define SGS_OK 0
+#define SGS_ERR_INVALID (-1)   /* bad argument / out-of-range vertex id   */
+#define SGS_ERR_CUDA (-2)      /* CUDA runtime error                       */
+#define SGS_ERR_OOM (-3)       /* device or pinned-host allocation failed  */
+#define SGS_ERR_STATE (-4)     /* call out of order (e.g. no graph loaded) */
+#define SGS_ERR_NOCONV (-5)    /* round limit reached before convergence   */
+
+/* algorithms: the four sample apps */
+#define SGS_BFS 0  /* samples/hybrid_bfs  : depth from source             */
+#define SGS_SSSP 1 /* samples/hybrid_sssp : integer-weight distance       */
+#define SGS_CC 2   /* samples/hybrid_cc   : min id reaching v (directed)  */
+#define SGS_PR 3   /* samples/hybrid_pr   : unnormalised delta PageRank   */
+
+/* where caller buffers live */
+#define SGS_MEM_HOST 0
+#define SGS_MEM_DEVICE 1
+
+/* edge weights (reference: push_functor.h:306 synthesizes (u+v)%128+1) */
+#define SGS_W_EXPLICIT 0 /* weights stored per edge (>= 1)                */
+#define SGS_W_SYNTH 1    /* (src+dst)%128+1 computed per edge, not stored */
+#define SGS_W_UNIT 2     /* every weight 1, not stored                    */
+
+/* gather fields */
+#define SGS_FIELD_VALUE 0  /* u32 value (BFS/SSSP/CC); f64 rank (PR)        */
+#define SGS_FIELD_PARENT 1 /* u32 parent (BFS/SSSP/CC)                      */
+#define SGS_FIELD_BUFFER 2 /* u32 buffer (== value once converged); f64
+                              residual (PR)                                 */
+
+typedef struct sgs_engine sgs_engine;
+
+typedef struct sgs_config {
+  int device;             /* CUDA device ordinal                           */
+  uint32_t segments;      /* -SEGMENT: vertex segments (residency unit)    */
+  uint32_t n_stream;      /* -n_stream: accepted for drop-in; unused       */
+  uint32_t block_size;    /* -block_size: accepted for drop-in; unused     */
+  double cache_gb;        /* -cache: accepted; see hbm_budget_gb           */
+  double hbm_budget_gb;   /* HBM budget for edge blocks; <= 0: unlimited.
+                             Segments beyond it live in pinned host memory
+                             and are read over the host link              */
+  int weight_mode;        /* SGS_W_*                                        */
+  uint32_t max_rounds;    /* round limit per convergence (reference: 1000) */
+  double pr_alpha;        /* damping, 0.85 (hybrid_pr_common.h:39)         */
+  double pr_tol;          /* stop when sum|residual| < pr_tol              */
+  uint32_t slack_div;     /* per-block slack: cap = deg + deg/slack_div + 2 */
+  double arena_headroom;  /* extra arena fraction for relocated blocks    */
+} sgs_config;
+
+typedef struct sgs_query_stats {
+  uint64_t edges_traversed;   /* edges visited by the last snapshot/start  */
+  uint64_t edges_total;       /* since the query was added                 */
+  uint64_t invalidated;       /* vertices reset by the last deletion phase */
+  uint32_t rounds;            /* relaxation rounds of the last update      */
+  uint32_t converged;         /* 1 if the last update converged            */
+  double ms;                  /* device time of the last update            */
+  double pr_residual_l1;      /* PR: residual L1 when stopped              */
+} sgs_query_stats;
+
+typedef struct sgs_engine_stats {
+  uint64_t nv;
+  uint64_t ne;                /* live edges                                */
+  uint64_t slots;             /* used slots (live + tombstones)            */
+  uint64_t arena_bytes_hbm;
+  uint64_t arena_bytes_host;
+  uint64_t hbm_resident_vertices; /* vertices whose block is in HBM        */
+  uint64_t last_inserted;     /* kept inserts of the last batch            */
+  uint64_t last_deleted;      /* slots tombstoned by the last batch        */
+  uint64_t last_relocated;    /* blocks relocated by the last batch        */
+  uint64_t repacks;           /* arena repacks so far                      */
+  double last_apply_ms;       /* device time of the last graph update      */
+  double last_batch_ms;       /* device time of the whole last snapshot    */
+} sgs_engine_stats;
+
+/* Per-kernel-class timing of the relaxation launches (CUDA events on the
+ * engine's stream around every launch that has work; off by default).
+ * bytes_alg = algorithmic bytes: per traversed slot 16 B (SSSP: id, weight,
+ * 8 B distance read+write), 12 B (BFS/CC/invalidation), 20 B (PR FP64
+ * residual push), plus 20 B per active vertex. */
+#define SGS_K_SSSP 0
+#define SGS_K_BFS 1
+#define SGS_K_CC 2
+#define SGS_K_INVALIDATE 3
+#define SGS_K_PR_PUSH 4
+#define SGS_K_COUNT 5
+typedef struct sgs_kernel_stats {
+  uint64_t launches;
+  uint64_t slots;      /* positions walked (edges incl. tombstones)          */
+  uint64_t entries;    /* active vertices                                    */
+  double bytes_alg;
+  double ms;
+} sgs_kernel_stats;
+
+SGS_API const char *sgs_version(void);
+SGS_API const char *sgs_last_error(void);
+SGS_API void sgs_config_default(sgs_config *cfg);
+
+SGS_API int sgs_create(const sgs_config *cfg, sgs_engine **out);
+SGS_API int sgs_destroy(sgs_engine *e);
+
+/* Graph load.  row has nv+1 entries, col/w row[nv]; w may be NULL unless
+ * weight_mode is SGS_W_EXPLICIT.  Lists are taken in the given order. */
+SGS_API int sgs_load_csr(sgs_engine *e, uint32_t nv, const uint64_t *row,
+                         const uint32_t *col, const uint32_t *w, int mem);
+/* Edge list in file order (market_big: parser.cpp:296-406); nv = 0 means
+ * max id + 1.  Duplicates and self-loops are kept, like the reference. */
+SGS_API int sgs_load_edge_list(sgs_engine *e, uint32_t nv, uint64_t ne,
+                               const uint32_t *src, const uint32_t *dst,
+                               const uint32_t *w, int mem);
+/* Synthetic directed R-MAT generated on the device (2^scale vertices,
+ * edge_factor*2^scale draws, self-loops and duplicates removed), weights
+ * uniform in [1,64] from wseed in SGS_W_EXPLICIT mode.  Bit-identical to the
+ * CPU generator used by the tests. */
+SGS_API int sgs_load_rmat(sgs_engine *e, uint32_t scale, uint32_t edge_factor,
+                          uint64_t seed, double a, double b, double c,
+                          uint64_t wseed);
+
+/* Registers a query and runs it to convergence on the current graph
+ * (InitGraph + Start).  source is clamped to [0, nv-1] as the samples do. */
+SGS_API int sgs_query_add(sgs_engine *e, int algo, uint32_t source, int *qid);
+SGS_API int sgs_query_remove(sgs_engine *e, int qid);
+
+/* One snapshot: applies the batch to the graph and brings every registered
+ * query up to date incrementally.  Inserts are applied first, then every
+ * (src,dst) listed in the deletes is removed (all copies), matching
+ * framework.cuh:1011-1012.  ins_w is read only in SGS_W_EXPLICIT mode. */
+SGS_API int sgs_apply_batch(sgs_engine *e, const uint32_t *ins_src,
+                            const uint32_t *ins_dst, const uint32_t *ins_w,
+                            uint64_t n_ins, const uint32_t *del_src,
+                            const uint32_t *del_dst, uint64_t n_del, int mem);
+
+/* Copies nv elements of a field (u32, or f64 for PR value/buffer). */
+SGS_API int sgs_gather(sgs_engine *e, int qid, int field, void *out, int mem);
+SGS_API int sgs_get_query_stats(sgs_engine *e, int qid, sgs_query_stats *out);
+SGS_API int sgs_get_engine_stats(sgs_engine *e, sgs_engine_stats *out);
+
+/* Live graph as a CSR (row: nv+1, col/w: ne).  Per-vertex order is not
+ * guaranteed.  w may be NULL. */
+SGS_API int sgs_graph_export(sgs_engine *e, uint64_t *row, uint32_t *col,
+                             uint32_t *w, int mem);
+SGS_API int sgs_synchronize(sgs_engine *e);
+
+/* Per-query summary computed on the device (a few bytes to read back per
+ * snapshot): out[0] = reached vertices (value != INF; PR: all), out[1] = sum
+ * of finite values (PR: sum of ranks as IEEE-754 bits of a double), out[2] =
+ * max finite value, out[3] = sum of parents of reached vertices. */
+SGS_API int sgs_query_summary(sgs_engine *e, int qid, uint64_t out[4]);
+
+/* Synthetic update stream (host arrays, no engine needed): n_del distinct
+ * existing edges sampled uniformly by edge index and n_ins distinct non-edges
+ * (u != v) sampled uniformly over vertex pairs, both w.r.t. the given CSR
+ * whose rows must be sorted (e.g. a freshly generated R-MAT graph).  The
+ * sequence for (seed, n_ins, n_del) is deterministic; snapshot k takes the
+ * k-th slice.  Returns SGS_ERR_INVALID if the graph cannot supply them. */
+SGS_API int sgs_gen_update_stream(uint32_t nv, const uint64_t *row,
+                                  const uint32_t *col, uint64_t seed,
+                                  uint64_t n_ins, uint64_t n_del,
+                                  uint32_t *ins_src, uint32_t *ins_dst,
+                                  uint32_t *del_src, uint32_t *del_dst);
+/* Seeded weights uniform in [1,64] for edge lists (same function as the
+ * R-MAT loader's weights). */
+SGS_API void sgs_hash_weights(uint64_t wseed, uint64_t n, const uint32_t *src,
+                              const uint32_t *dst, uint32_t *w);
+
+SGS_API int sgs_kernel_timing(sgs_engine *e, int enable);
+SGS_API int sgs_get_kernel_stats(sgs_engine *e, int kind, sgs_kernel_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SGS_H */
