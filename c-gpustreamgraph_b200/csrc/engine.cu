@@ -38,6 +38,15 @@ struct SgsError {
 
 [[noreturn]] void fail(int code, const std::string &msg) { throw SgsError{code, msg}; }
 
+}  // namespace
+
+// Shared with the other translation units of the library (not exported).
+namespace sgs {
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+}  // namespace sgs
+
+namespace {
+
 void ck(cudaError_t e, const char *what) {
   if (e == cudaSuccess) return;
   cudaGetLastError();
@@ -245,6 +254,7 @@ struct sgs_engine {
     if (n == 0) fail(SGS_ERR_INVALID, "empty graph");
     if (n >= (1u << 27)) fail(SGS_ERR_INVALID, "more than 2^27-1 vertices is not supported");
     queries.clear();
+    loaded = false;
     est = sgs_engine_stats{};
     nv = n;
     uint64_t ne_in = 0;
@@ -253,6 +263,18 @@ struct sgs_engine {
     if (ne_in >= (1ull << CNT_SHIFT)) fail(SGS_ERR_INVALID, "too many edges");
     if (cfg.weight_mode == SGS_W_EXPLICIT && ne_in && !d_w)
       fail(SGS_ERR_INVALID, "explicit weight mode needs weights");
+    {
+      CK(cudaMemsetAsync(b_err.p, 0, sizeof(unsigned int), s));
+      k_validate_csr<<<grid_elem(std::max<uint64_t>(ne_in, nv)), 256, 0, s>>>(
+          d_row, d_col, cfg.weight_mode == SGS_W_EXPLICIT ? d_w : nullptr, n, ne_in, b_err.p);
+      CK(cudaGetLastError());
+      unsigned int herr = 0;
+      CK(cudaMemcpyAsync(&herr, b_err.p, sizeof(herr), cudaMemcpyDeviceToHost, s));
+      sync();
+      if (herr & 4u) fail(SGS_ERR_INVALID, "row offsets must start at 0 and not decrease");
+      if (herr & 1u) fail(SGS_ERR_INVALID, "edge destination out of range");
+      if (herr & 2u) fail(SGS_ERR_INVALID, "edge weight 0 (weights must be >= 1)");
+    }
     off.ensure(nv);
     slots.ensure(nv);
     live.ensure(nv);

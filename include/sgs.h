@@ -210,6 +210,27 @@ SGS_API void sgs_hash_weights(uint64_t wseed, uint64_t n, const uint32_t *src,
                               const uint32_t *dst, uint32_t *w);
 
 SGS_API int sgs_kernel_timing(sgs_engine *e, int enable);
+
+/* From-scratch SSSP (w != NULL) or BFS (w == NULL) over a CSR that the caller
+ * already holds in device memory (row: nv+1 u64 offsets, col/w: row[nv] u32),
+ * writing dist[nv] and, if parent != NULL, parent[nv] (device pointers) on
+ * `stream` (a cudaStream_t; NULL = default stream).  No counterpart in the
+ * reference.  It allocates nothing: for callers that cannot call cudaMalloc
+ * (allocator hooks, code running while a graph is being captured, embedders
+ * whose device memory is fixed at start-up), its scratch is a fixed static
+ * device array (about 36 MB, reserved on every GPU that loads the library
+ * until exit), so nv <= SGS_NOALLOC_MAX_VERTICES and row[nv] <=
+ * SGS_NOALLOC_MAX_EDGES, else SGS_ERR_INVALID.  Results equal those of an
+ * SGS_SSSP / SGS_BFS query on the same graph (values and smallest-id tight
+ * parents).  All calls on a device share the scratch: calls that overlap on
+ * the GPU race and must be serialised.  The first call on a device looks up
+ * the scratch address; make it before any stream capture starts. */
+#define SGS_NOALLOC_MAX_VERTICES (1u << 20)
+#define SGS_NOALLOC_MAX_EDGES (1ull << 25)
+SGS_API int sgs_sssp_csr_noalloc(uint32_t nv, const uint64_t *row,
+                                 const uint32_t *col, const uint32_t *w,
+                                 uint32_t source, uint32_t *dist,
+                                 uint32_t *parent, void *stream);
 SGS_API int sgs_get_kernel_stats(sgs_engine *e, int kind, sgs_kernel_stats *out);
 
 #ifdef __cplusplus
