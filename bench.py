@@ -373,10 +373,72 @@ def cpu_baseline(e, a):
 
 # ----------------------------------------------------------------- reference arm
 def reference_arm(a, R):
+    """The reference's own CPU code for this path, on the host cores.
+
+    The reference computes its per-snapshot answers on the GPU; its CPU path
+    is the serial host oracles of the samples.  Each step runs the
+    reference's BFSHost (samples/hybrid_bfs/hybrid_bfs_host.cpp:33-60, built
+    from the reference sources into oracle/_ref) from scratch on that
+    snapshot's graph, once per host core with a different source, all
+    concurrently.  The snapshot's 1M updates are applied to the host graph
+    between steps, outside the timed region.  GTEPS = edges of the reached
+    vertices summed over the runs / wall time of the step."""
     if R.rank != 0:
         return None
-    return {"impl": "reference", "metric": METRIC, "unit": UNIT,
-            "unavailable": "reference CPU arm not wired yet"}
+    import threading as _th
+
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+
+    base = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True,
+            "n_gpus": R.world, "steps": a.steps, "warmup": a.warmup}
+    if O.ref_lib() is None:
+        base["unavailable"] = "oracle/_ref (the reference's host code) was not built"
+        return base
+    cores = os.cpu_count() or 1
+    t0 = time.time()
+    nv, row, col = O.rmat_csr_par(a.scale, a.edge_factor, a.seed)
+    half = a.updates // 2
+    nb = a.warmup + a.steps
+    i_s, i_d, d_s, d_d = O.gen_updates(nv, row, col, a.seed * 1000003, nb * half, nb * half)
+    setup_s = time.time() - t0
+    sources = [int(s) for s in np.linspace(0, nv - 1, cores, dtype=np.int64)]
+    sources[0] = 0
+    outs = [np.empty(nv, np.uint32) for _ in sources]
+    tot_e, tot_t, step_ms = 0, 0.0, []
+    for k in range(nb):
+        s = slice(k * half, (k + 1) * half)
+        row, col, _ = O.apply(nv, row, col, None, i_s[s], i_d[s], None, d_s[s], d_d[s])
+        g = O.RefGraph(nv, row, col)
+        deg = np.diff(row)
+        ths = [_th.Thread(target=g.bfs, args=(src, out)) for src, out in zip(sources, outs)]
+        t1 = time.perf_counter()
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        dt = time.perf_counter() - t1
+        g.close()
+        edges = int(sum(int(deg[o != O.INF].sum()) for o in outs))
+        if k >= a.warmup:
+            tot_e += edges
+            tot_t += dt
+            step_ms.append(dt * 1e3)
+    value = tot_e / tot_t / 1e9
+    base.update({
+        "value": round(value, 4), "ms_per_step": round(statistics.mean(step_ms), 2),
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (CPU R-MAT and update stream, same graph and stream as the engine arm)",
+        "config": {"workload": f"incremental SSSP/BFS/CC, R-MAT scale {a.scale} ef {a.edge_factor} seed {a.seed}, "
+                               f"{a.updates} updates/snapshot (50/50), source 0, HBM budget {a.budget_gb} GB",
+                   "nv": nv, "setup_s": round(setup_s, 1)},
+        "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": "per snapshot: the reference's BFSHost (compiled from its sources) from "
+                                   f"scratch on the updated graph, {cores} sources run concurrently, one per "
+                                   "host core; updates applied outside the timed region"},
+        "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    })
+    return base
 
 
 def main():

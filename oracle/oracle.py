@@ -56,6 +56,7 @@ def lib():
     sig = {
         "sgso_mix64": (u64, [u64]),
         "sgso_rmat_raw": (None, [u32, u64, u64, u64, u64, u64, _u32p, _u32p]),
+        "sgso_rmat_csr_par": (u64, [u32, u32, u64, u64, u64, u64, _u64p, _u32p]),
         "sgso_build_csr": (u64, [u32, u64, _u32p, _u32p, i32, i32, _u64p, _u32p]),
         "sgso_csr_file_order": (None, [u32, u64, _u32p, _u32p, _vp, _u64p, _u32p, _vp]),
         "sgso_weight_of": (u32, [u64, u32, u32]),
@@ -96,6 +97,11 @@ def ref_lib():
     L.ref_sssp_host.argtypes = [u32, _u64p, _u32p, u32, _u32p]
     L.ref_bfs_host.argtypes = [u32, _u64p, _u32p, u32, _u32p]
     L.ref_pr_host.argtypes = [u32, _u64p, _u32p, dbl, _f32p]
+    L.ref_graph_create.restype = _vp
+    L.ref_graph_create.argtypes = [u32, _u64p, _u32p]
+    L.ref_graph_destroy.argtypes = [_vp]
+    L.ref_graph_bfs.argtypes = [_vp, u32, _u32p]
+    L.ref_graph_sssp.argtypes = [_vp, u32, _u32p]
     L.ref_pma_create.restype = _vp
     L.ref_pma_create.argtypes = [u32, _u64p, _u32p]
     L.ref_pma_insert.argtypes = [_vp, u32, u32]
@@ -132,6 +138,16 @@ def rmat_csr(scale, edge_factor=16, seed=1, a=0.57, b=0.19, c=0.19):
     col = np.empty(ne, np.uint32)
     m = L.sgso_build_csr(nv, ne, src, dst, 1, 1, row, col)
     return nv, row, col[:m].copy()
+
+
+def rmat_csr_par(scale, edge_factor=16, seed=1, a=0.57, b=0.19, c=0.19):
+    """rmat_csr built with OpenMP threads (same graph)."""
+    nv = 1 << scale
+    tA, tAB, tABC = rmat_thresholds(a, b, c)
+    row = np.empty(nv + 1, np.uint64)
+    col = np.empty(nv * edge_factor, np.uint32)
+    m = lib().sgso_rmat_csr_par(scale, edge_factor, seed, tA, tAB, tABC, row, col)
+    return nv, row, col[:m]
 
 
 def csr_from_edges(nv, src, dst, dedupe=True, drop_self=True):
@@ -320,3 +336,28 @@ def ref_pr_host(nv, row, col, err=1e-6):
     r = np.empty(max(nv, 1), np.float32)
     ref_lib().ref_pr_host(nv, row, col, err, r)
     return r[:nv]
+
+
+class RefGraph:
+    """A CSR bound once into the reference's groute host::CSRGraph, for timed
+    calls of its BFSHost / SSSPHostNaive (ctypes releases the GIL, so calls
+    from several Python threads run concurrently)."""
+
+    def __init__(self, nv, row, col):
+        R = ref_lib()
+        if R is None:
+            raise RuntimeError("oracle/_ref not built (make -C oracle ref)")
+        self.R, self.nv = R, nv
+        self.h = R.ref_graph_create(nv, np.ascontiguousarray(row, np.uint64),
+                                    np.ascontiguousarray(col, np.uint32))
+
+    def bfs(self, source, out):
+        self.R.ref_graph_bfs(self.h, int(source), out)
+
+    def sssp(self, source, out):
+        self.R.ref_graph_sssp(self.h, int(source), out)
+
+    def close(self):
+        if self.h:
+            self.R.ref_graph_destroy(self.h)
+            self.h = None

@@ -63,6 +63,24 @@ void ref_pr_host(uint32_t nv, const uint64_t *row, const uint32_t *col,
   std::memcpy(out, r.data(), sizeof(float) * nv);
 }
 
+/* A graph built once and reused by many timed oracle calls. */
+void *ref_graph_create(uint32_t nv, const uint64_t *row, const uint32_t *col) {
+  auto *g = new groute::graphs::host::CSRGraph(nv, row[nv]);
+  fill_csr(*g, nv, row, col);
+  return g;
+}
+void ref_graph_destroy(void *h) { delete (groute::graphs::host::CSRGraph *)h; }
+void ref_graph_bfs(void *h, uint32_t source, uint32_t *out) {
+  auto &g = *(groute::graphs::host::CSRGraph *)h;
+  std::vector<uint32_t> d = BFSHost(g, source);
+  std::memcpy(out, d.data(), sizeof(uint32_t) * g.nnodes);
+}
+void ref_graph_sssp(void *h, uint32_t source, uint32_t *out) {
+  auto &g = *(groute::graphs::host::CSRGraph *)h;
+  std::vector<ref_dist_t> d = SSSPHostNaive(g, source);
+  std::memcpy(out, d.data(), sizeof(uint32_t) * g.nnodes);
+}
+
 /* The PMA is bound the way traversal.h:165-170 does (row/col of the input
  * graph, no weights), then updated with the reference's own insert/del_edge. */
 struct ref_pma {

@@ -8,8 +8,10 @@
  */
 #include "sgs_oracle.h"
 
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #define GAMMA 0x9E3779B97F4A7C15ull
 
@@ -100,6 +102,110 @@ uint64_t sgso_build_csr(uint32_t nv, uint64_t ne, const uint32_t *src,
   for (uint64_t i = 0; i < k; ++i) col[i] = (uint32_t)keys[i];
   free(keys);
   return k;
+}
+
+static int cmp_u32(const void *a, const void *b) {
+  uint32_t x = *(const uint32_t *)a, y = *(const uint32_t *)b;
+  return x < y ? -1 : x > y;
+}
+static void sort_u32(uint32_t *a, uint64_t n) {
+  if (n < 32) {
+    for (uint64_t i = 1; i < n; ++i) {
+      uint32_t x = a[i];
+      uint64_t j = i;
+      while (j > 0 && a[j - 1] > x) { a[j] = a[j - 1]; --j; }
+      a[j] = x;
+    }
+  } else {
+    qsort(a, n, sizeof(uint32_t), cmp_u32);
+  }
+}
+
+/* Minimal parallel-for over [0,n) with pthreads, static contiguous blocks. */
+typedef struct {
+  void (*fn)(void *, uint64_t, uint64_t);
+  void *arg;
+  uint64_t lo, hi;
+} pf_task;
+static void *pf_run(void *p) {
+  pf_task *t = (pf_task *)p;
+  t->fn(t->arg, t->lo, t->hi);
+  return NULL;
+}
+static void parallel_for(uint64_t n, void (*fn)(void *, uint64_t, uint64_t), void *arg) {
+  long nt = sysconf(_SC_NPROCESSORS_ONLN);
+  if (nt < 1) nt = 1;
+  if (nt > 64) nt = 64;
+  pthread_t th[64];
+  pf_task tk[64];
+  for (long i = 0; i < nt; ++i) {
+    tk[i].fn = fn;
+    tk[i].arg = arg;
+    tk[i].lo = n * i / nt;
+    tk[i].hi = n * (i + 1) / nt;
+    pthread_create(&th[i], NULL, pf_run, &tk[i]);
+  }
+  for (long i = 0; i < nt; ++i) pthread_join(th[i], NULL);
+}
+
+typedef struct {
+  uint32_t scale;
+  uint64_t seed, tA, tAB, tABC;
+  uint64_t *cnt, *fill;
+  uint32_t *col;
+} rmat_par;
+
+static void rmat_count(void *p, uint64_t lo, uint64_t hi) {
+  rmat_par *a = (rmat_par *)p;
+  for (uint64_t k = lo; k < hi; ++k) {
+    uint32_t u, v;
+    sgso_rmat_edge(a->scale, a->seed, k, a->tA, a->tAB, a->tABC, &u, &v);
+    if (u != v) __atomic_fetch_add(&a->cnt[u + 1], 1, __ATOMIC_RELAXED);
+  }
+}
+static void rmat_scatter(void *p, uint64_t lo, uint64_t hi) {
+  rmat_par *a = (rmat_par *)p;
+  for (uint64_t k = lo; k < hi; ++k) {
+    uint32_t u, v;
+    sgso_rmat_edge(a->scale, a->seed, k, a->tA, a->tAB, a->tABC, &u, &v);
+    if (u != v) a->col[__atomic_fetch_add(&a->fill[u], 1, __ATOMIC_RELAXED)] = v;
+  }
+}
+static void rmat_rows(void *p, uint64_t lo, uint64_t hi) {
+  rmat_par *a = (rmat_par *)p;
+  for (uint64_t u = lo; u < hi; ++u) {
+    uint32_t *x = a->col + a->cnt[u];
+    uint64_t n = a->cnt[u + 1] - a->cnt[u], m = 0;
+    sort_u32(x, n);
+    for (uint64_t i = 0; i < n; ++i)
+      if (i == 0 || x[i] != x[i - 1]) x[m++] = x[i];
+    a->fill[u] = m;
+  }
+}
+
+uint64_t sgso_rmat_csr_par(uint32_t scale, uint32_t edge_factor, uint64_t seed,
+                           uint64_t tA, uint64_t tAB, uint64_t tABC,
+                           uint64_t *row, uint32_t *col) {
+  const uint64_t nv = 1ull << scale, ne = nv * edge_factor;
+  rmat_par a;
+  a.scale = scale; a.seed = seed; a.tA = tA; a.tAB = tAB; a.tABC = tABC;
+  a.cnt = (uint64_t *)calloc(nv + 1, sizeof(uint64_t));
+  a.fill = (uint64_t *)malloc(nv * sizeof(uint64_t));
+  a.col = col;
+  parallel_for(ne, rmat_count, &a);      /* out-degrees, self loops dropped */
+  for (uint64_t v = 0; v < nv; ++v) a.cnt[v + 1] += a.cnt[v];
+  memcpy(a.fill, a.cnt, nv * sizeof(uint64_t));
+  parallel_for(ne, rmat_scatter, &a);    /* destinations into buckets */
+  parallel_for(nv, rmat_rows, &a);       /* sort + unique each bucket */
+  row[0] = 0;
+  for (uint64_t u = 0; u < nv; ++u) row[u + 1] = row[u] + a.fill[u];
+  /* compact left to right: a row's target never passes its source */
+  for (uint64_t u = 0; u < nv; ++u)
+    if (row[u] != a.cnt[u]) memmove(col + row[u], col + a.cnt[u], a.fill[u] * sizeof(uint32_t));
+  uint64_t m = row[nv];
+  free(a.cnt);
+  free(a.fill);
+  return m;
 }
 
 /* parser.cpp:296-406: two passes over the file; per-source lists keep file
@@ -246,10 +352,23 @@ uint64_t sgso_apply(uint32_t nv, const uint64_t *row, const uint32_t *col,
   memcpy(ifill, ib, ((uint64_t)nv + 1) * sizeof(uint64_t));
   uint64_t *iord = (uint64_t *)malloc((n_ins ? n_ins : 1) * sizeof(uint64_t));
   for (uint64_t i = 0; i < n_ins; ++i) iord[ifill[ins_src[i]]++] = i;
+  /* sources that have deletes: only their lists need the per-edge lookup */
+  uint8_t *hasdel = (uint8_t *)calloc((uint64_t)nv + 1, 1);
+  for (uint64_t i = 0; i < n_del; ++i) hasdel[del_src[i]] = 1;
   uint64_t m = 0;
   int overflow = 0;
   for (uint32_t u = 0; u < nv; ++u) {
     row_out[u] = m;
+    if (!hasdel[u]) {
+      uint64_t d = row[u + 1] - row[u];
+      if (m + d > cap_out) { overflow = 1; break; }
+      memcpy(col_out + m, col + row[u], d * sizeof(uint32_t));
+      if (w_out) {
+        if (w) memcpy(w_out + m, w + row[u], d * sizeof(uint32_t));
+        else for (uint64_t i = 0; i < d; ++i) w_out[m + i] = 1u;
+      }
+      m += d;
+    } else
     for (uint64_t e = row[u]; e < row[u + 1]; ++e) {
       uint64_t k = ((uint64_t)u << 32) | col[e];
       if (n_del && in_sorted(dk, n_del, k)) continue;
@@ -270,6 +389,7 @@ uint64_t sgso_apply(uint32_t nv, const uint64_t *row, const uint32_t *col,
     if (overflow) break;
   }
   row_out[nv] = m;
+  free(hasdel);
   free(dk);
   free(ib);
   free(ifill);

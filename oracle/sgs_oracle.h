@@ -45,6 +45,12 @@ void sgso_rmat_raw(uint32_t scale, uint64_t ne, uint64_t seed, uint64_t tA,
 uint64_t sgso_build_csr(uint32_t nv, uint64_t ne, const uint32_t *src,
                         const uint32_t *dst, int dedupe, int drop_self,
                         uint64_t *row, uint32_t *col);
+/* Same graph as sgso_rmat_raw + sgso_build_csr(dedupe, drop_self), built
+ * with OpenMP threads (for scale 20+ inputs of the CPU baselines).  col must
+ * hold edge_factor << scale entries.  Returns the edge count. */
+uint64_t sgso_rmat_csr_par(uint32_t scale, uint32_t edge_factor, uint64_t seed,
+                           uint64_t tA, uint64_t tAB, uint64_t tABC,
+                           uint64_t *row, uint32_t *col);
 /* CSR in input (file) order: counting sort by source, stable. */
 void sgso_csr_file_order(uint32_t nv, uint64_t ne, const uint32_t *src,
                          const uint32_t *dst, const uint32_t *w, uint64_t *row,
