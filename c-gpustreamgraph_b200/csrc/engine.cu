@@ -14,6 +14,7 @@
 #include <cub/device/device_select.cuh>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -22,7 +23,10 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/sgs.h"
+#include "sgs_group.cuh"
 #include "sgs_kernels.cuh"
 
 using namespace sgs;
@@ -95,18 +99,34 @@ struct HBuf {  // pinned, mapped host memory
 
 struct Frontier {
   DBuf<uint32_t> vtx;
+  DBuf<uint32_t> len;
   DBuf<uint64_t> ebase;
   DBuf<uint32_t> ustart;
+};
+
+// A group: up to GMAX integer queries sharing one edge stream (sgs_group.cuh).
+struct Group {
+  static constexpr int S = GMAX;
+  DBuf<unsigned long long> st;  // [nv * S] packed (value, parent)
+  DBuf<uint32_t> val;           // [nv * S] value mirror (read-side filter)
+  uint32_t used = 0;            // lanes in use
+  uint32_t algo_packed = 0;     // 8 bits per lane
+  uint64_t inval[GMAX] = {};    // resets per lane in the last deletion phase
+  LaneAlgo algo() const { return LaneAlgo{algo_packed}; }
+  bool any_sssp(uint32_t lanes) const {
+    for (int q = 0; q < GMAX; ++q)
+      if ((lanes >> q & 1u) && ((algo_packed >> (8 * q)) & 0xFF) == A_SSSP) return true;
+    return false;
+  }
 };
 
 struct Query {
   int id = 0;
   int algo = 0;
   uint32_t source = 0;
-  DBuf<unsigned long long> st;
-  DBuf<uint32_t> mark;
-  uint32_t stamp = 1;
-  DBuf<double> x, r, pv;
+  Group *grp = nullptr;  // BFS / SSSP / CC: group and lane
+  int lane = -1;
+  DBuf<double> x, r, pv;  // PageRank
   sgs_query_stats stats{};
 };
 
@@ -120,6 +140,13 @@ struct Events {
     if (a) cudaEventDestroy(a);
     if (b) cudaEventDestroy(b);
   }
+};
+
+// NVTX range for the lifetime of a scope (phases show up in Nsight tools and
+// let an ncu capture select kernels by phase).
+struct Range {
+  explicit Range(const char *name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
 };
 
 inline uint32_t blocks_for(uint64_t n, uint32_t cap) {
@@ -150,7 +177,8 @@ struct sgs_engine {
   uint64_t repacks = 0;
 
   // frontier scratch
-  Frontier fb[2];
+  Frontier fb[3];                          // rotating frontier buffers
+  DBuf<uint32_t> gm[3];                    // rotating group lane masks
   uint32_t ucap = 0;
   static constexpr uint32_t kSpecial = 8;  // extra counter slots at the end
   DBuf<unsigned long long> cnt;            // [max_rounds + 2 + kSpecial]
@@ -158,6 +186,9 @@ struct sgs_engine {
   DBuf<uint32_t> emark;                    // engine-level marks (touched sets)
   uint32_t estamp = 1;
   DBuf<double> l1;                         // PR per-round L1
+  DBuf<unsigned long long> rstat;          // per-round instance-edge counts
+  DBuf<unsigned long long> b_lane;         // [GMAX] per-lane edge counts
+  DBuf<unsigned long long> b_inval;        // [GMAX] per-lane resets
 
   // batch scratch
   DBuf<uint32_t> b_isrc, b_idst, b_iw, b_dsrc, b_ddst;
@@ -179,6 +210,7 @@ struct sgs_engine {
   sgs_kernel_stats kst[SGS_K_COUNT]{};
 
   std::vector<std::unique_ptr<Query>> queries;
+  std::vector<std::unique_ptr<Group>> groups;
   int next_qid = 1;
   sgs_engine_stats est{};
   Events ev_batch, ev_apply, ev_q;
@@ -205,9 +237,10 @@ struct sgs_engine {
   }
   FrontierView fview(uint32_t buf, unsigned long long *counter) {
     FrontierView f;
-    f.vtx = fb[buf & 1].vtx.p;
-    f.ebase = fb[buf & 1].ebase.p;
-    f.ustart = fb[buf & 1].ustart.p;
+    f.vtx = fb[buf % 3].vtx.p;
+    f.len = fb[buf % 3].len.p;
+    f.ebase = fb[buf % 3].ebase.p;
+    f.ustart = fb[buf % 3].ustart.p;
     f.counter = (uint64_t *)counter;
     f.ucap = ucap;
     return f;
@@ -240,6 +273,10 @@ struct sgs_engine {
     b_nkept.ensure(1);
     rl_count.ensure(1);
     l1.ensure(cfg.max_rounds + 2);
+    rstat.ensure(cfg.max_rounds + 2);
+    b_lane.ensure(GMAX);
+    b_inval.ensure(GMAX);
+    if (cfg.group_size < 1 || cfg.group_size > GMAX) cfg.group_size = GMAX;
     ev_batch.init();
     ev_apply.init();
     ev_q.init();
@@ -254,6 +291,7 @@ struct sgs_engine {
     if (n == 0) fail(SGS_ERR_INVALID, "empty graph");
     if (n >= (1u << 27)) fail(SGS_ERR_INVALID, "more than 2^27-1 vertices is not supported");
     queries.clear();
+    groups.clear();
     loaded = false;
     est = sgs_engine_stats{};
     nv = n;
@@ -286,7 +324,7 @@ struct sgs_engine {
     // copy lists
     reset_counters(1);
     FrontierView f0 = fview(0, special(0));
-    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), nullptr, 2, f0);
+    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), f0);
     LoadCsrOp op{view(), d_row, d_col, cfg.weight_mode == SGS_W_EXPLICIT ? d_w : nullptr};
     seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(f0, fview(1, special(1)), op, nullptr);
     CK(cudaGetLastError());
@@ -358,9 +396,14 @@ struct sgs_engine {
   }
 
   void ensure_frontier(uint64_t max_slots) {
-    const uint32_t need_u = (uint32_t)std::min<uint64_t>(max_slots / UNIT + 2, 0xFFFFFFF0ull);
-    for (int i = 0; i < 2; ++i) {
+    // padded ranges: at most 3 extra positions per vertex
+    const uint64_t max_pos = max_slots + 3ull * nv;
+    const uint32_t need_u = (uint32_t)std::min<uint64_t>(max_pos / UNIT + 2, 0xFFFFFFF0ull);
+    for (int i = 0; i < 3; ++i) {
+      gm[i].ensure(nv);
+      CK(cudaMemsetAsync(gm[i].p, 0, sizeof(uint32_t) * nv, s));
       fb[i].vtx.ensure((size_t)nv + 1);
+      fb[i].len.ensure((size_t)nv + 1);
       fb[i].ebase.ensure((size_t)nv + 1);
       if (need_u > ucap) fb[i].ustart.ensure(need_u);
     }
@@ -385,7 +428,7 @@ struct sgs_engine {
     layout_from(slots.p, extra);
     reset_counters(1);
     FrontierView f0 = fview(0, special(0));
-    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), nullptr, 2, f0);
+    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), f0);
     CopyBlockOp op{view(), old_off.p, off.p, od.p, ow.p, oh.p, ohw.p};
     seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(f0, fview(1, special(1)), op, nullptr);
     CK(cudaGetLastError());
@@ -409,80 +452,91 @@ struct sgs_engine {
     }
   }
 
-  // Accounts one timed launch: in = packed input counter of the launch.
-  void account(int kind, unsigned long long in, cudaEvent_t a, cudaEvent_t b) {
+  // Accounts one timed launch: in = packed input counter of the launch,
+  // inst = (instance, edge) pairs it relaxed, per_slot / per_inst = bytes.
+  void account(int kind, unsigned long long in, unsigned long long inst, double per_slot,
+               double per_inst, cudaEvent_t a, cudaEvent_t b) {
     const uint64_t n = in >> CNT_SHIFT, T = in & EDGE_MASK;
     if (!n) return;
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, a, b));
-    static const double per_slot[SGS_K_COUNT] = {16, 12, 12, 12, 20};
     sgs_kernel_stats &k = kst[kind];
     k.launches += 1;
     k.slots += T;
     k.entries += n;
-    k.bytes_alg += per_slot[kind] * (double)T + 20.0 * (double)n;
+    k.bytes_alg += per_slot * (double)T + per_inst * (double)inst + 20.0 * (double)n;
     k.ms += ms;
   }
 
+  // Rounds of a group op from the frontier in buffer 0 / cnt[0] (lane masks in
+  // gm[0]) until a round appends nothing.  Rounds are queued in batches and
+  // the host reads the batch's counters once.  Masks of the last non-empty
+  // frontier are cleared at the end, so all mask buffers are zero again.
   template <class MakeOp>
-  uint32_t run_rounds(MakeOp make_op, unsigned long long *edge_stat, bool &converged,
-                      int kind) {
+  uint32_t run_group_rounds(MakeOp make_op, bool &converged, int kind, double per_slot,
+                            const char *round0 = nullptr) {
     const uint32_t maxr = cfg.max_rounds;
-    uint32_t r = 0;
-    uint32_t rb = 2;
+    uint32_t r = 0, rb = 2;
     converged = false;
-    // empty initial frontier?
+    CK(cudaMemsetAsync(rstat.p, 0, sizeof(unsigned long long) * (maxr + 2), s));
     CK(cudaMemcpyAsync(h_cnt, cnt.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     sync();
     if (h_cnt[0] == 0) { converged = true; return 0; }
+    std::vector<unsigned long long> hr(18);
     while (r < maxr) {
       const uint32_t nb = std::min(rb, maxr - r);
       if (ktiming) ensure_kev(2 * nb);
       for (uint32_t k = 0; k < nb; ++k) {
         const uint32_t rr = r + k;
-        auto op = make_op(rr);
+        auto op = make_op(gm[rr % 3].p, gm[(rr + 1) % 3].p);
+        const bool hp = rr >= 1;
         if (ktiming) CK(cudaEventRecord(kev[2 * k], s));
-        seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(rr, cnt.p + rr), fview(rr + 1, cnt.p + rr + 1),
-                                                     op, edge_stat);
+        if (rr == 0 && round0) nvtxRangePushA(round0);
+        group_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
+            fview(rr, cnt.p + rr), fview(rr + 1, cnt.p + rr + 1), op,
+            hp ? fb[(rr - 1) % 3].vtx.p : nullptr, hp ? cnt.p + rr - 1 : nullptr,
+            hp ? gm[(rr - 1) % 3].p : nullptr, b_lane.p, rstat.p + rr);
+        if (rr == 0 && round0) nvtxRangePop();
         if (ktiming) CK(cudaEventRecord(kev[2 * k + 1], s));
       }
       CK(cudaGetLastError());
-      // counters r .. r+nb: inputs of the queued rounds and the last output
       CK(cudaMemcpyAsync(h_cnt, cnt.p + r, sizeof(unsigned long long) * (nb + 1),
                          cudaMemcpyDeviceToHost, s));
+      if (ktiming)
+        CK(cudaMemcpyAsync(hr.data(), rstat.p + r, sizeof(unsigned long long) * nb,
+                           cudaMemcpyDeviceToHost, s));
       sync();
       if (ktiming)
-        for (uint32_t k = 0; k < nb; ++k) account(kind, h_cnt[k], kev[2 * k], kev[2 * k + 1]);
+        for (uint32_t k = 0; k < nb; ++k)
+          account(kind, h_cnt[k], hr[k], per_slot, 8.0, kev[2 * k], kev[2 * k + 1]);
       for (uint32_t k = 0; k < nb; ++k)
-        if (h_cnt[k + 1] == 0) { converged = true; return r + k + 1; }
+        if (h_cnt[k + 1] == 0) {
+          const uint32_t z = r + k + 1;  // first empty frontier
+          k_clear_masks<<<grid_elem(nv), 256, 0, s>>>(fb[(z - 1) % 3].vtx.p, cnt.p + z - 1,
+                                                      gm[(z - 1) % 3].p);
+          CK(cudaGetLastError());
+          converged = true;
+          return z;
+        }
       r += nb;
       rb = std::min<uint32_t>(rb * 2, 16);
     }
+    // not converged: leave the masks clean for the next call
+    for (uint32_t f = (r >= 1 ? r - 1 : 0); f <= r; ++f)
+      k_clear_masks<<<grid_elem(nv), 256, 0, s>>>(fb[f % 3].vtx.p, cnt.p + f, gm[f % 3].p);
+    CK(cudaGetLastError());
     return r;
   }
 
-  uint32_t next_stamps(Query &q, uint32_t n) {
-    if ((uint64_t)q.stamp + n + 2 >= 0xFFFFFFF0ull) {
-      CK(cudaMemsetAsync(q.mark.p, 0, sizeof(uint32_t) * nv, s));
-      q.stamp = 1;
-    }
-    uint32_t base = q.stamp;
-    q.stamp += n;
-    return base;
-  }
-
-  // Relax from the frontier already in buffer 0 until convergence.
-  uint32_t converge_query(Query &q, unsigned long long *edge_stat, bool &conv) {
-    const uint32_t base = next_stamps(q, cfg.max_rounds + 2);
+  // Relaxation rounds for the lanes whose frontier is in buffer 0.
+  uint32_t group_relax(Group &G, bool &conv, const char *round0 = nullptr) {
     GraphView g = view();
-    if (q.algo == SGS_CC) {
-      return run_rounds([&](uint32_t rr) { return RelaxLabelOp{g, q.st.p, q.mark.p, base + rr + 1}; },
-                        edge_stat, conv, SGS_K_CC);
-    }
-    const int unit = q.algo == SGS_BFS;
-    return run_rounds(
-        [&](uint32_t rr) { return RelaxMinOp{g, q.st.p, q.mark.p, base + rr + 1, unit}; },
-        edge_stat, conv, unit ? SGS_K_BFS : SGS_K_SSSP);
+    const uint32_t anyw = G.any_sssp(G.used | 0xF) && cfg.weight_mode == SGS_W_EXPLICIT;
+    return run_group_rounds(
+        [&](uint32_t *mi, uint32_t *mo) {
+          return GroupRelaxOp<Group::S>{g, G.st.p, G.val.p, mi, mo, G.algo(), anyw};
+        },
+        conv, SGS_K_GROUP, anyw ? 8.0 : 4.0, round0);
   }
 
   // PageRank rounds over the static frontier of all non-empty blocks:
@@ -491,7 +545,7 @@ struct sgs_engine {
   uint32_t pr_rounds(Query &q, unsigned long long *edge_stat, bool &conv, double &last_l1) {
     GraphView g = view();
     reset_counters(0);
-    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(g, nullptr, 2, fview(0, cnt.p));
+    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(g, fview(0, cnt.p));
     const uint32_t maxr = cfg.max_rounds;
     CK(cudaMemsetAsync(l1.p, 0, sizeof(double) * (maxr + 2), s));
     std::vector<double> hl(maxr + 2);
@@ -500,10 +554,9 @@ struct sgs_engine {
     last_l1 = 0;
     PrPushOp op{g, q.pv.p, q.r.p};
     unsigned long long pr_in = 0;
-    if (ktiming) {
-      CK(cudaMemcpyAsync(&pr_in, cnt.p, sizeof(pr_in), cudaMemcpyDeviceToHost, s));
-      sync();
-    }
+    CK(cudaMemcpyAsync(&pr_in, cnt.p, sizeof(pr_in), cudaMemcpyDeviceToHost, s));
+    sync();
+    const unsigned long long pr_inst = (pr_in & EDGE_MASK);
     while (r < maxr) {
       const uint32_t nb = std::min(rb, maxr - r);
       if (ktiming) ensure_kev(2 * nb);
@@ -519,7 +572,8 @@ struct sgs_engine {
       CK(cudaMemcpyAsync(hl.data(), l1.p + r, sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
       sync();
       if (ktiming)
-        for (uint32_t k = 0; k < nb; ++k) account(SGS_K_PR_PUSH, pr_in, kev[2 * k], kev[2 * k + 1]);
+        for (uint32_t k = 0; k < nb; ++k)
+          account(SGS_K_PR_PUSH, pr_in, pr_inst, 4.0, 16.0, kev[2 * k], kev[2 * k + 1]);
       for (uint32_t k = 0; k < nb; ++k) {
         last_l1 = hl[k];
         if (hl[k] < cfg.pr_tol) { conv = true; return r + k + 1; }
@@ -537,36 +591,34 @@ struct sgs_engine {
     fail(SGS_ERR_INVALID, "unknown query id");
   }
 
-  void start_query(Query &q) {
-    GraphView g = view();
-    CK(cudaEventRecord(ev_q.a, s));
-    CK(cudaMemsetAsync(b_stat.p, 0, sizeof(unsigned long long) * 8, s));
-    unsigned long long *es = b_stat.p + 4;
-    bool conv = false;
-    uint32_t rounds = 0;
-    double l1v = 0;
-    if (q.algo == SGS_PR) {
-      k_pr_init<<<grid_elem(nv), 256, 0, s>>>(q.x.p, q.r.p, nv, 1.0 - cfg.pr_alpha);
-      rounds = pr_rounds(q, es, conv, l1v);
-    } else {
-      k_init_state<<<grid_elem(nv), 256, 0, s>>>(q.st.p, nv, q.algo, q.source);
-      reset_counters(0);
-      if (q.algo == SGS_CC) {
-        k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(g, q.st.p, 1, fview(0, cnt.p));
-      } else {
-        uint32_t d = 0;
-        CK(cudaMemcpyAsync(&d, slots.p + q.source, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-        sync();
-        k_append_one<<<1, 32, 0, s>>>(fview(0, cnt.p), q.source, d);
-      }
-      CK(cudaGetLastError());
-      rounds = converge_query(q, es, conv);
+  // Per-lane stats of every query of a group after a group phase.
+  void lane_stats(Group &G, uint32_t rounds, bool conv, float ms, const uint64_t *extra_edges,
+                  const uint64_t *inval) {
+    unsigned long long le[GMAX];
+    CK(cudaMemcpyAsync(le, b_lane.p, sizeof(le), cudaMemcpyDeviceToHost, s));
+    sync();
+    for (auto &q : queries) {
+      if (q->grp != &G) continue;
+      const int l = q->lane;
+      const uint64_t e = le[l] + (extra_edges ? extra_edges[l] : 0);
+      q->stats.edges_traversed = e;
+      q->stats.edges_total += e;
+      q->stats.rounds = rounds;
+      q->stats.converged = conv ? 1 : 0;
+      q->stats.ms = ms;
+      q->stats.pr_residual_l1 = 0;
+      q->stats.invalidated = inval ? inval[l] : 0;
     }
-    CK(cudaEventRecord(ev_q.b, s));
-    finish_stats(q, rounds, conv, l1v, 0);
   }
 
-  void finish_stats(Query &q, uint32_t rounds, bool conv, double l1v, uint64_t inval) {
+  void start_pr(Query &q) {
+    CK(cudaEventRecord(ev_q.a, s));
+    CK(cudaMemsetAsync(b_stat.p, 0, sizeof(unsigned long long) * 8, s));
+    bool conv = false;
+    double l1v = 0;
+    k_pr_init<<<grid_elem(nv), 256, 0, s>>>(q.x.p, q.r.p, nv, 1.0 - cfg.pr_alpha);
+    const uint32_t rounds = pr_rounds(q, b_stat.p + 4, conv, l1v);
+    CK(cudaEventRecord(ev_q.b, s));
     unsigned long long e = 0;
     CK(cudaMemcpyAsync(&e, b_stat.p + 4, sizeof(e), cudaMemcpyDeviceToHost, s));
     sync();
@@ -578,7 +630,39 @@ struct sgs_engine {
     q.stats.converged = conv ? 1 : 0;
     q.stats.ms = ms;
     q.stats.pr_residual_l1 = l1v;
-    q.stats.invalidated = inval;
+    q.stats.invalidated = 0;
+  }
+
+  // Static convergence of one new lane (InitGraph + Start for that query).
+  void start_lane(Query &q) {
+    Group &G = *q.grp;
+    const int l = q.lane;
+    GraphView g = view();
+    CK(cudaEventRecord(ev_q.a, s));
+    CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * GMAX, s));
+    k_group_init_lane<Group::S><<<grid_elem(nv), 256, 0, s>>>(G.st.p, G.val.p, nv, l, q.algo, q.source);
+    reset_counters(0);
+    if (q.algo == SGS_CC)
+      k_group_dense<Group::S><<<grid_elem(nv), 256, 0, s>>>(g, G.val.p, 1u << l, G.algo(), gm[0].p,
+                                                            fview(0, cnt.p));
+    else
+      k_group_seed_one<<<1, 32, 0, s>>>(g, q.source, 1u << l, gm[0].p, fview(0, cnt.p));
+    CK(cudaGetLastError());
+    bool conv = false;
+    const uint32_t rounds = group_relax(G, conv);
+    CK(cudaEventRecord(ev_q.b, s));
+    sync();
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ev_q.a, ev_q.b));
+    unsigned long long le[GMAX];
+    CK(cudaMemcpyAsync(le, b_lane.p, sizeof(le), cudaMemcpyDeviceToHost, s));
+    sync();
+    q.stats.edges_traversed = le[l];
+    q.stats.edges_total += le[l];
+    q.stats.rounds = rounds;
+    q.stats.converged = conv ? 1 : 0;
+    q.stats.ms = ms;
+    q.stats.invalidated = 0;
   }
 
   int add_query(int algo, uint32_t source) {
@@ -593,14 +677,51 @@ struct sgs_engine {
       q->r.ensure(nv);
       q->pv.ensure(nv);
     } else {
-      q->st.ensure(nv);
-      q->mark.ensure(nv);
-      CK(cudaMemsetAsync(q->mark.p, 0, sizeof(uint32_t) * nv, s));
+      // first group with a free lane among the first group_size lanes
+      const uint32_t full = (1u << cfg.group_size) - 1u;
+      Group *G = nullptr;
+      for (auto &gp : groups)
+        if ((gp->used & full) != full) { G = gp.get(); break; }
+      if (!G) {
+        auto ng = std::make_unique<Group>();
+        ng->st.ensure((size_t)nv * Group::S);
+        ng->val.ensure((size_t)nv * Group::S);
+        G = ng.get();
+        groups.push_back(std::move(ng));
+      }
+      int l = 0;
+      while (G->used >> l & 1u) ++l;
+      G->algo_packed = (G->algo_packed & ~(0xFFu << (8 * l))) | ((uint32_t)algo << (8 * l));
+      q->grp = G;
+      q->lane = l;
     }
     Query &ref = *q;
     queries.push_back(std::move(q));
-    start_query(ref);
+    if (algo == SGS_PR) {
+      start_pr(ref);
+    } else {
+      start_lane(ref);
+      ref.grp->used |= 1u << ref.lane;
+    }
     return ref.id;
+  }
+
+  void remove_query(int qid) {
+    for (size_t i = 0; i < queries.size(); ++i)
+      if (queries[i]->id == qid) {
+        sync();
+        Query &q = *queries[i];
+        if (q.grp) q.grp->used &= ~(1u << q.lane);
+        queries.erase(queries.begin() + i);
+        for (size_t j = 0; j < groups.size(); ++j)
+          if (groups[j]->used == 0) {
+            bool ref = false;
+            for (auto &o : queries) ref |= o->grp == groups[j].get();
+            if (!ref) { groups.erase(groups.begin() + j); break; }
+          }
+        return;
+      }
+    fail(SGS_ERR_INVALID, "unknown query id");
   }
 
   // ------------------------------------------------------------ snapshots
@@ -674,102 +795,132 @@ struct sgs_engine {
 
     bool any_pr = false;
     for (auto &q : queries) any_pr |= q->algo == SGS_PR;
-    // per-query timing accumulators
-    std::vector<float> qms(queries.size(), 0.f);
-    std::vector<unsigned long long> qedges(queries.size(), 0);
-    std::vector<uint64_t> qinval(queries.size(), 0);
+    const size_t ng = groups.size();
+    std::vector<float> gms(ng, 0.f);
+    std::vector<std::array<uint64_t, GMAX>> gedges(ng), ginval(ng);
+    for (size_t i = 0; i < ng; ++i) {
+      gedges[i].fill(0);
+      ginval[i].fill(0);
+    }
 
     // ---- PR cancel over the old out-lists of touched sources
     if (any_pr) {
       build_touched(g, ni, nd);
-      for (size_t i = 0; i < queries.size(); ++i) {
-        Query &q = *queries[i];
+      for (auto &qp : queries) {
+        Query &q = *qp;
         if (q.algo != SGS_PR) continue;
         PrAmendOp op{g, q.x.p, q.r.p, -cfg.pr_alpha};
         seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(2)), fview(1, special(3)), op,
                                                      nullptr);
       }
     }
-    // ---- deletion phase: parent-tree invalidation on the old graph
-    for (size_t i = 0; i < queries.size() && nd; ++i) {
-      Query &q = *queries[i];
-      if (q.algo == SGS_PR) continue;
+    // ---- deletion phase: parent-tree invalidation on the old graph, all
+    // lanes of a group together
+    for (size_t i = 0; i < ng && nd; ++i) {
+      Range rg("sgs:invalidate");
+      Group &G = *groups[i];
+      if (!G.used) continue;
       CK(cudaEventRecord(ev_q.a, s));
-      CK(cudaMemsetAsync(b_stat.p + 3, 0, sizeof(unsigned long long) * 2, s));
+      CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * GMAX, s));
+      CK(cudaMemsetAsync(b_inval.p, 0, sizeof(unsigned long long) * GMAX, s));
       reset_counters(0);
-      k_seed_deleted<<<grid_elem(nd), 256, 0, s>>>(g, q.st.p, q.algo == SGS_CC, b_dkeys_s.p,
-                                                   (uint32_t)nd, b_stat.p + 3, fview(0, cnt.p));
+      k_group_seed_deleted<Group::S><<<grid_elem(nd), 256, 0, s>>>(
+          g, G.st.p, G.val.p, G.used, G.algo(), b_dkeys_s.p, (uint32_t)nd, b_inval.p, gm[0].p,
+          fview(0, cnt.p));
+      CK(cudaGetLastError());
       bool conv = false;
-      InvalidateOp base{g, q.st.p, q.algo == SGS_CC, b_stat.p + 3};
-      run_rounds([&](uint32_t) { return base; }, b_stat.p + 4, conv, SGS_K_INVALIDATE);
+      run_group_rounds(
+          [&](uint32_t *mi, uint32_t *mo) {
+            return GroupInvalidateOp<Group::S>{g, G.st.p, G.val.p, mi, mo, G.algo(), b_inval.p};
+          },
+          conv, SGS_K_GROUP_INVAL, 4.0);
       if (!conv) fail(SGS_ERR_NOCONV, "invalidation did not converge");
       CK(cudaEventRecord(ev_q.b, s));
-      unsigned long long hv[2];
-      CK(cudaMemcpyAsync(hv, b_stat.p + 3, sizeof(hv), cudaMemcpyDeviceToHost, s));
+      unsigned long long hv[GMAX], he[GMAX];
+      CK(cudaMemcpyAsync(hv, b_inval.p, sizeof(hv), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(he, b_lane.p, sizeof(he), cudaMemcpyDeviceToHost, s));
       sync();
       float ms = 0;
       CK(cudaEventElapsedTime(&ms, ev_q.a, ev_q.b));
-      qms[i] += ms;
-      qinval[i] = hv[0];
-      qedges[i] += hv[1];
+      gms[i] += ms;
+      for (int q = 0; q < GMAX; ++q) {
+        ginval[i][q] = hv[q];
+        gedges[i][q] = he[q];
+        G.inval[q] = hv[q];
+      }
     }
 
     // ---- graph update
     CK(cudaEventRecord(ev_apply.a, s));
-    apply_graph(ni, nd);
+    {
+      Range rg("sgs:apply_graph");
+      apply_graph(ni, nd);
+    }
     CK(cudaEventRecord(ev_apply.b, s));
     g = view();
 
-    // ---- PR compensate over the new out-lists
+    // ---- PR compensate over the new out-lists, then convergence
     if (any_pr) {
       build_touched(g, ni, nd);
-      for (size_t i = 0; i < queries.size(); ++i) {
-        Query &q = *queries[i];
+      for (auto &qp : queries) {
+        Query &q = *qp;
         if (q.algo != SGS_PR) continue;
         PrAmendOp op{g, q.x.p, q.r.p, cfg.pr_alpha};
         seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(2)), fview(1, special(3)), op,
                                                      nullptr);
       }
-    }
-    // ---- add phase + convergence per query
-    for (size_t i = 0; i < queries.size(); ++i) {
-      Query &q = *queries[i];
-      CK(cudaEventRecord(ev_q.a, s));
-      CK(cudaMemsetAsync(b_stat.p + 4, 0, sizeof(unsigned long long), s));
-      bool conv = false;
-      uint32_t rounds = 0;
-      double l1v = 0;
-      if (q.algo == SGS_PR) {
-        rounds = pr_rounds(q, b_stat.p + 4, conv, l1v);
-      } else {
-        reset_counters(0);
-        const uint32_t st0 = next_stamps(q, 1);
-        if (qinval[i] > 0) {
-          // re-push from every reached vertex (SyncPushDDBAll)
-          k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(g, q.st.p, q.algo == SGS_CC ? 1 : 0,
-                                                         fview(0, cnt.p));
-        } else if (ni) {
-          k_relax_inserted<<<grid_elem(ni), 256, 0, s>>>(g, q.st.p, q.algo, b_ikept.p,
-                                                         explicit_w ? b_iw_kept.p : nullptr,
-                                                         b_nkept.p, q.mark.p, st0, fview(0, cnt.p),
-                                                         b_stat.p + 4);
-        }
-        CK(cudaGetLastError());
-        rounds = converge_query(q, b_stat.p + 4, conv);
+      for (auto &qp : queries) {
+        Query &q = *qp;
+        if (q.algo != SGS_PR) continue;
+        CK(cudaEventRecord(ev_q.a, s));
+        CK(cudaMemsetAsync(b_stat.p + 4, 0, sizeof(unsigned long long), s));
+        bool conv = false;
+        double l1v = 0;
+        const uint32_t rounds = pr_rounds(q, b_stat.p + 4, conv, l1v);
+        CK(cudaEventRecord(ev_q.b, s));
+        unsigned long long e = 0;
+        CK(cudaMemcpyAsync(&e, b_stat.p + 4, sizeof(e), cudaMemcpyDeviceToHost, s));
+        sync();
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev_q.a, ev_q.b));
+        q.stats.edges_traversed = e;
+        q.stats.edges_total += e;
+        q.stats.rounds = rounds;
+        q.stats.converged = conv;
+        q.stats.ms = ms;
+        q.stats.pr_residual_l1 = l1v;
+        q.stats.invalidated = 0;
+        if (!conv) fail(SGS_ERR_NOCONV, "round limit reached before convergence");
       }
+    }
+    // ---- add phase per group: re-push from every reached vertex of every
+    // lane when some lane was invalidated (SyncPushDDBAll), else relax only
+    // the inserted edges; then rounds to convergence
+    for (size_t i = 0; i < ng; ++i) {
+      Group &G = *groups[i];
+      if (!G.used) continue;
+      Range rg("sgs:repair");
+      bool any_inval = false;
+      for (int q = 0; q < GMAX; ++q) any_inval |= (G.used >> q & 1u) && ginval[i][q] > 0;
+      CK(cudaEventRecord(ev_q.a, s));
+      CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * GMAX, s));
+      reset_counters(0);
+      if (any_inval) {
+        k_group_dense<Group::S><<<grid_elem(nv), 256, 0, s>>>(g, G.val.p, G.used, G.algo(), gm[0].p,
+                                                              fview(0, cnt.p));
+      } else if (ni) {
+        k_group_relax_inserted<Group::S><<<grid_elem(ni), 256, 0, s>>>(
+            g, G.st.p, G.val.p, G.used, G.algo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr, b_nkept.p,
+            gm[0].p, fview(0, cnt.p), b_lane.p);
+      }
+      CK(cudaGetLastError());
+      bool conv = false;
+      const uint32_t rounds = group_relax(G, conv, any_inval ? "sgs:sweep" : nullptr);
       CK(cudaEventRecord(ev_q.b, s));
-      unsigned long long e = 0;
-      CK(cudaMemcpyAsync(&e, b_stat.p + 4, sizeof(e), cudaMemcpyDeviceToHost, s));
       sync();
       float ms = 0;
       CK(cudaEventElapsedTime(&ms, ev_q.a, ev_q.b));
-      q.stats.edges_traversed = qedges[i] + e;
-      q.stats.edges_total += qedges[i] + e;
-      q.stats.rounds = rounds;
-      q.stats.converged = conv;
-      q.stats.ms = qms[i] + ms;
-      q.stats.pr_residual_l1 = l1v;
-      q.stats.invalidated = qinval[i];
+      lane_stats(G, rounds, conv, gms[i] + ms, gedges[i].data(), ginval[i].data());
       if (!conv) fail(SGS_ERR_NOCONV, "round limit reached before convergence");
     }
     CK(cudaEventRecord(ev_batch.b, s));
@@ -882,6 +1033,7 @@ struct sgs_engine {
     const cudaMemcpyKind kind = mem == SGS_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     if (q.algo == SGS_PR) {
       if (field == SGS_FIELD_PARENT) fail(SGS_ERR_INVALID, "PageRank has no parent field");
+      if (field != SGS_FIELD_VALUE && field != SGS_FIELD_BUFFER) fail(SGS_ERR_INVALID, "unknown field");
       const double *src = field == SGS_FIELD_VALUE ? q.x.p : q.r.p;
       CK(cudaMemcpyAsync(out, src, sizeof(double) * nv, kind, s));
       sync();
@@ -890,9 +1042,9 @@ struct sgs_engine {
     DBuf<uint32_t> tmp;
     tmp.ensure(nv);
     if (field == SGS_FIELD_PARENT)
-      k_split_state<<<grid_elem(nv), 256, 0, s>>>(q.st.p, nv, nullptr, tmp.p);
+      k_group_split<Group::S><<<grid_elem(nv), 256, 0, s>>>(q.grp->st.p, nv, q.lane, nullptr, tmp.p);
     else if (field == SGS_FIELD_VALUE || field == SGS_FIELD_BUFFER)
-      k_split_state<<<grid_elem(nv), 256, 0, s>>>(q.st.p, nv, tmp.p, nullptr);
+      k_group_split<Group::S><<<grid_elem(nv), 256, 0, s>>>(q.grp->st.p, nv, q.lane, tmp.p, nullptr);
     else
       fail(SGS_ERR_INVALID, "unknown field");
     CK(cudaMemcpyAsync(out, tmp.p, sizeof(uint32_t) * nv, kind, s));
@@ -900,12 +1052,12 @@ struct sgs_engine {
   }
 
   void summary(Query &q, uint64_t out[4]) {
-    b_stat.ensure(8);
     CK(cudaMemsetAsync(b_stat.p, 0, sizeof(unsigned long long) * 4, s));
     if (q.algo == SGS_PR) {
       k_summary_pr<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.x.p, nv, (double *)b_stat.p + 1);
     } else {
-      k_summary<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.st.p, nv, b_stat.p);
+      k_group_summary<Group::S><<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.grp->st.p, nv, q.lane,
+                                                                         b_stat.p);
     }
     CK(cudaGetLastError());
     unsigned long long h[4];
@@ -930,7 +1082,7 @@ struct sgs_engine {
     fill.ensure(nv);
     CK(cudaMemsetAsync(fill.p, 0, sizeof(uint32_t) * nv, s));
     reset_counters(0);
-    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), nullptr, 2, fview(0, special(0)));
+    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), fview(0, special(0)));
     ExportOp op{view(), drow.p, dcol.p, w ? dw.p : nullptr, fill.p};
     seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(0)), fview(1, special(1)), op,
                                                  nullptr);
@@ -1040,6 +1192,7 @@ SGS_API void sgs_config_default(sgs_config *c) {
   c->pr_tol = 1e-6 * 0.15;
   c->slack_div = 8;
   c->arena_headroom = 0.10;
+  c->group_size = 4;
 }
 
 SGS_API int sgs_create(const sgs_config *cfg, sgs_engine **out) {
@@ -1167,15 +1320,7 @@ SGS_API int sgs_query_add(sgs_engine *e, int algo, uint32_t source, int *qid) {
 
 SGS_API int sgs_query_remove(sgs_engine *e, int qid) {
   if (!e) { g_last_error = "null engine"; return SGS_ERR_INVALID; }
-  return guarded([&] {
-    for (size_t i = 0; i < e->queries.size(); ++i)
-      if (e->queries[i]->id == qid) {
-        CK(cudaStreamSynchronize(e->s));
-        e->queries.erase(e->queries.begin() + i);
-        return;
-      }
-    fail(SGS_ERR_INVALID, "unknown query id");
-  });
+  return guarded([&] { e->remove_query(qid); });
 }
 
 SGS_API int sgs_apply_batch(sgs_engine *e, const uint32_t *ins_src, const uint32_t *ins_dst,

@@ -38,7 +38,7 @@ using namespace sgs;
 
 constexpr uint32_t NA_MAX_NV = SGS_NOALLOC_MAX_VERTICES;
 constexpr uint64_t NA_MAX_E = SGS_NOALLOC_MAX_EDGES;
-constexpr uint32_t NA_UNITS = (uint32_t)(NA_MAX_E / UNIT + 2);
+constexpr uint32_t NA_UNITS = (uint32_t)((NA_MAX_E + 3ull * NA_MAX_NV) / UNIT + 2);
 constexpr uint32_t NA_MAX_ROUNDS = 1000;  // the engine's default round limit
 constexpr uint32_t NA_BATCH = 16;
 
@@ -50,7 +50,9 @@ constexpr size_t OFF_VTX0 = al(OFF_MARK + sizeof(uint32_t) * NA_MAX_NV);
 constexpr size_t OFF_VTX1 = al(OFF_VTX0 + sizeof(uint32_t) * NA_MAX_NV);
 constexpr size_t OFF_EB0 = al(OFF_VTX1 + sizeof(uint32_t) * NA_MAX_NV);
 constexpr size_t OFF_EB1 = al(OFF_EB0 + sizeof(uint64_t) * NA_MAX_NV);
-constexpr size_t OFF_US0 = al(OFF_EB1 + sizeof(uint64_t) * NA_MAX_NV);
+constexpr size_t OFF_LEN0 = al(OFF_EB1 + sizeof(uint64_t) * NA_MAX_NV);
+constexpr size_t OFF_LEN1 = al(OFF_LEN0 + sizeof(uint32_t) * NA_MAX_NV);
+constexpr size_t OFF_US0 = al(OFF_LEN1 + sizeof(uint32_t) * NA_MAX_NV);
 constexpr size_t OFF_US1 = al(OFF_US0 + sizeof(uint32_t) * NA_UNITS);
 constexpr size_t OFF_CNT = al(OFF_US1 + sizeof(uint32_t) * NA_UNITS);
 constexpr size_t OFF_ERR = al(OFF_CNT + sizeof(unsigned long long) * (NA_MAX_ROUNDS + 2));
@@ -79,6 +81,7 @@ struct CsrPay {
 // zero weights are recorded in err and skipped.
 struct CsrRelaxOp {
   static constexpr bool kAppends = true;
+  static constexpr bool kQuad = false;
   using Payload = CsrPay;
   const uint64_t *row;
   const uint32_t *col;
@@ -186,6 +189,8 @@ void run(uint32_t nv, const uint64_t *row, const uint32_t *col, const uint32_t *
   f[1].vtx = (uint32_t *)(base + OFF_VTX1);
   f[0].ebase = (uint64_t *)(base + OFF_EB0);
   f[1].ebase = (uint64_t *)(base + OFF_EB1);
+  f[0].len = (uint32_t *)(base + OFF_LEN0);
+  f[1].len = (uint32_t *)(base + OFF_LEN1);
   f[0].ustart = (uint32_t *)(base + OFF_US0);
   f[1].ustart = (uint32_t *)(base + OFF_US1);
   f[0].ucap = f[1].ucap = NA_UNITS;

@@ -57,7 +57,8 @@ struct GraphView {
 
 struct FrontierView {
   uint32_t *vtx;       // [cap] vertex of each entry
-  uint64_t *ebase;     // [cap] exclusive prefix of block sizes
+  uint32_t *len;       // [cap] slots of the entry (its range is padded to 4)
+  uint64_t *ebase;     // [cap] exclusive prefix of padded block sizes
   uint32_t *ustart;    // [ucap] first entry of each UNIT-edge unit
   uint64_t *counter;   // packed (count << 37 | edges)
   uint32_t ucap;
@@ -103,7 +104,8 @@ __device__ __forceinline__ void frontier_append(const FrontierView &f, bool want
   unsigned m = __ballot_sync(full, want);
   if (!m) return;
   const int lane = threadIdx.x & 31;
-  uint64_t inc = want ? ((1ull << CNT_SHIFT) | (uint64_t)d) : 0ull;
+  const uint32_t dp = (d + 3u) & ~3u;  // ranges padded to whole 16-B quads
+  uint64_t inc = want ? ((1ull << CNT_SHIFT) | (uint64_t)dp) : 0ull;
   // inclusive warp scan of inc
   uint64_t x = inc;
 #pragma unroll
@@ -120,13 +122,23 @@ __device__ __forceinline__ void frontier_append(const FrontierView &f, bool want
     uint32_t slot = (uint32_t)((base >> CNT_SHIFT) + (excl >> CNT_SHIFT));
     uint64_t eb = (base & EDGE_MASK) + (excl & EDGE_MASK);
     f.vtx[slot] = v;
+    f.len[slot] = d;
     f.ebase[slot] = eb;
     if (aux) aux[slot] = aux_val;
-    if (d) {
-      uint64_t u0 = (eb + UNIT - 1) / UNIT, u1 = (eb + d - 1) / UNIT;
+    if (dp) {
+      uint64_t u0 = (eb + UNIT - 1) / UNIT, u1 = (eb + dp - 1) / UNIT;
       for (uint64_t u = u0; u <= u1 && u < f.ucap; ++u) f.ustart[u] = slot;
     }
   }
+}
+
+// 16-B read-only load of four consecutive u32 slots (block starts and j0 are
+// multiples of 4 elements, so the address is 16-B aligned).
+__device__ __forceinline__ uint4 ld_quad(const uint32_t *p) {
+  return __ldg(reinterpret_cast<const uint4 *>(p));
+}
+__device__ __forceinline__ uint32_t quad_at(const uint4 &q, int k) {
+  return k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w;
 }
 
 // Block-wide helpers --------------------------------------------------------

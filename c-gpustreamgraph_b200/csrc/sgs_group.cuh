@@ -1,0 +1,489 @@
+// sgs_group.cuh -- query groups: up to GMAX integer queries (BFS / SSSP / CC,
+// any sources) relaxed together over one edge stream.
+//
+// Layout: st[v * S + lane] u64 packed (value << 32 | parent), S = 1, 2 or 4,
+// so one vertex's states share one 32-B sector and a random access to a
+// destination serves every lane.  Lane masks mask[k][v] (u32, three rotating
+// buffers) record which lanes improved v in a round; the thread whose
+// atomicOr turns the mask non-zero appends v, which replaces per-query
+// de-duplication stamps.  Round r reads mask[r%3], writes mask[(r+1)%3] and
+// clears the masks of frontier r-1 in mask[(r+2)%3], which round r+1 writes
+// next; frontier buffers rotate the same way, so no grid barrier is needed.
+//
+// Reference semantics per lane are those of the single-query ops
+// (hybrid_sssp.cu:97-118 min relaxation, hybrid_cc.cu:96-110 label
+// propagation, reset_del_edges / SyncPushDDB_del parent-tree invalidation,
+// driver.cuh:398-430 and :1985-2031).
+#pragma once
+#include "sgs_device.cuh"
+#include "sgs_segmap.cuh"
+
+namespace sgs {
+
+constexpr int GMAX = 4;
+constexpr int GCHUNK = 512;  // entries staged per chunk by group_map
+
+struct LaneAlgo {
+  uint32_t packed;  // 8 bits per lane: A_BFS / A_SSSP / A_CC
+  __device__ __forceinline__ int at(int q) const { return (packed >> (8 * q)) & 0xFF; }
+};
+
+template <int S>
+struct GPay {
+  uint64_t off;
+  uint32_t mask;
+  uint32_t val[S];
+};
+
+// S u32 values of vertex v (one 16-B load for S = 4).
+template <int S>
+__device__ __forceinline__ void load_vals(const uint32_t *val, uint32_t v, uint32_t (&o)[S]) {
+  if constexpr (S == 4) {
+    const uint4 x = __ldcg(reinterpret_cast<const uint4 *>(val + (uint64_t)v * 4));
+    o[0] = x.x; o[1] = x.y; o[2] = x.z; o[3] = x.w;
+  } else if constexpr (S == 2) {
+    const uint2 x = __ldcg(reinterpret_cast<const uint2 *>(val + (uint64_t)v * 2));
+    o[0] = x.x; o[1] = x.y;
+  } else {
+    o[0] = __ldcg(val + v);
+  }
+}
+
+// Clears the masks of the previous frontier (grid-stride, all threads).
+__device__ __forceinline__ void clear_prev_masks(const uint32_t *vtx, const unsigned long long *cnt,
+                                                 uint32_t *mask) {
+  if (!cnt) return;
+  const uint32_t n = (uint32_t)(__ldcg(cnt) >> CNT_SHIFT);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    mask[__ldcg(&vtx[i])] = 0;
+}
+
+// Relaxation of every active lane of every source over its out-edges.  The
+// u32 mirror `val` filters candidates with one 16-B read per destination; the
+// packed (value,parent) word is touched only by the atomic of a strict
+// improvement, after which the mirror is lowered too (it never drops below
+// the packed value, so the filter never rejects a real improvement).
+template <int S>
+struct GroupRelaxOp {
+  using Payload = GPay<S>;
+  GraphView g;
+  unsigned long long *st;
+  uint32_t *val;
+  const uint32_t *m_in;
+  uint32_t *m_out;
+  LaneAlgo algo;
+  uint32_t any_w;  // some lane reads stored weights
+  __device__ __forceinline__ Payload load(uint32_t v) const {
+    Payload p;
+    p.off = g.off[v];
+    p.mask = __ldcg(&m_in[v]);
+    load_vals<S>(val, v, p.val);
+    return p;
+  }
+  // Returns a 4-bit mask of destinations to append; dst[] holds them.
+  __device__ __forceinline__ uint32_t visit4(uint32_t u, const Payload &p, uint32_t j0, uint32_t len,
+                                             uint32_t (&dst)[4]) const {
+    const uint4 ids = ld_quad(adj_ptr(g, p.off) + j0);
+    const uint4 ws = any_w ? ld_quad(wgt_ptr(g, p.off) + j0) : make_uint4(1, 1, 1, 1);
+    uint32_t okm = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      dst[k] = quad_at(ids, k);
+      if (j0 + k < len && dst[k] != SGS_TOMB) okm |= 1u << k;
+    }
+    uint32_t cur[4][S];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (okm >> k & 1u) load_vals<S>(val, dst[k], cur[k]);
+    uint32_t app = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (!(okm >> k & 1u)) continue;
+      uint32_t bits = 0;
+#pragma unroll
+      for (int q = 0; q < S; ++q) {
+        if (!(p.mask >> q & 1u)) continue;
+        const int a = algo.at(q);
+        uint32_t cand;
+        if (a == A_CC) {
+          cand = p.val[q];
+        } else {
+          if (p.val[q] == INF32) continue;
+          uint32_t w = 1u;
+          if (a == A_SSSP)
+            w = g.wmode == W_EXPLICIT ? quad_at(ws, k)
+                : g.wmode == W_SYNTH  ? (u + dst[k]) % 128u + 1u
+                                      : 1u;
+          const uint64_t nd = (uint64_t)p.val[q] + w;
+          if (nd >= INF32) continue;
+          cand = (uint32_t)nd;
+        }
+        if (cand >= cur[k][q]) continue;
+        const uint64_t idx = (uint64_t)dst[k] * S + q;
+        const unsigned long long old = atomicMin(&st[idx], ((unsigned long long)cand << 32) | u);
+        if (cand < (uint32_t)(old >> 32)) {
+          atomicMin(&val[idx], cand);
+          bits |= 1u << q;
+        }
+      }
+      if (bits && g.slots[dst[k]] && atomicOr(&m_out[dst[k]], bits) == 0u) app |= 1u << k;
+    }
+    return app;
+  }
+};
+
+// Parent-tree invalidation per lane: a child whose lane-q parent is u (and u
+// was reset in lane q) is reset exactly once (CAS on the packed word); the
+// mirror is reset with it.
+template <int S>
+struct GroupInvalidateOp {
+  struct Payload {
+    uint64_t off;
+    uint32_t mask;
+    uint32_t pad;
+  };
+  GraphView g;
+  unsigned long long *st;
+  uint32_t *val;
+  const uint32_t *m_in;
+  uint32_t *m_out;
+  LaneAlgo algo;
+  unsigned long long *inval;  // [GMAX] per-lane reset counts
+  __device__ __forceinline__ Payload load(uint32_t v) const {
+    Payload p;
+    p.off = g.off[v];
+    p.mask = __ldcg(&m_in[v]);
+    p.pad = 0;
+    return p;
+  }
+  __device__ __forceinline__ uint32_t visit4(uint32_t u, const Payload &p, uint32_t j0, uint32_t len,
+                                             uint32_t (&dst)[4]) const {
+    const uint4 ids = ld_quad(adj_ptr(g, p.off) + j0);
+    uint32_t okm = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      dst[k] = quad_at(ids, k);
+      if (j0 + k < len && dst[k] != SGS_TOMB) okm |= 1u << k;
+    }
+    uint32_t app = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (!(okm >> k & 1u)) continue;
+      uint32_t bits = 0;
+#pragma unroll
+      for (int q = 0; q < S; ++q) {
+        if (!(p.mask >> q & 1u)) continue;
+        const uint64_t idx = (uint64_t)dst[k] * S + q;
+        const unsigned long long cu = __ldcg(&st[idx]);
+        if ((uint32_t)cu != u) continue;
+        const bool cc = algo.at(q) == A_CC;
+        const unsigned long long rst = cc ? (((unsigned long long)dst[k] << 32) | INF32) : ~0ull;
+        if (atomicCAS(&st[idx], cu, rst) == cu) {
+          val[idx] = cc ? dst[k] : INF32;
+          bits |= 1u << q;
+          atomicAdd(&inval[q], 1ull);
+        }
+      }
+      if (bits && g.slots[dst[k]] && atomicOr(&m_out[dst[k]], bits) == 0u) app |= 1u << k;
+    }
+    return app;
+  }
+};
+
+// Load-balanced map for group ops (same unit/chunk scheme as seg_map).
+// Edges are attributed per entry: the CTA whose range holds an entry's first
+// position adds live[v] for every lane of its mask, which counts exactly the
+// (query, edge) pairs relaxed.  The kernel also clears the previous
+// frontier's masks.
+template <class Op>
+__global__ void __launch_bounds__(RELAX_THREADS, 5)
+    group_map(FrontierView in, FrontierView out, Op op, const uint32_t *prev_vtx,
+              const unsigned long long *prev_cnt, uint32_t *prev_mask,
+              unsigned long long *lane_edges, unsigned long long *edge_stat) {
+  using P = typename Op::Payload;
+  constexpr int GC = GCHUNK;
+  __shared__ uint64_t s_eb[GC + 1];
+  __shared__ uint32_t s_len[GC];
+  __shared__ P s_pay[GC];
+  __shared__ uint32_t s_vtx[GC];
+  __shared__ unsigned long long s_lane[GMAX];
+  clear_prev_masks(prev_vtx, prev_cnt, prev_mask);
+  if (threadIdx.x < GMAX) s_lane[threadIdx.x] = 0;
+  uint32_t lane_acc[GMAX] = {0, 0, 0, 0};  // (query, edge) pairs of owned entries
+  const uint64_t packed = __ldcg((const unsigned long long *)in.counter);
+  const uint32_t n = (uint32_t)(packed >> CNT_SHIFT);
+  const uint64_t T = packed & EDGE_MASK;
+  const uint64_t nunits = (T + UNIT - 1) / UNIT;
+  const uint64_t ub = (uint64_t)blockIdx.x * nunits / gridDim.x;
+  const uint64_t ue = (uint64_t)(blockIdx.x + 1) * nunits / gridDim.x;
+  if (n != 0 && ub < ue) {
+    const uint64_t E0 = ub * UNIT;
+    const uint64_t E1 = min(ue * (uint64_t)UNIT, T);
+    uint32_t s = __ldcg(&in.ustart[ub]);
+    for (;;) {
+      __syncthreads();
+#pragma unroll
+      for (int h = 0; h < GC / RELAX_THREADS; ++h) {
+        const uint32_t t = threadIdx.x + h * RELAX_THREADS;
+        const uint32_t idx = s + t;
+        const uint64_t eb = idx < n ? __ldcg((const unsigned long long *)&in.ebase[idx]) : T;
+        s_eb[t] = eb;
+        if (t == 0) {
+          const uint32_t j = s + GC;
+          s_eb[GC] = j < n ? __ldcg((const unsigned long long *)&in.ebase[j]) : T;
+        }
+        if (idx < n && eb < E1) {
+          const uint32_t v = __ldcg(&in.vtx[idx]);
+          s_vtx[t] = v;
+          s_len[t] = __ldcg(&in.len[idx]);
+          const P pay = op.load(v);
+          s_pay[t] = pay;
+          if (eb >= E0 && pay.mask) {
+            const uint32_t l = op.g.live[v];
+#pragma unroll
+            for (int q = 0; q < GMAX; ++q) lane_acc[q] += (pay.mask >> q & 1u) ? l : 0u;
+          }
+        }
+      }
+      __syncthreads();
+      const uint64_t lo = max(E0, s_eb[0]);
+      const uint64_t hi = min(E1, s_eb[GC]);
+      for (uint64_t base = lo; base < hi; base += 4 * RELAX_THREADS) {
+        const uint64_t e = base + 4 * threadIdx.x;
+        uint32_t app = 0;
+        uint32_t dst[4] = {0, 0, 0, 0};
+        if (e < hi) {
+          int l = 0, r = GC - 1;
+          while (l < r) {
+            const int m = (l + r + 1) >> 1;
+            if (s_eb[m] <= e) l = m;
+            else r = m - 1;
+          }
+          const uint32_t j0 = (uint32_t)(e - s_eb[l]);
+          if (j0 < s_len[l]) app = op.visit4(s_vtx[l], s_pay[l], j0, s_len[l], dst);
+        }
+        if (__ballot_sync(0xFFFFFFFFu, app != 0u)) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const bool w = app >> k & 1u;
+            frontier_append(out, w, dst[k], w ? op.g.slots[dst[k]] : 0u);
+          }
+        }
+      }
+      if (s_eb[GC] >= E1 || s + GC >= n) break;
+      s += GC;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < GMAX; ++q) {
+    const unsigned long long x = warp_sum((unsigned long long)lane_acc[q]);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(&s_lane[q], x);
+  }
+  __syncthreads();
+  if (threadIdx.x < GMAX && s_lane[threadIdx.x]) {
+    if (lane_edges) atomicAdd(&lane_edges[threadIdx.x], s_lane[threadIdx.x]);
+    if (edge_stat) atomicAdd(edge_stat, s_lane[threadIdx.x]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Group frontier builders
+// ---------------------------------------------------------------------------
+template <int S>
+__global__ void k_group_init_lane(unsigned long long *st, uint32_t *val, uint32_t nv, int lane,
+                                  int algo, uint32_t source) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride) {
+    unsigned long long s;
+    if (algo == A_CC) s = (v << 32) | INF32;
+    else s = v == source ? (unsigned long long)INF32 : ~0ull;
+    st[v * S + lane] = s;
+    val[v * S + lane] = (uint32_t)(s >> 32);
+  }
+}
+
+// Every vertex with a non-empty block; mask = selected lanes whose value is
+// finite there (CC lanes always).  One writer per vertex: plain stores.
+template <int S>
+__global__ void k_group_dense(GraphView g, const uint32_t *val, uint32_t lanes,
+                              LaneAlgo algo, uint32_t *m_out, FrontierView out) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < g.nv; b += stride) {
+    const uint64_t v = b + threadIdx.x;
+    bool want = false;
+    uint32_t d = 0;
+    if (v < g.nv) {
+      d = g.slots[v];
+      if (d) {
+        uint32_t blk[S];
+        load_vals<S>(val, (uint32_t)v, blk);
+        uint32_t m = 0;
+#pragma unroll
+        for (int q = 0; q < S; ++q)
+          if ((lanes >> q & 1u) && (algo.at(q) == A_CC || blk[q] != INF32)) m |= 1u << q;
+        if (m) {
+          m_out[v] = m;
+          want = true;
+        }
+      }
+    }
+    frontier_append(out, want, (uint32_t)v, d);
+  }
+}
+
+// One vertex, given lanes (the source of new BFS/SSSP lanes).
+__global__ void k_group_seed_one(GraphView g, uint32_t v, uint32_t bits, uint32_t *m_out,
+                                 FrontierView out) {
+  if (threadIdx.x >= 32) return;
+  const uint32_t d = g.slots[v];
+  bool want = false;
+  if (threadIdx.x == 0 && d) want = atomicOr(&m_out[v], bits) == 0u;
+  frontier_append(out, want, v, d);
+}
+
+// Deletion seeds: deleted (u,v) whose lane-q parent of v is u reset lane q.
+template <int S>
+__global__ void k_group_seed_deleted(GraphView g, unsigned long long *st, uint32_t *val, uint32_t lanes,
+                                     LaneAlgo algo, const uint64_t *keys, uint32_t n,
+                                     unsigned long long *inval, uint32_t *m_out, FrontierView out) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < n; b += stride) {
+    const uint64_t i = b + threadIdx.x;
+    bool want = false;
+    uint32_t v = 0, d = 0;
+    if (i < n) {
+      const uint64_t k = keys[i];
+      const uint32_t u = (uint32_t)(k >> 32);
+      v = (uint32_t)k;
+      uint32_t bits = 0;
+#pragma unroll
+      for (int q = 0; q < S; ++q) {
+        if (!(lanes >> q & 1u)) continue;
+        const uint64_t idx = (uint64_t)v * S + q;
+        const unsigned long long cu = __ldcg(&st[idx]);
+        if ((uint32_t)cu != u) continue;
+        const bool cc = algo.at(q) == A_CC;
+        const unsigned long long rst = cc ? (((unsigned long long)v << 32) | INF32) : ~0ull;
+        if (atomicCAS(&st[idx], cu, rst) == cu) {
+          val[idx] = cc ? v : INF32;
+          bits |= 1u << q;
+          atomicAdd(&inval[q], 1ull);
+        }
+      }
+      if (bits) {
+        d = g.slots[v];
+        want = d && atomicOr(&m_out[v], bits) == 0u;
+      }
+    }
+    frontier_append(out, want, v, d);
+  }
+}
+
+// Insert-only fast path: relax just the kept inserted edges in the selected
+// lanes.
+template <int S>
+__global__ void k_group_relax_inserted(GraphView g, unsigned long long *st, uint32_t *val, uint32_t lanes,
+                                       LaneAlgo algo, const uint64_t *keys, const uint32_t *w,
+                                       const uint32_t *n_ptr, uint32_t *m_out, FrontierView out,
+                                       unsigned long long *lane_edges) {
+  const uint32_t n = *n_ptr;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint32_t counted = 0;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < n; b += stride) {
+    const uint64_t i = b + threadIdx.x;
+    bool want = false;
+    uint32_t v = 0, d = 0;
+    if (i < n) {
+      const uint64_t k = keys[i];
+      const uint32_t u = (uint32_t)(k >> 32);
+      v = (uint32_t)k;
+      ++counted;
+      uint32_t su[S], sv[S];
+      load_vals<S>(val, u, su);
+      load_vals<S>(val, v, sv);
+      uint32_t bits = 0;
+#pragma unroll
+      for (int q = 0; q < S; ++q) {
+        if (!(lanes >> q & 1u)) continue;
+        const int a = algo.at(q);
+        uint32_t cand;
+        if (a == A_CC) {
+          cand = su[q];
+        } else {
+          if (su[q] == INF32) continue;
+          uint32_t wt = 1;
+          if (a == A_SSSP)
+            wt = g.wmode == W_EXPLICIT ? w[i] : g.wmode == W_SYNTH ? (u + v) % 128u + 1u : 1u;
+          const uint64_t nd = (uint64_t)su[q] + wt;
+          if (nd >= INF32) continue;
+          cand = (uint32_t)nd;
+        }
+        if (cand >= sv[q]) continue;
+        const uint64_t idx = (uint64_t)v * S + q;
+        const unsigned long long old = atomicMin(&st[idx], ((unsigned long long)cand << 32) | u);
+        if (cand < (uint32_t)(old >> 32)) {
+          atomicMin(&val[idx], cand);
+          bits |= 1u << q;
+        }
+      }
+      if (bits) {
+        d = g.slots[v];
+        want = d && atomicOr(&m_out[v], bits) == 0u;
+      }
+    }
+    frontier_append(out, want, v, d);
+  }
+  if (counted) {
+#pragma unroll
+    for (int q = 0; q < S; ++q)
+      if (lanes >> q & 1u) atomicAdd(&lane_edges[q], (unsigned long long)counted);
+  }
+}
+
+template <int S>
+__global__ void k_group_split(const unsigned long long *st, uint32_t nv, int lane, uint32_t *val,
+                              uint32_t *par) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride) {
+    const unsigned long long s = st[v * S + lane];
+    if (val) val[v] = (uint32_t)(s >> 32);
+    if (par) par[v] = (uint32_t)s;
+  }
+}
+
+template <int S>
+__global__ void k_group_summary(const unsigned long long *st, uint32_t nv, int lane,
+                                unsigned long long *out) {
+  unsigned long long reached = 0, sum = 0, mx = 0, psum = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride) {
+    const unsigned long long s = st[v * S + lane];
+    const uint32_t val = (uint32_t)(s >> 32);
+    if (val == INF32) continue;
+    reached += 1;
+    sum += val;
+    mx = val > mx ? val : mx;
+    if ((uint32_t)s != INF32) psum += (uint32_t)s;
+  }
+  reached = warp_sum(reached);
+  sum = warp_sum(sum);
+  psum = warp_sum(psum);
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    const unsigned long long o = __shfl_xor_sync(0xFFFFFFFFu, mx, s);
+    mx = o > mx ? o : mx;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (reached) atomicAdd(&out[0], reached);
+    if (sum) atomicAdd(&out[1], sum);
+    atomicMax(&out[2], mx);
+    if (psum) atomicAdd(&out[3], psum);
+  }
+}
+
+// Masks of the last non-empty frontier (after convergence).
+__global__ void k_clear_masks(const uint32_t *vtx, const unsigned long long *cnt, uint32_t *mask) {
+  clear_prev_masks(vtx, cnt, mask);
+}
+
+}  // namespace sgs

@@ -2,20 +2,18 @@
 //
 // Reference behaviour each kernel re-implements (paths relative to the
 // reference project):
-//   seg_map + RelaxOp     <- kernel::SyncPushDDBDelta / RelaxCTADB /
+//   seg_map (sgs_segmap.cuh) and the group ops (sgs_group.cuh)
+//                         <- kernel::SyncPushDDBDelta / RelaxCTADB /
 //                            CTAWorkSchedulerNew / PushFunctorDB
 //                            (variants/driver.cuh:1893-1935,
 //                             variants/sync_push_dd.cuh:170-268,
 //                             groute/device/cta_scheduler_hybrid.cuh:59-245,
-//                             variants/push_functor.h:252-321)
+//                             variants/push_functor.h:252-321), the deletion
+//                            phase reset_del_edges + SyncPushDDB_del
+//                            (driver.cuh:398-430, :1985-2031) and the
+//                            all-vertices re-push SyncPushDDBAll (:1727-1761)
 //   frontier_append       <- RebuildWorklist* + dev::Queue::append
 //                            (driver.cuh:654-909, groute/device/queue.cuh:84-88)
-//   InvalidateOp, k_seed_deleted
-//                         <- reset_del_edges + SyncPushDDB_del
-//                            (driver.cuh:398-430, :1985-2031,
-//                             hybrid_sssp.cu:154-167)
-//   k_dense_frontier      <- RebuildWorklist_AllVertices + SyncPushDDBAll
-//                            (driver.cuh:704-720, :1727-1761)
 //   PR absorb/push/amend  <- hybrid_pr.cu:66-122 CombineValueBuffer /
 //                            CombineValueBufferAmend / AccumulateBuffer and
 //                            SyncPushDDBAmend (driver.cuh:1770-1804)
@@ -33,128 +31,6 @@ namespace sgs {
 // ---------------------------------------------------------------------------
 // Ops
 // ---------------------------------------------------------------------------
-struct SrcPay {
-  uint64_t off;
-  uint32_t val;
-  uint32_t pad;
-};
-
-// BFS / SSSP relaxation on packed (value,parent): atomicMin keeps value and
-// parent consistent; the parent is the smallest-id tight predecessor at the
-// fixed point (deterministic).  A vertex is re-activated only when its value
-// strictly drops (hybrid_sssp.cu:97-118 semantics).
-struct RelaxMinOp {
-  static constexpr bool kAppends = true;
-  using Payload = SrcPay;
-  GraphView g;
-  unsigned long long *st;
-  uint32_t *mark;
-  uint32_t stamp;
-  int unit_weight;  // BFS
-  __device__ __forceinline__ Payload load(uint32_t, uint32_t v) const {
-    SrcPay p;
-    p.off = g.off[v];
-    p.val = (uint32_t)(__ldcg(&st[v]) >> 32);
-    p.pad = 0;
-    return p;
-  }
-  __device__ __forceinline__ uint32_t visit(uint32_t u, const Payload &p, uint32_t j,
-                                            bool &app, uint32_t &av,
-                                            uint32_t &ad) const {
-    const uint32_t dst = adj_ptr(g, p.off)[j];
-    if (dst == SGS_TOMB) return 0;
-    if (p.val == INF32) return 1;
-    const uint32_t w = unit_weight ? 1u : edge_weight(g, p.off, j, u, dst);
-    const uint64_t nd = (uint64_t)p.val + w;
-    if (nd >= INF32) return 1;
-    const unsigned long long np = ((unsigned long long)nd << 32) | u;
-    if (np >= __ldcg(&st[dst])) return 1;
-    const unsigned long long old = atomicMin(&st[dst], np);
-    if (nd < (old >> 32)) {
-      if (__ldcg(&mark[dst]) != stamp && atomicExch(&mark[dst], stamp) != stamp) {
-        const uint32_t d = g.slots[dst];
-        if (d) { app = true; av = dst; ad = d; }
-      }
-    }
-    return 1;
-  }
-};
-
-// Directed min-label propagation (hybrid_cc.cu:96-110).  Only a strictly
-// smaller label is accepted (CAS), so the parent of v is the vertex that
-// delivered v's current label first; parent chains are then acyclic.
-struct RelaxLabelOp {
-  static constexpr bool kAppends = true;
-  using Payload = SrcPay;
-  GraphView g;
-  unsigned long long *st;
-  uint32_t *mark;
-  uint32_t stamp;
-  __device__ __forceinline__ Payload load(uint32_t, uint32_t v) const {
-    SrcPay p;
-    p.off = g.off[v];
-    p.val = (uint32_t)(__ldcg(&st[v]) >> 32);
-    p.pad = 0;
-    return p;
-  }
-  __device__ __forceinline__ uint32_t visit(uint32_t u, const Payload &p, uint32_t j,
-                                            bool &app, uint32_t &av,
-                                            uint32_t &ad) const {
-    const uint32_t dst = adj_ptr(g, p.off)[j];
-    if (dst == SGS_TOMB) return 0;
-    const uint32_t L = p.val;
-    unsigned long long cur = __ldcg(&st[dst]);
-    while ((uint32_t)(cur >> 32) > L) {
-      const unsigned long long nw = ((unsigned long long)L << 32) | u;
-      const unsigned long long old = atomicCAS(&st[dst], cur, nw);
-      if (old == cur) {
-        if (__ldcg(&mark[dst]) != stamp && atomicExch(&mark[dst], stamp) != stamp) {
-          const uint32_t d = g.slots[dst];
-          if (d) { app = true; av = dst; ad = d; }
-        }
-        break;
-      }
-      cur = old;
-    }
-    return 1;
-  }
-};
-
-// Parent-tree invalidation: a child whose parent is an invalidated vertex is
-// reset (to INF, or to its own id for CC) exactly once (CAS on the packed
-// word), which also makes the appended frontier duplicate-free.
-struct InvalidateOp {
-  static constexpr bool kAppends = true;
-  using Payload = SrcPay;
-  GraphView g;
-  unsigned long long *st;
-  int cc;
-  unsigned long long *n_inval;
-  __device__ __forceinline__ Payload load(uint32_t, uint32_t v) const {
-    SrcPay p;
-    p.off = g.off[v];
-    p.val = 0;
-    p.pad = 0;
-    return p;
-  }
-  __device__ __forceinline__ uint32_t visit(uint32_t u, const Payload &p, uint32_t j,
-                                            bool &app, uint32_t &av,
-                                            uint32_t &ad) const {
-    const uint32_t dst = adj_ptr(g, p.off)[j];
-    if (dst == SGS_TOMB) return 0;
-    const unsigned long long cur = __ldcg(&st[dst]);
-    if ((uint32_t)cur != u) return 1;
-    const unsigned long long rst =
-        cc ? (((unsigned long long)dst << 32) | INF32) : ~0ull;
-    if (atomicCAS(&st[dst], cur, rst) == cur) {
-      atomicAdd(n_inval, 1ull);
-      const uint32_t d = g.slots[dst];
-      if (d) { app = true; av = dst; ad = d; }
-    }
-    return 1;
-  }
-};
-
 // PageRank push of a per-source scalar (absorbed residual or +-alpha*x/deg).
 struct PrPay {
   uint64_t off;
@@ -162,6 +38,7 @@ struct PrPay {
 };
 struct PrPushOp {
   static constexpr bool kAppends = false;
+  static constexpr bool kQuad = true;
   using Payload = PrPay;
   GraphView g;
   const double *pv;   // per-vertex push value (alpha * r / outdeg)
@@ -179,11 +56,25 @@ struct PrPushOp {
     if (p.c != 0.0) atomicAdd(&r[dst], p.c);
     return 1;
   }
+  __device__ __forceinline__ uint32_t visit4(uint32_t, const Payload &p, uint32_t j0, uint32_t len,
+                                             bool (&)[4], uint32_t (&)[4], uint32_t (&)[4]) const {
+    const uint4 ids = ld_quad(adj_ptr(g, p.off) + j0);
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t dst = quad_at(ids, k);
+      if (j0 + k >= len || dst == SGS_TOMB) continue;
+      ++c;
+      if (p.c != 0.0) atomicAdd(&r[dst], p.c);
+    }
+    return c;
+  }
 };
 // Cancel (sign=-1, old graph) / compensate (sign=+1, new graph) of
 // hybrid_pr.cu:88-106, restricted to sources whose out-edges changed.
 struct PrAmendOp {
   static constexpr bool kAppends = false;
+  static constexpr bool kQuad = false;
   using Payload = PrPay;
   GraphView g;
   const double *x;
@@ -213,6 +104,7 @@ struct GroupPay {
 };
 struct TombOp {
   static constexpr bool kAppends = false;
+  static constexpr bool kQuad = false;
   using Payload = GroupPay;
   GraphView g;
   const uint64_t *keys;   // sorted delete keys (src<<32|dst)
@@ -262,6 +154,7 @@ struct CopyPay {
 };
 struct CopyBlockOp {
   static constexpr bool kAppends = false;
+  static constexpr bool kQuad = false;
   using Payload = CopyPay;
   GraphView g;
   const uint64_t *from_off;  // per vertex: old offset (tier bit included)
@@ -287,6 +180,7 @@ struct CopyBlockOp {
 // Copy an input CSR (device arrays) into the arena blocks.
 struct LoadCsrOp {
   static constexpr bool kAppends = false;
+  static constexpr bool kQuad = false;
   using Payload = CopyPay;
   GraphView g;
   const uint64_t *row;
@@ -317,6 +211,7 @@ struct ExportPay {
 };
 struct ExportOp {
   static constexpr bool kAppends = false;
+  static constexpr bool kQuad = false;
   using Payload = ExportPay;
   GraphView g;
   const uint64_t *row_out;
@@ -350,11 +245,8 @@ __global__ void k_append_one(FrontierView out, uint32_t v, uint32_t d) {
   frontier_append(out, threadIdx.x == 0 && d > 0, v, d);
 }
 
-// Every vertex whose value is finite (all vertices for CC) and whose block is
-// non-empty: the all-vertices re-push after a batch (SyncPushDDBAll).
-__global__ void k_dense_frontier(GraphView g, const unsigned long long *st,
-                                 int mode /*0: st finite, 1: all, 2: slots only*/,
-                                 FrontierView out) {
+// Every vertex with a non-empty block (PageRank rounds, loads, repacks).
+__global__ void k_dense_frontier(GraphView g, FrontierView out) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < g.nv; b += stride) {
     const uint64_t v = b + threadIdx.x;
@@ -363,112 +255,8 @@ __global__ void k_dense_frontier(GraphView g, const unsigned long long *st,
     if (v < g.nv) {
       d = g.slots[v];
       want = d > 0;
-      if (want && mode == 0) want = (uint32_t)(__ldcg(&st[v]) >> 32) != INF32;
     }
     frontier_append(out, want, (uint32_t)v, d);
-  }
-}
-
-// Seeds of the deletion phase: deleted (u,v) with parent[v]==u resets v
-// (reset_del_edges, driver.cuh:398-430).
-__global__ void k_seed_deleted(GraphView g, unsigned long long *st, int cc,
-                               const uint64_t *keys, uint32_t n,
-                               unsigned long long *n_inval, FrontierView out) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < n; b += stride) {
-    const uint64_t i = b + threadIdx.x;
-    bool want = false;
-    uint32_t v = 0, d = 0;
-    if (i < n) {
-      const uint64_t k = keys[i];
-      const uint32_t u = (uint32_t)(k >> 32);
-      v = (uint32_t)k;
-      const unsigned long long cur = __ldcg(&st[v]);
-      if ((uint32_t)cur == u) {
-        const unsigned long long rst = cc ? (((unsigned long long)v << 32) | INF32) : ~0ull;
-        if (atomicCAS(&st[v], cur, rst) == cur) {
-          atomicAdd(n_inval, 1ull);
-          d = g.slots[v];
-          want = d > 0;
-        }
-      }
-    }
-    frontier_append(out, want, v, d);
-  }
-}
-
-// Relax only the inserted edges (no invalidation happened): the insert-only
-// fast path of the add phase.
-__global__ void k_relax_inserted(GraphView g, unsigned long long *st, int algo,
-                                 const uint64_t *keys, const uint32_t *w,
-                                 const uint32_t *n_ptr, uint32_t *mark,
-                                 uint32_t stamp, FrontierView out,
-                                 unsigned long long *edge_stat) {
-  const uint32_t n = *n_ptr;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  uint64_t counted = 0;
-  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < n; b += stride) {
-    const uint64_t i = b + threadIdx.x;
-    bool want = false;
-    uint32_t v = 0, d = 0;
-    if (i < n) {
-      const uint64_t k = keys[i];
-      const uint32_t u = (uint32_t)(k >> 32);
-      v = (uint32_t)k;
-      ++counted;
-      const unsigned long long su = __ldcg(&st[u]);
-      const uint32_t du = (uint32_t)(su >> 32);
-      bool improved = false;
-      if (algo == A_CC) {
-        unsigned long long cur = __ldcg(&st[v]);
-        while ((uint32_t)(cur >> 32) > du) {
-          const unsigned long long nw = ((unsigned long long)du << 32) | u;
-          const unsigned long long old = atomicCAS(&st[v], cur, nw);
-          if (old == cur) { improved = true; break; }
-          cur = old;
-        }
-      } else if (du != INF32) {
-        uint32_t wt = 1;
-        if (algo == A_SSSP)
-          wt = g.wmode == W_EXPLICIT ? w[i] : g.wmode == W_SYNTH ? (u + v) % 128u + 1u : 1u;
-        const uint64_t nd = (uint64_t)du + wt;
-        if (nd < INF32) {
-          const unsigned long long np = (nd << 32) | u;
-          const unsigned long long old = atomicMin(&st[v], np);
-          improved = nd < (old >> 32);
-        }
-      }
-      if (improved && __ldcg(&mark[v]) != stamp && atomicExch(&mark[v], stamp) != stamp) {
-        d = g.slots[v];
-        want = d > 0;
-      }
-    }
-    frontier_append(out, want, v, d);
-  }
-  if (edge_stat && counted) atomicAdd(edge_stat, (unsigned long long)counted);
-}
-
-// ---------------------------------------------------------------------------
-// Per-query state init (InitGraph, driver.cuh:200-229)
-// ---------------------------------------------------------------------------
-__global__ void k_init_state(unsigned long long *st, uint32_t nv, int algo,
-                             uint32_t source) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride) {
-    unsigned long long s;
-    if (algo == A_CC) s = ((unsigned long long)v << 32) | INF32;
-    else s = (v == source) ? (unsigned long long)INF32 : ~0ull;
-    st[v] = s;
-  }
-}
-
-__global__ void k_split_state(const unsigned long long *st, uint32_t nv,
-                              uint32_t *val, uint32_t *par) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride) {
-    const unsigned long long s = st[v];
-    if (val) val[v] = (uint32_t)(s >> 32);
-    if (par) par[v] = (uint32_t)s;
   }
 }
 
@@ -678,6 +466,7 @@ __global__ void k_reloc_frontier(const unsigned int *rl_count, const uint32_t *r
 // Copy op over relocation entries: vertex field = relocation list index.
 struct RelocCopyOp {
   static constexpr bool kAppends = false;
+  static constexpr bool kQuad = false;
   using Payload = CopyPay;
   GraphView g;
   const uint64_t *rl_from;
@@ -805,37 +594,6 @@ __global__ void k_keys_low(const uint64_t *keys, const uint32_t *n_ptr, uint32_t
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
     col[i] = (uint32_t)keys[i];
-}
-
-// Per-query summary: reached count, sum / max of finite values, sum of the
-// parents of reached vertices.
-__global__ void k_summary(const unsigned long long *st, uint32_t nv, unsigned long long *out) {
-  unsigned long long reached = 0, sum = 0, mx = 0, psum = 0;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride) {
-    const unsigned long long s = st[v];
-    const uint32_t val = (uint32_t)(s >> 32);
-    if (val == INF32) continue;
-    reached += 1;
-    sum += val;
-    mx = val > mx ? val : mx;
-    if ((uint32_t)s != INF32) psum += (uint32_t)s;
-  }
-  typedef cub::BlockReduce<unsigned long long, RELAX_THREADS> BR;
-  __shared__ typename BR::TempStorage tmp;
-  unsigned long long r = BR(tmp).Sum(reached);
-  __syncthreads();
-  unsigned long long sm = BR(tmp).Sum(sum);
-  __syncthreads();
-  unsigned long long m = BR(tmp).Reduce(mx, cub::Max());
-  __syncthreads();
-  unsigned long long ps = BR(tmp).Sum(psum);
-  if (threadIdx.x == 0) {
-    atomicAdd(&out[0], r);
-    atomicAdd(&out[1], sm);
-    atomicMax(&out[2], m);
-    atomicAdd(&out[3], ps);
-  }
 }
 
 __global__ void k_summary_pr(const double *x, uint32_t nv, double *out) {

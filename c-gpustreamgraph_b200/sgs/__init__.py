@@ -47,9 +47,8 @@ EXPORTS = [
     "sgs_query_summary", "sgs_gen_update_stream", "sgs_hash_weights",
 ]
 
-K_SSSP, K_BFS, K_CC, K_INVALIDATE, K_PR_PUSH = range(5)
-KERNEL_KINDS = {"sssp": K_SSSP, "bfs": K_BFS, "cc": K_CC, "invalidate": K_INVALIDATE,
-                "pr_push": K_PR_PUSH}
+K_GROUP, K_GROUP_INVAL, K_PR_PUSH = range(3)
+KERNEL_KINDS = {"group_relax": K_GROUP, "group_invalidate": K_GROUP_INVAL, "pr_push": K_PR_PUSH}
 
 
 class SgsError(RuntimeError):
@@ -72,6 +71,7 @@ class Config(C.Structure):
         ("pr_tol", C.c_double),
         ("slack_div", C.c_uint32),
         ("arena_headroom", C.c_double),
+        ("group_size", C.c_uint32),
     ]
 
 

@@ -92,6 +92,8 @@ typedef struct sgs_config {
   double pr_tol;          /* stop when sum|residual| < pr_tol              */
   uint32_t slack_div;     /* per-block slack: cap = deg + deg/slack_div + 2 */
   double arena_headroom;  /* extra arena fraction for relocated blocks    */
+  uint32_t group_size;    /* BFS/SSSP/CC queries relaxed together per edge
+                             pass (1..4); 1 = one query per pass            */
 } sgs_config;
 
 typedef struct sgs_query_stats {
@@ -121,15 +123,14 @@ typedef struct sgs_engine_stats {
 
 /* Per-kernel-class timing of the relaxation launches (CUDA events on the
  * engine's stream around every launch that has work; off by default).
- * bytes_alg = algorithmic bytes: per traversed slot 16 B (SSSP: id, weight,
- * 8 B distance read+write), 12 B (BFS/CC/invalidation), 20 B (PR FP64
- * residual push), plus 20 B per active vertex. */
-#define SGS_K_SSSP 0
-#define SGS_K_BFS 1
-#define SGS_K_CC 2
-#define SGS_K_INVALIDATE 3
-#define SGS_K_PR_PUSH 4
-#define SGS_K_COUNT 5
+ * bytes_alg = algorithmic bytes: per walked slot the 4-B id (+4-B weight when
+ * a lane needs stored weights) read once for all lanes of a group, per
+ * (query, edge) relaxation 8 B of state read+write (PageRank: 16 B FP64
+ * residual), plus 20 B per active vertex. */
+#define SGS_K_GROUP 0        /* BFS/SSSP/CC relaxation of a query group   */
+#define SGS_K_GROUP_INVAL 1  /* parent-tree invalidation of a query group */
+#define SGS_K_PR_PUSH 2      /* PageRank residual push                    */
+#define SGS_K_COUNT 3
 typedef struct sgs_kernel_stats {
   uint64_t launches;
   uint64_t slots;      /* positions walked (edges incl. tombstones)          */

@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_config_defaults_without_gpu():
     c = sgs.default_config()
-    assert c.segments == 512 and c.max_rounds == 1000
+    assert c.segments == 512 and c.max_rounds == 1000 and c.group_size == 4
     assert abs(c.pr_alpha - 0.85) < 1e-12
     assert sgs.lib().sgs_version().startswith(b"sgs-b200")
 

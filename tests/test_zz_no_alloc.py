@@ -35,6 +35,10 @@ def test_noalloc_matches_engine_queries():
         e.load_csr(nv, row, col, w)
         qs, qb = e.add_query(sgs.SSSP, 0), e.add_query(sgs.BFS, 11)
         ref = {"sssp": (qs.value(), qs.parent()), "bfs": (qb.value(), qb.parent())}
+    # values must equal the engine's; parents (not unique) must be valid tight
+    # predecessors, and this kernel keeps the smallest-id one, like the oracle
+    exact = {"sssp": O.sssp(nv, row, col, w, 0)[1], "bfs": O.bfs(nv, row, col, 11)[1]}
+    weights = {"sssp": w, "bfs": None}
     dev = torch.device("cuda", 0)
     d_row = torch.from_numpy(row.view(np.int64)).to(dev)
     d_col = torch.from_numpy(col.view(np.int32)).to(dev)
@@ -51,8 +55,11 @@ def test_noalloc_matches_engine_queries():
                     par.data_ptr(), None)
             torch.cuda.synchronize()
             assert rc == 0, sgs.lib().sgs_last_error()
-            assert np.array_equal(dist.cpu().numpy().view(np.uint32), ref[name][0]), (name, call)
-            assert np.array_equal(par.cpu().numpy().view(np.uint32), ref[name][1]), (name, call)
+            got_d = dist.cpu().numpy().view(np.uint32)
+            got_p = par.cpu().numpy().view(np.uint32)
+            assert np.array_equal(got_d, ref[name][0]), (name, call)
+            assert np.array_equal(got_p, exact[name]), (name, call)
+            assert O.check_tree(nv, row, col, weights[name], src, got_d, ref[name][1]) == 0
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
