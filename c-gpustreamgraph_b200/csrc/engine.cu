@@ -201,7 +201,7 @@ struct sgs_engine {
   DBuf<uint64_t> wbase;
   DBuf<uint32_t> rl_vtx, rl_len;
   DBuf<uint64_t> rl_from, rl_to;
-  DBuf<unsigned int> rl_count;
+  DBuf<unsigned long long> rl_count;
   DBuf<unsigned char> cub_tmp;
 
   // per-kernel-class timing
@@ -360,8 +360,11 @@ struct sgs_engine {
       // segment s = vertices [b_s, b_{s+1}) with ~total/nseg slots each
       sp = 0;
       for (uint32_t sg = 1; sg <= nseg; ++sg) {
+        // segment boundaries by slot count; the last one ends at nv so that
+        // trailing empty vertices stay with the resident segments
         uint64_t target = (uint64_t)((double)total * sg / nseg);
-        uint32_t b = (uint32_t)(std::lower_bound(hs.begin(), hs.end(), target) - hs.begin());
+        uint32_t b = sg == nseg ? nv
+                                : (uint32_t)(std::lower_bound(hs.begin(), hs.end(), target) - hs.begin());
         b = std::min(b, nv);
         if ((double)hs[b] <= usable) sp = b;
         else break;
@@ -746,6 +749,7 @@ struct sgs_engine {
     const bool explicit_w = cfg.weight_mode == SGS_W_EXPLICIT;
     if (ni && explicit_w && !iw) fail(SGS_ERR_INVALID, "explicit weight mode needs insert weights");
     GraphView g = view();
+    Range snap("sgs:snapshot");
     CK(cudaEventRecord(ev_batch.a, s));
     // ---- upload + keys + sort
     upload(b_isrc, is, ni, mem);
@@ -958,8 +962,8 @@ struct sgs_engine {
     unsigned long long *tombs = b_stat.p + 2;
     CK(cudaMemsetAsync(tombs, 0, sizeof(unsigned long long), s));
     if (nd) {
-      b_gstart.ensure((size_t)nv + 1);
       CK(cudaMemsetAsync(special(4), 0, sizeof(unsigned long long), s));
+      b_gstart.ensure((size_t)nv + 1);
       k_group_heads<<<grid_elem(nd), 256, 0, s>>>(g, b_dkeys_s.p, nullptr, (uint32_t)nd, b_gstart.p,
                                                   nullptr, 0, fview(0, special(4)));
       TombOp op{g, b_dkeys_s.p, b_gstart.p, (uint32_t)nd};
@@ -999,8 +1003,8 @@ struct sgs_engine {
       c.rl_from = rl_from.p;
       c.rl_to = rl_to.p;
       c.rl_len = rl_len.p;
-      c.rl_count = rl_count.p;
-      CK(cudaMemsetAsync(rl_count.p, 0, sizeof(unsigned int), s));
+      c.rl_count64 = rl_count.p;
+      CK(cudaMemsetAsync(rl_count.p, 0, sizeof(unsigned long long), s));
       CK(cudaMemsetAsync(b_err.p, 0, sizeof(unsigned int), s));
       k_insert_plan<<<grid_elem(ni), 256, 0, s>>>(g, b_ikept.p, b_nkept.p, c, 0, nullptr);
       k_insert_write<<<grid_elem(ni), 256, 0, s>>>(
@@ -1011,7 +1015,8 @@ struct sgs_engine {
       seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(6)), fview(1, special(7)), op,
                                                    nullptr);
       CK(cudaGetLastError());
-      unsigned int herr = 0, hrl = 0;
+      unsigned int herr = 0;
+      unsigned long long hrl = 0;
       CK(cudaMemcpyAsync(&herr, b_err.p, sizeof(herr), cudaMemcpyDeviceToHost, s));
       CK(cudaMemcpyAsync(&hrl, rl_count.p, sizeof(hrl), cudaMemcpyDeviceToHost, s));
       sync();
@@ -1191,7 +1196,7 @@ SGS_API void sgs_config_default(sgs_config *c) {
   c->pr_alpha = 0.85;
   c->pr_tol = 1e-6 * 0.15;
   c->slack_div = 8;
-  c->arena_headroom = 0.10;
+  c->arena_headroom = 0.30;
   c->group_size = 4;
 }
 

@@ -132,6 +132,75 @@ __device__ __forceinline__ void frontier_append(const FrontierView &f, bool want
   }
 }
 
+// Block-aggregated append: one atomic per CTA instead of one per warp, for
+// builders where most threads append.  Every thread of the CTA (blockDim.x ==
+// RELAX_THREADS) must call it the same number of times.
+__device__ __forceinline__ void frontier_append_block(const FrontierView &f, bool want,
+                                                      uint32_t v, uint32_t d,
+                                                      uint32_t *aux = nullptr,
+                                                      uint32_t aux_val = 0) {
+  constexpr int NW = RELAX_THREADS / 32;
+  __shared__ unsigned long long s_warp[NW];
+  __shared__ unsigned long long s_base;
+  const unsigned full = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const uint32_t dp = (d + 3u) & ~3u;
+  const unsigned long long inc = want ? ((1ull << CNT_SHIFT) | (unsigned long long)dp) : 0ull;
+  unsigned long long x = inc;
+#pragma unroll
+  for (int s = 1; s < 32; s <<= 1) {
+    const unsigned long long y = __shfl_up_sync(full, x, s);
+    if (lane >= s) x += y;
+  }
+  if (lane == 31) s_warp[wid] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long run = 0;
+    for (int w = 0; w < NW; ++w) {
+      const unsigned long long t = s_warp[w];
+      s_warp[w] = run;
+      run += t;
+    }
+    s_base = run ? atomicAdd((unsigned long long *)f.counter, run) : 0ull;
+  }
+  __syncthreads();
+  if (want) {
+    const unsigned long long pos = s_base + s_warp[wid] + (x - inc);
+    const uint32_t slot = (uint32_t)(pos >> CNT_SHIFT);
+    const uint64_t eb = pos & EDGE_MASK;
+    f.vtx[slot] = v;
+    f.len[slot] = d;
+    f.ebase[slot] = eb;
+    if (aux) aux[slot] = aux_val;
+    if (dp) {
+      const uint64_t u0 = (eb + UNIT - 1) / UNIT, u1 = (eb + dp - 1) / UNIT;
+      for (uint64_t u = u0; u <= u1 && u < f.ucap; ++u) f.ustart[u] = slot;
+    }
+  }
+  __syncthreads();  // s_warp / s_base are reused by the next call
+}
+
+// Warp-aggregated atomicAdd: lanes with want add val to *p; returns each
+// lane's old value (exclusive prefix within the warp added).  All 32 lanes of
+// a converged warp must call it.
+__device__ __forceinline__ unsigned long long warp_atomic_add(unsigned long long *p, bool want,
+                                                              unsigned long long val) {
+  const unsigned full = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31;
+  unsigned long long x = want ? val : 0ull;
+  const unsigned long long inc = x;
+#pragma unroll
+  for (int s = 1; s < 32; s <<= 1) {
+    const unsigned long long y = __shfl_up_sync(full, x, s);
+    if (lane >= s) x += y;
+  }
+  const unsigned long long total = __shfl_sync(full, x, 31);
+  unsigned long long base = 0;
+  if (lane == 31 && total) base = atomicAdd(p, total);
+  base = __shfl_sync(full, base, 31);
+  return base + x - inc;
+}
+
 // 16-B read-only load of four consecutive u32 slots (block starts and j0 are
 // multiples of 4 elements, so the address is 16-B aligned).
 __device__ __forceinline__ uint4 ld_quad(const uint32_t *p) {

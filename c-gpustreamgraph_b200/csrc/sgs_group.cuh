@@ -327,7 +327,7 @@ __global__ void k_group_dense(GraphView g, const uint32_t *val, uint32_t lanes,
         }
       }
     }
-    frontier_append(out, want, (uint32_t)v, d);
+    frontier_append_block(out, want, (uint32_t)v, d);
   }
 }
 

@@ -97,14 +97,16 @@ struct PrAmendOp {
 };
 
 // Tombstone every slot of u whose destination is in u's sorted delete group
-// (PMAGraph::del_edge removes every matching entry).
+// (PMAGraph::del_edge removes every matching entry).  Four slots per thread,
+// each looked up by binary search in the group (a few L1-resident lines); the
+// block is read with a plain (coherent) load because this kernel writes it.
 struct GroupPay {
   uint64_t off;
   uint32_t gs, ge;
 };
 struct TombOp {
   static constexpr bool kAppends = false;
-  static constexpr bool kQuad = false;
+  static constexpr bool kQuad = true;
   using Payload = GroupPay;
   GraphView g;
   const uint64_t *keys;   // sorted delete keys (src<<32|dst)
@@ -125,24 +127,33 @@ struct TombOp {
     p.ge = l;
     return p;
   }
-  __device__ __forceinline__ uint32_t visit(uint32_t u, const Payload &p, uint32_t j,
-                                            bool &, uint32_t &, uint32_t &) const {
-    uint32_t *a = adj_wptr(g, p.off);
-    const uint32_t dst = a[j];
-    if (dst == SGS_TOMB) return 0;
-    const uint64_t k = ((uint64_t)u << 32) | dst;
-    uint32_t l = p.gs, r = p.ge;
-    while (l < r) {
-      uint32_t m = (l + r) >> 1;
-      if (keys[m] < k) l = m + 1;
-      else r = m;
-    }
-    if (l < p.ge && keys[l] == k) {
-      a[j] = SGS_TOMB;
-      atomicSub(&g.live[u], 1u);
-      return 1;
-    }
+  __device__ __forceinline__ uint32_t visit(uint32_t, const Payload &, uint32_t, bool &, uint32_t &,
+                                            uint32_t &) const {
     return 0;
+  }
+  __device__ __forceinline__ uint32_t visit4(uint32_t u, const Payload &p, uint32_t j0, uint32_t len,
+                                             bool (&)[4], uint32_t (&)[4], uint32_t (&)[4]) const {
+    uint32_t *a = adj_wptr(g, p.off) + j0;
+    const uint4 q = *reinterpret_cast<const uint4 *>(a);
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t dst = quad_at(q, k);
+      if (j0 + k >= len || dst == SGS_TOMB) continue;
+      const uint64_t key = ((uint64_t)u << 32) | dst;
+      uint32_t l = p.gs, r = p.ge;
+      while (l < r) {
+        const uint32_t m = (l + r) >> 1;
+        if (keys[m] < key) l = m + 1;
+        else r = m;
+      }
+      if (l < p.ge && keys[l] == key) {
+        a[k] = SGS_TOMB;
+        ++c;
+      }
+    }
+    if (c) atomicSub(&g.live[u], c);
+    return c;
   }
 };
 
@@ -256,7 +267,7 @@ __global__ void k_dense_frontier(GraphView g, FrontierView out) {
       d = g.slots[v];
       want = d > 0;
     }
-    frontier_append(out, want, (uint32_t)v, d);
+    frontier_append_block(out, want, (uint32_t)v, d);
   }
 }
 
@@ -351,7 +362,7 @@ __global__ void k_group_heads(GraphView g, const uint64_t *keys,
         if (want && mark) want = atomicExch(&mark[u], stamp) != stamp;
       }
     }
-    frontier_append(out, want, u, d, gstart, (uint32_t)i);
+    frontier_append_block(out, want, u, d, gstart, (uint32_t)i);
   }
 }
 
@@ -370,7 +381,7 @@ struct InsertCtx {
   uint64_t *rl_from;
   uint64_t *rl_to;
   uint32_t *rl_len;
-  unsigned int *rl_count;
+  unsigned long long *rl_count64;
 };
 
 __device__ __forceinline__ uint32_t grow_cap(uint32_t need) {
@@ -383,48 +394,77 @@ __global__ void k_insert_plan(GraphView g, const uint64_t *keys, const uint32_t 
                               InsertCtx c, int dry, unsigned long long *demand) {
   const uint32_t n = *n_ptr;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const uint32_t u = (uint32_t)(keys[i] >> 32);
-    if (i > 0 && (uint32_t)(keys[i - 1] >> 32) == u) continue;
-    // group end
-    const uint64_t lim = ((uint64_t)u + 1) << 32;
-    uint32_t l = (uint32_t)i, r = n;
-    while (l < r) {
-      uint32_t m = (l + r) >> 1;
-      if (keys[m] < lim) l = m + 1;
-      else r = m;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < n; b += stride) {
+    const uint64_t i = b + threadIdx.x;
+    // per-lane decision; the arena/demand/relocation atomics are warp-aggregated
+    bool head = false, reloc = false;
+    uint32_t u = 0, k = 0, sl = 0, nc = 0;
+    uint64_t o = 0;
+    int tier = 0;
+    if (i < n) {
+      u = (uint32_t)(keys[i] >> 32);
+      head = i == 0 || (uint32_t)(keys[i - 1] >> 32) != u;
     }
-    const uint32_t k = l - (uint32_t)i;
-    const uint32_t sl = g.slots[u], cp = g.cap[u];
-    const uint64_t need = (uint64_t)sl + k;
-    const uint64_t o = g.off[u];
-    const int tier = (o & HOST_BIT) ? 1 : 0;
-    if (need <= cp) {
-      if (!dry) {
-        c.wbase[u] = o + sl;
-        g.slots[u] = (uint32_t)need;
-        g.live[u] += k;
+    if (head) {
+      // group end: exponential then binary search (groups are usually tiny)
+      const uint64_t lim = ((uint64_t)u + 1) << 32;
+      uint32_t lo = (uint32_t)i + 1, step = 1, hi = lo;
+      while (hi < n && keys[hi] < lim) {
+        lo = hi + 1;
+        hi = (uint32_t)min((uint64_t)hi + step, (uint64_t)n);
+        step <<= 1;
       }
+      while (lo < hi) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (keys[m] < lim) lo = m + 1;
+        else hi = m;
+      }
+      k = lo - (uint32_t)i;
+      sl = g.slots[u];
+      const uint32_t cp = g.cap[u];
+      const uint64_t need = (uint64_t)sl + k;
+      o = g.off[u];
+      tier = (o & HOST_BIT) ? 1 : 0;
+      if (need <= cp) {
+        if (!dry) {
+          c.wbase[u] = o + sl;
+          g.slots[u] = (uint32_t)need;
+          g.live[u] += k;
+        }
+      } else if (need > 0xFFFFFFF0ull) {
+        atomicOr(c.err, 4u);
+      } else {
+        reloc = true;
+        nc = grow_cap((uint32_t)need);
+      }
+    }
+    if (dry) {
+      for (int t = 0; t < 2; ++t) warp_atomic_add(&demand[t], reloc && tier == t, nc);
       continue;
     }
-    if (need > 0xFFFFFFF0ull) { atomicOr(c.err, 4u); continue; }
-    const uint32_t nc = grow_cap((uint32_t)need);
-    if (dry) { atomicAdd(&demand[tier], (unsigned long long)nc); continue; }
-    const unsigned long long pos = atomicAdd(&c.arena_top[tier], (unsigned long long)nc);
-    if (pos + nc > c.arena_cap[tier]) { atomicOr(c.err, 8u); continue; }
-    const uint64_t no = pos | (tier ? HOST_BIT : 0);
-    if (sl) {
-      const unsigned int q = atomicAdd(c.rl_count, 1u);
-      c.rl_vtx[q] = u;
-      c.rl_from[q] = o;
-      c.rl_to[q] = no;
-      c.rl_len[q] = sl;
+    unsigned long long pos[2];
+    for (int t = 0; t < 2; ++t) pos[t] = warp_atomic_add(&c.arena_top[t], reloc && tier == t, nc);
+    const unsigned long long q =
+        warp_atomic_add((unsigned long long *)c.rl_count64, reloc && sl > 0, 1ull);
+    if (reloc) {
+      const unsigned long long p0 = pos[tier];
+      if (p0 + nc > c.arena_cap[tier]) {
+        atomicOr(c.err, 8u);
+      } else {
+        const uint64_t no = p0 | (tier ? HOST_BIT : 0);
+        if (sl) {
+          c.rl_vtx[q] = u;
+          c.rl_from[q] = o;
+          c.rl_to[q] = no;
+          c.rl_len[q] = sl;
+        }
+        c.wbase[u] = no + sl;
+        g.off[u] = no;
+        g.cap[u] = nc;
+        g.slots[u] = sl + k;
+        g.live[u] += k;
+      }
     }
-    c.wbase[u] = no + sl;
-    g.off[u] = no;
-    g.cap[u] = nc;
-    g.slots[u] = (uint32_t)need;
-    g.live[u] += k;
   }
 }
 
@@ -437,14 +477,20 @@ __global__ void k_insert_write(GraphView g, const uint64_t *keys, const uint32_t
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     const uint64_t k = keys[i];
     const uint32_t u = (uint32_t)(k >> 32), v = (uint32_t)k;
+    // group start: exponential search backwards, then binary search
     const uint64_t lo_key = (uint64_t)u << 32;
-    uint32_t l = 0, r = (uint32_t)i;
-    while (l < r) {
-      uint32_t m = (l + r) >> 1;
-      if (keys[m] < lo_key) l = m + 1;
-      else r = m;
+    uint32_t hi = (uint32_t)i, step = 1, lo = hi;
+    while (lo > 0 && keys[lo - 1] >= lo_key) {
+      hi = lo - 1;
+      lo = lo > step ? lo - step : 0;
+      step <<= 1;
     }
-    const uint64_t pos = wbase[u] + (i - l);
+    while (lo < hi) {
+      const uint32_t m = (lo + hi) >> 1;
+      if (keys[m] < lo_key) lo = m + 1;
+      else hi = m;
+    }
+    const uint64_t pos = wbase[u] + (i - lo);
     adj_wptr(g, pos)[0] = v;
     if (g.wmode == W_EXPLICIT) wgt_wptr(g, pos)[0] = w[i];
   }
@@ -452,9 +498,9 @@ __global__ void k_insert_write(GraphView g, const uint64_t *keys, const uint32_t
 
 // Relocation list -> frontier of copy entries; the entry's vertex field holds
 // the relocation list index.
-__global__ void k_reloc_frontier(const unsigned int *rl_count, const uint32_t *rl_len,
+__global__ void k_reloc_frontier(const unsigned long long *rl_count, const uint32_t *rl_len,
                                  FrontierView out) {
-  const uint32_t n = *rl_count;
+  const uint32_t n = (uint32_t)*rl_count;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < n; b += stride) {
     const uint64_t i = b + threadIdx.x;
