@@ -288,16 +288,22 @@ def engine_arm(a, R):
     kd = kst[dom]
     peak, peak_src = measured_peak_hbm()
     achieved = kd["bytes_alg"] / (kd["ms"] * 1e-3) / 1e9 if kd["ms"] > 0 else 0.0
+    # traffic: DRAM bytes per walked slot of this kernel from the committed
+    # ncu capture (profiles/relax_traffic.json), scaled to the average launch
     tr = profile_traffic()
     traffic = None
-    if tr and dom in tr.get("per_kind", {}):
-        pk = tr["per_kind"][dom]
-        traffic = (pk["bytes_per_slot"] * kd["slots"] + pk["bytes_per_entry"] * kd["entries"]) / max(kd["launches"], 1)
-    roof = {"bound": "hbm", "kernel": f"seg_map<{dom}>", "achieved": round(achieved, 1),
+    if tr and dom in tr.get("per_kind", {}) and kd["launches"]:
+        traffic = round(tr["per_kind"][dom]["dram_bytes_per_slot"] * kd["slots"] / kd["launches"])
+    roof = {"bound": "hbm", "kernel": f"group_map<{dom}>", "achieved": round(achieved, 1),
             "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "peak_source": peak_src, "traffic": traffic,
             "launches": kd["launches"], "avg_launch_ms": kd["ms"] / max(kd["launches"], 1),
             "alg_bytes_per_launch": kd["bytes_alg"] / max(kd["launches"], 1)}
+    if kd["max_ms"] > 0:
+        sweep = kd["max_bytes_alg"] / (kd["max_ms"] * 1e-3) / 1e9
+        roof["largest_launch"] = {"slots": kd["max_slots"], "entries": kd["max_entries"],
+                                  "ms": round(kd["max_ms"], 4), "achieved": round(sweep, 1),
+                                  "frac": round(sweep / peak, 4)}
     launches = int(sum(k["launches"] for k in kst.values()))
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": R.world,

@@ -464,11 +464,18 @@ struct sgs_engine {
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, a, b));
     sgs_kernel_stats &k = kst[kind];
+    const double bytes = per_slot * (double)T + per_inst * (double)inst + 20.0 * (double)n;
     k.launches += 1;
     k.slots += T;
     k.entries += n;
-    k.bytes_alg += per_slot * (double)T + per_inst * (double)inst + 20.0 * (double)n;
+    k.bytes_alg += bytes;
     k.ms += ms;
+    if (T > k.max_slots) {
+      k.max_slots = T;
+      k.max_entries = n;
+      k.max_bytes_alg = bytes;
+      k.max_ms = ms;
+    }
   }
 
   // Rounds of a group op from the frontier in buffer 0 / cnt[0] (lane masks in

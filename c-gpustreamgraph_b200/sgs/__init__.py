@@ -117,6 +117,10 @@ class KernelStats(C.Structure):
         ("entries", C.c_uint64),
         ("bytes_alg", C.c_double),
         ("ms", C.c_double),
+        ("max_slots", C.c_uint64),
+        ("max_entries", C.c_uint64),
+        ("max_bytes_alg", C.c_double),
+        ("max_ms", C.c_double),
     ]
 
     def as_dict(self):

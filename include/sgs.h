@@ -137,6 +137,10 @@ typedef struct sgs_kernel_stats {
   uint64_t entries;    /* active vertices                                    */
   double bytes_alg;
   double ms;
+  uint64_t max_slots;  /* the largest launch (e.g. the all-vertices sweep)   */
+  uint64_t max_entries;
+  double max_bytes_alg;
+  double max_ms;
 } sgs_kernel_stats;
 
 SGS_API const char *sgs_version(void);
