@@ -45,6 +45,7 @@ EXPORTS = [
     "sgs_get_query_stats", "sgs_get_engine_stats", "sgs_graph_export",
     "sgs_synchronize", "sgs_kernel_timing", "sgs_get_kernel_stats",
     "sgs_query_summary", "sgs_gen_update_stream", "sgs_hash_weights",
+    "sgs_read_edge_list", "sgs_read_stream_sizes", "sgs_read_update_file", "sgs_free",
 ]
 
 K_GROUP, K_GROUP_INVAL, K_PR_PUSH = range(3)
@@ -162,9 +163,16 @@ def lib():
     L.sgs_gen_update_stream.argtypes = [u32, vp, vp, u64, u64, u64, vp, vp, vp, vp]
     L.sgs_hash_weights.argtypes = [u64, u64, vp, vp, vp]
     L.sgs_hash_weights.restype = None
+    pp = C.POINTER(C.c_void_p)
+    L.sgs_read_edge_list.argtypes = [C.c_char_p, C.POINTER(u32), C.POINTER(u64), pp, pp, pp]
+    L.sgs_read_stream_sizes.argtypes = [C.c_char_p, C.POINTER(u32), pp, pp]
+    L.sgs_read_update_file.argtypes = [C.c_char_p, C.POINTER(u64), pp, pp, pp, C.POINTER(u64),
+                                       pp, pp, pp]
+    L.sgs_free.argtypes = [vp]
+    L.sgs_free.restype = None
     for name in EXPORTS:
         if name not in ("sgs_version", "sgs_last_error", "sgs_config_default",
-                        "sgs_hash_weights"):
+                        "sgs_hash_weights", "sgs_free"):
             getattr(L, name).restype = i32
     _lib = L
     return L
@@ -206,6 +214,47 @@ def gen_update_stream(nv, row, col, seed, n_ins, n_del):
     _check(lib().sgs_gen_update_stream(nv, _ptr(row), _ptr(col), seed, n_ins, n_del,
                                        *[_ptr(a) for a in out]))
     return out[0][:n_ins], out[1][:n_ins], out[2][:n_del], out[3][:n_del]
+
+
+def _take(ptr, n, dtype):
+    """Copies n elements out of a library-allocated array and frees it."""
+    if not ptr:
+        return None
+    ct = C.c_uint32 if dtype == np.uint32 else C.c_uint64
+    out = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(max(n, 1),))[:n].copy()
+    lib().sgs_free(ptr)
+    return out.astype(dtype, copy=False)
+
+
+def read_edge_list(path):
+    """market_big edge list: (nv, src, dst, w or None), edges in file order."""
+    nv, ne = C.c_uint32(), C.c_uint64()
+    s, d, w = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    _check(lib().sgs_read_edge_list(str(path).encode(), C.byref(nv), C.byref(ne), C.byref(s),
+                                    C.byref(d), C.byref(w)))
+    n = ne.value
+    return nv.value, _take(s.value, n, np.uint32), _take(d.value, n, np.uint32), \
+        _take(w.value, n, np.uint32)
+
+
+def read_stream_sizes(path):
+    """Stream-size file: (adds[k], dels[k]) per snapshot."""
+    n = C.c_uint32()
+    a, d = C.c_void_p(), C.c_void_p()
+    _check(lib().sgs_read_stream_sizes(str(path).encode(), C.byref(n), C.byref(a), C.byref(d)))
+    return _take(a.value, n.value, np.uint64), _take(d.value, n.value, np.uint64)
+
+
+def read_update_file(path):
+    """Update file: dict of add_u/add_v/add_w and del_u/del_v/del_w arrays."""
+    na, nd = C.c_uint64(), C.c_uint64()
+    ptrs = [C.c_void_p() for _ in range(6)]
+    _check(lib().sgs_read_update_file(str(path).encode(), C.byref(na), C.byref(ptrs[0]),
+                                      C.byref(ptrs[1]), C.byref(ptrs[2]), C.byref(nd),
+                                      C.byref(ptrs[3]), C.byref(ptrs[4]), C.byref(ptrs[5])))
+    names = ["add_u", "add_v", "add_w", "del_u", "del_v", "del_w"]
+    counts = [na.value] * 3 + [nd.value] * 3
+    return {k: _take(p.value, n, np.uint32) for k, p, n in zip(names, ptrs, counts)}
 
 
 def hash_weights(wseed, src, dst):

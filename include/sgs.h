@@ -214,6 +214,25 @@ SGS_API int sgs_gen_update_stream(uint32_t nv, const uint64_t *row,
 SGS_API void sgs_hash_weights(uint64_t wseed, uint64_t n, const uint32_t *src,
                               const uint32_t *dst, uint32_t *w);
 
+/* Readers for the reference's input files (host only; arrays are malloc'd,
+ * release them with sgs_free):
+ *   edge list "src dst [w]" per line (market_big, parser.cpp:296-406): nv is
+ *     max id + 1, edges keep file order; *w is NULL without a third column;
+ *   stream sizes "adds dels" per snapshot (Loader.h:27-62);
+ *   update file "a|d src dst [w]" lines (Loader.h:64-100); missing weights
+ *     read as 0.
+ * Blank lines and lines starting with '#' or '%' are skipped. */
+SGS_API int sgs_read_edge_list(const char *path, uint32_t *nv, uint64_t *ne,
+                               uint32_t **src, uint32_t **dst, uint32_t **w);
+SGS_API int sgs_read_stream_sizes(const char *path, uint32_t *nsnap,
+                                  uint64_t **adds, uint64_t **dels);
+SGS_API int sgs_read_update_file(const char *path, uint64_t *n_add,
+                                 uint32_t **add_u, uint32_t **add_v,
+                                 uint32_t **add_w, uint64_t *n_del,
+                                 uint32_t **del_u, uint32_t **del_v,
+                                 uint32_t **del_w);
+SGS_API void sgs_free(void *p);
+
 SGS_API int sgs_kernel_timing(sgs_engine *e, int enable);
 
 /* From-scratch SSSP (w != NULL) or BFS (w == NULL) over a CSR that the caller
