@@ -9,6 +9,8 @@ Two spellings are offered:
 
 * :class:`Engine` -- the C ABI in Python form (load / add_query /
   apply_batch / gather);
+* :class:`Ppr` -- differentiable weighted personalized PageRank on a
+  prepared graph (``sgs_ppr_*``; the torch op is in :mod:`sgs.autograd`);
 * :class:`HybridEngine` -- the call sequence of the reference's sample
   drivers (``samples/hybrid_sssp/hybrid_sssp.cu:204-296``,
   ``samples/hybrid_pr/hybrid_pr.cu:154-200``): ``LoadGraph``, ``InitGraph``,
@@ -46,6 +48,8 @@ EXPORTS = [
     "sgs_synchronize", "sgs_kernel_timing", "sgs_get_kernel_stats",
     "sgs_query_summary", "sgs_gen_update_stream", "sgs_hash_weights",
     "sgs_read_edge_list", "sgs_read_stream_sizes", "sgs_read_update_file", "sgs_free",
+    "sgs_ppr_create_csr", "sgs_ppr_create", "sgs_ppr_destroy", "sgs_ppr_info",
+    "sgs_ppr_export", "sgs_ppr_forward", "sgs_ppr_backward",
 ]
 
 K_GROUP, K_GROUP_INVAL, K_PR_PUSH = range(3)
@@ -170,6 +174,13 @@ def lib():
                                        pp, pp, pp]
     L.sgs_free.argtypes = [vp]
     L.sgs_free.restype = None
+    L.sgs_ppr_create_csr.argtypes = [i32, u32, vp, vp, i32, C.POINTER(vp)]
+    L.sgs_ppr_create.argtypes = [vp, C.POINTER(vp)]
+    L.sgs_ppr_destroy.argtypes = [vp]
+    L.sgs_ppr_info.argtypes = [vp, C.POINTER(u32), C.POINTER(u64)]
+    L.sgs_ppr_export.argtypes = [vp, vp, vp, i32]
+    L.sgs_ppr_forward.argtypes = [vp, vp, vp, u32, dbl, dbl, u32, vp, C.POINTER(i32), i32]
+    L.sgs_ppr_backward.argtypes = [vp, vp, vp, vp, u32, dbl, dbl, u32, vp, vp, C.POINTER(i32), i32]
     for name in EXPORTS:
         if name not in ("sgs_version", "sgs_last_error", "sgs_config_default",
                         "sgs_hash_weights", "sgs_free"):
@@ -465,3 +476,124 @@ class HybridEngine:
 
     def GetNodeNum(self):
         return self.engine.nv
+
+
+class Ppr:
+    """A graph prepared for differentiable weighted personalized PageRank
+    (``sgs_ppr_*``): FP64 forward X = (1-alpha) T + alpha P^T X and its
+    adjoint.  Edge weights are given per edge in the CSR order of the
+    prepared graph (:meth:`export`).
+
+    Arrays may be numpy (host) or CUDA torch tensors (device, float64,
+    contiguous); results come back in the same form as ``T`` / ``X``.
+    ``tol`` is the L1 change of one Jacobi step summed over all nv*K entries
+    below which the iteration stops (default 1e-13 * nv * K).
+    """
+
+    def __init__(self, nv=None, row=None, col=None, engine: Engine | None = None, device=0):
+        h = C.c_void_p()
+        if engine is not None:
+            _check(lib().sgs_ppr_create(engine.h, C.byref(h)))
+        else:
+            row = np.ascontiguousarray(row, np.uint64)
+            col = np.ascontiguousarray(col, np.uint32)
+            _check(lib().sgs_ppr_create_csr(device, nv, _ptr(row), _ptr(col), MEM_HOST, C.byref(h)))
+        self.h = h
+        n, m = C.c_uint32(), C.c_uint64()
+        _check(lib().sgs_ppr_info(self.h, C.byref(n), C.byref(m)))
+        self.nv, self.ne = n.value, m.value
+        self.last_iters = 0
+
+    def close(self):
+        if self.h:
+            lib().sgs_ppr_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def export(self):
+        row = np.empty(self.nv + 1, np.uint64)
+        col = np.empty(max(self.ne, 1), np.uint32)
+        _check(lib().sgs_ppr_export(self.h, _ptr(row), _ptr(col), MEM_HOST))
+        return row, col[: self.ne]
+
+    def _tol(self, tol, K):
+        return 1e-13 * self.nv * K if tol is None else float(tol)
+
+    @staticmethod
+    def _is_torch(a):
+        return type(a).__module__.startswith("torch")
+
+    @staticmethod
+    def _dev_args(*arrs):
+        import torch
+
+        for a in arrs:
+            if a is None:
+                continue
+            if not (a.is_cuda and a.dtype == torch.float64 and a.is_contiguous()):
+                raise ValueError("device arrays must be contiguous float64 CUDA tensors")
+        # the library runs on its own stream: make the caller's work visible
+        torch.cuda.current_stream().synchronize()
+
+    def forward(self, w, T, alpha=0.85, tol=None, max_iter=100000):
+        it = C.c_int()
+        if self._is_torch(T):
+            import torch
+
+            T2 = T.reshape(self.nv, -1)
+            K = T2.shape[1]
+            X = torch.empty_like(T2)
+            self._dev_args(w, T2, X)
+            _check(lib().sgs_ppr_forward(self.h, w.data_ptr(), T2.data_ptr(), K, alpha,
+                                         self._tol(tol, K), max_iter, X.data_ptr(), C.byref(it),
+                                         MEM_DEVICE))
+        else:
+            w = np.ascontiguousarray(w, np.float64)
+            T2 = np.ascontiguousarray(np.asarray(T, np.float64).reshape(self.nv, -1))
+            K = T2.shape[1]
+            X = np.empty_like(T2)
+            _check(lib().sgs_ppr_forward(self.h, _ptr(w), _ptr(T2), K, alpha, self._tol(tol, K),
+                                         max_iter, _ptr(X), C.byref(it), MEM_HOST))
+        self.last_iters = it.value
+        return X
+
+    def backward(self, w, X, G, alpha=0.85, tol=None, max_iter=100000, want_w=True, want_T=True):
+        """(dL/dw, dL/dT) for the upstream gradient G = dL/dX."""
+        it = C.c_int()
+        if self._is_torch(X):
+            import torch
+
+            K = X.shape[1]
+            G = G.reshape(self.nv, K).contiguous()
+            gw = torch.empty(max(self.ne, 1), dtype=torch.float64, device=X.device) if want_w else None
+            gT = torch.empty_like(X) if want_T else None
+            self._dev_args(w, X, G, gw, gT)
+            _check(lib().sgs_ppr_backward(self.h, w.data_ptr(), X.data_ptr(), G.data_ptr(), K,
+                                          alpha, self._tol(tol, K), max_iter,
+                                          gw.data_ptr() if gw is not None else None,
+                                          gT.data_ptr() if gT is not None else None,
+                                          C.byref(it), MEM_DEVICE))
+        else:
+            w = np.ascontiguousarray(w, np.float64)
+            X = np.ascontiguousarray(X, np.float64)
+            K = X.shape[1]
+            G = np.ascontiguousarray(np.asarray(G, np.float64).reshape(self.nv, K))
+            gw = np.empty(max(self.ne, 1)) if want_w else None
+            gT = np.empty_like(X) if want_T else None
+            _check(lib().sgs_ppr_backward(self.h, _ptr(w), _ptr(X), _ptr(G), K, alpha,
+                                          self._tol(tol, K), max_iter, _ptr(gw), _ptr(gT),
+                                          C.byref(it), MEM_HOST))
+        gw = gw[: self.ne] if gw is not None else None
+        self.last_iters = it.value
+        return gw, gT

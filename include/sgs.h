@@ -257,6 +257,39 @@ SGS_API int sgs_sssp_csr_noalloc(uint32_t nv, const uint64_t *row,
                                  uint32_t *parent, void *stream);
 SGS_API int sgs_get_kernel_stats(sgs_engine *e, int kind, sgs_kernel_stats *out);
 
+/* Differentiable weighted personalized PageRank (FP64).  Generalises the
+ * reference's PageRank fixed point (samples/hybrid_pr/hybrid_pr.cu:26-151,
+ * x = (1-alpha) + alpha * sum_{u->v} x_u / outdeg_u, dangling mass dropped)
+ * to edge weights w (P[u,v] = w_uv / sum_v' w_uv') and K teleport vectors:
+ *     X[:,k] = (1-alpha) T[:,k] + alpha P^T X[:,k]
+ * With T = 1 and unit weights X is the reference's PageRank.  The backward
+ * pass has no counterpart in the reference.  Layout: X, T, G, gT are
+ * vertex-major [nv][K] doubles; w and gw are per edge in the CSR order of
+ * the prepared graph (sgs_ppr_export).  `mem` says where all arrays live.
+ * Convergence: Jacobi steps until the L1 change summed over all nv*K entries
+ * is below tol; SGS_ERR_NOCONV after max_iter steps.  *iters (optional) gets
+ * the steps taken.  Weights must be positive and finite (else
+ * SGS_ERR_INVALID).  A handle is not thread-safe. */
+typedef struct sgs_ppr sgs_ppr;
+SGS_API int sgs_ppr_create_csr(int device, uint32_t nv, const uint64_t *row,
+                               const uint32_t *col, int mem, sgs_ppr **out);
+/* Prepares the engine's current graph (a snapshot of the dynamic graph). */
+SGS_API int sgs_ppr_create(sgs_engine *e, sgs_ppr **out);
+SGS_API int sgs_ppr_destroy(sgs_ppr *p);
+SGS_API int sgs_ppr_info(sgs_ppr *p, uint32_t *nv, uint64_t *ne);
+SGS_API int sgs_ppr_export(sgs_ppr *p, uint64_t *row, uint32_t *col, int mem);
+SGS_API int sgs_ppr_forward(sgs_ppr *p, const double *w, const double *T,
+                            uint32_t K, double alpha, double tol,
+                            uint32_t max_iter, double *X, int *iters, int mem);
+/* Adjoint for the upstream gradient G = dL/dX of a forward result X:
+ *     Y = G + alpha P Y,  gT = dL/dT = (1-alpha) Y,
+ *     gw[e=(u,v)] = dL/dw_uv = sum_k X[u,k] (alpha Y[v,k] - Y[u,k] + G[u,k]) / s_u
+ * gw or gT may be NULL to skip them. */
+SGS_API int sgs_ppr_backward(sgs_ppr *p, const double *w, const double *X,
+                             const double *G, uint32_t K, double alpha,
+                             double tol, uint32_t max_iter, double *gw,
+                             double *gT, int *iters, int mem);
+
 #ifdef __cplusplus
 }
 #endif
