@@ -57,6 +57,13 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="snapshot", choices=["snapshot", "ppr"],
+                    help="snapshot: incremental SSSP/BFS/CC (the headline); ppr: weighted "
+                         "personalized PageRank forward + adjoint")
+    ap.add_argument("--ppr-scale", type=int, default=22)
+    ap.add_argument("--ppr-vectors", type=int, default=64)
+    ap.add_argument("--ppr-seeds", type=int, default=32)
+    ap.add_argument("--ppr-targets", type=int, default=1024)
     return ap.parse_args()
 
 
@@ -219,6 +226,7 @@ def engine_arm(a, R):
     R.barrier()
     torch.cuda.synchronize()
     e.synchronize()
+    launches0 = e.engine_stats()["kernel_launches"]
     clocks.start()
     w0 = time.perf_counter()
     edges = 0
@@ -235,6 +243,7 @@ def engine_arm(a, R):
     R.barrier()
     wall_ms = (time.perf_counter() - w0) * 1e3
     clk = clocks.stop()
+    gpu_launches = int(e.engine_stats()["kernel_launches"] - launches0)
     kst = e.kernel_stats()
     e.kernel_timing(False)
     del dev_batches
@@ -321,7 +330,7 @@ def engine_arm(a, R):
                    "parallelism": "replicas" if R.world > 1 else "single GPU",
                    "queries": ["sssp:0", "bfs:0", "cc"]},
         "e2e": e2e,
-        "gpu_launches": None,
+        "gpu_launches": gpu_launches,
         "roofline": roof,
         "clocks": clk,
         "wall_ms_timed": round(wall_ms, 2),
@@ -333,6 +342,7 @@ def engine_arm(a, R):
                          for k, v in kst.items()},
     }
     out["gpu_launches_relax"] = launches
+    out["gpu_launches_note"] = "own kernels only; CUB sorts/scans of the update batch not counted"
     if R.rank == 0 and R.world == 1 and not a.no_cpu:
         out["cpu_baseline"] = cpu_baseline(e, a)
     e.close()
@@ -375,6 +385,168 @@ def cpu_baseline(e, a):
                       "from source 0, each stopped after %d relaxations, plus full directed CC, on the "
                       "final scale-%d graph; single thread" % (budget, a.scale),
             "parts": {k: {"edges": int(v[0]), "s": round(v[1], 3)} for k, v in parts.items()}}
+
+
+# ----------------------------------------------------------------- PPR adjoint arm
+PPR_METRIC = ("PPR forward+adjoint relaxations/s (weighted personalized PageRank, R-MAT s{scale}, "
+              "{K} vectors x {seeds} seeds, loss on {targets} targets)")
+PPR_UNIT = "G edge-vector relaxations/s"
+
+
+def ppr_inputs(nv, ne, a):
+    """Seeded synthetic inputs: fp32 weights log-uniform in [0.1, 10] (the
+    row normalisation happens inside P), K teleport vectors with mass 1/seeds
+    on `seeds` random vertices each, and `targets` random target vertices
+    (loss = sum of all K scores over the targets, so dL/dX = 1 on their rows)."""
+    rng = np.random.default_rng(a.seed)
+    w32 = np.exp(rng.uniform(np.log(0.1), np.log(10.0), ne)).astype(np.float32)
+    K = a.ppr_vectors
+    T = np.zeros((nv, K), np.float32)
+    for k in range(K):
+        T[rng.choice(nv, a.ppr_seeds, replace=False), k] = 1.0 / a.ppr_seeds
+    targets = np.sort(rng.choice(nv, a.ppr_targets, replace=False)).astype(np.int64)
+    return w32, T, targets
+
+
+def ppr_arm(a, R):
+    """One step = forward solve of all K vectors + adjoint solve + per-edge and
+    teleport gradients, through the C ABI on device-resident FP64 inputs;
+    device time from the library's CUDA events.  e2e: the torch op
+    (sgs.autograd.personalized_pagerank) from pinned host fp32 inputs to the
+    loss and dL/dw back on the host."""
+    import torch
+
+    import sgs
+    from sgs.autograd import personalized_pagerank
+
+    dev = torch.device("cuda", R.local)
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    e = sgs.Engine(device=R.local, weight_mode=sgs.W_UNIT)
+    e.load_rmat(a.ppr_scale, a.edge_factor, a.seed, 0.57, 0.19, 0.19, wseed=a.seed)
+    g = sgs.Ppr(engine=e)
+    e.close()
+    nv, ne, K = g.nv, g.ne, a.ppr_vectors
+    w32, T32, targets = ppr_inputs(nv, ne, a)
+    t_gen = time.time() - t0
+    w = torch.from_numpy(w32).to(dev).double()
+    T = torch.from_numpy(T32).to(dev).double()
+    G = torch.zeros(nv, K, dtype=torch.float64, device=dev)
+    G[torch.from_numpy(targets).to(dev)] = 1.0
+    tol = 1e-10 * nv * K
+
+    def step():
+        X = g.forward(w, T, tol=tol)
+        sf = g.stats()
+        gw, gT = g.backward(w, X, G, tol=tol)
+        sb = g.stats()
+        return sf, sb
+
+    for _ in range(a.warmup):
+        step()
+    g.timing(True)
+    clocks = Clocks(R.local)
+    R.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    w0 = time.perf_counter()
+    dev_ms, steps_ms, relax, nbytes, nsteps, it_f, it_b = 0.0, 0.0, 0, 0.0, 0, 0, 0
+    l0 = g.stats()["kernel_launches"]
+    for _ in range(a.steps):
+        sf, sb = step()
+        dev_ms += sf["ms"] + sb["ms"]
+        steps_ms += sf["steps_ms"] + sb["steps_ms"]
+        nsteps += sf["iters"] + sb["iters"]
+        it_f, it_b = sf["iters"], sb["iters"]
+        relax += ne * K * (sf["iters"] + sb["iters"])
+        nbytes += sf["bytes_alg_step"] * sf["iters"] + sb["bytes_alg_step"] * sb["iters"]
+    torch.cuda.synchronize()
+    R.barrier()
+    wall_ms = (time.perf_counter() - w0) * 1e3
+    clk = clocks.stop()
+    launches = int(g.stats()["kernel_launches"] - l0)
+    g.timing(False)
+    st = g.stats()
+    T_ms = R.max(dev_ms)
+    value = R.sum(relax) / (T_ms * 1e6)
+    peak, peak_src = measured_peak_hbm()
+    achieved = nbytes / (steps_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": "k_ppr_step (+ k_ppr_finalize for hub pieces)",
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": peak_src, "traffic": None,
+            "launches": nsteps, "avg_launch_ms": round(steps_ms / nsteps, 4),
+            "alg_bytes_per_launch": sf["bytes_alg_step"]}
+    # ---------------- e2e through the torch op from pinned host memory
+    e2e = None
+    if not a.no_e2e:
+        wp = torch.from_numpy(w32).pin_memory()
+        Tp = torch.from_numpy(T32).pin_memory()
+        tp = torch.from_numpy(targets).pin_memory()
+        R.barrier()
+        torch.cuda.synchronize()
+        e_ms, d2h = 0.0, 0
+        for _ in range(a.steps):
+            t1 = time.perf_counter()
+            wd = wp.to(dev, non_blocking=True).requires_grad_(True)
+            Td = Tp.to(dev, non_blocking=True)
+            td = tp.to(dev, non_blocking=True)
+            X = personalized_pagerank(g, wd, Td, tol=tol)
+            loss = X[td].sum()
+            loss.backward()
+            lh = loss.detach().cpu()
+            gh = wd.grad.cpu()
+            e_ms += (time.perf_counter() - t1) * 1e3
+            d2h = lh.numel() * lh.element_size() + gh.numel() * gh.element_size()
+            del X, loss, wd
+        e_ms = R.max(e_ms)
+        e2e = {"value": round(R.sum(relax) / (e_ms * 1e6), 3), "unit": PPR_UNIT,
+               "h2d_bytes_per_step": int(w32.nbytes + T32.nbytes + targets.nbytes),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e_ms / a.steps, 2),
+               "path": "sgs.autograd.personalized_pagerank forward + loss.backward()"}
+    out = {
+        "metric": PPR_METRIC.format(scale=a.ppr_scale, K=K, seeds=a.ppr_seeds, targets=a.ppr_targets),
+        "value": round(value, 3), "unit": PPR_UNIT, "n_gpus": R.world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": round(T_ms / a.steps, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (device R-MAT; seeded fp32 log-uniform weights, teleport seeds, targets)",
+        "config": {"workload": f"PPR forward + adjoint, R-MAT scale {a.ppr_scale} ef {a.edge_factor} "
+                               f"seed {a.seed}, {K} vectors x {a.ppr_seeds} seeds, {a.ppr_targets} targets, "
+                               f"alpha 0.85, stop at L1 step change < {tol:.3g}",
+                   "nv": nv, "ne": ne, "iters_forward": it_f, "iters_adjoint": it_b,
+                   "hub_pieces_csc": st["pieces_in"], "hub_pieces_csr": st["pieces_out"],
+                   "l2": "inputs larger than L2 (state %.1f GB vs %d MB L2)" % (
+                       nv * K * 8 / 1e9, L2_BYTES // 2**20),
+                   "parallelism": "replicas" if R.world > 1 else "single GPU"},
+        "e2e": e2e, "gpu_launches": launches, "roofline": roof, "clocks": clk,
+        "wall_ms_timed": round(wall_ms, 2), "gen_s": round(t_gen, 2),
+    }
+    if R.rank == 0 and R.world == 1 and not a.no_cpu:
+        out["cpu_baseline"] = ppr_cpu_baseline(g, w32, T32, a)
+    g.close()
+    return out
+
+
+def ppr_cpu_baseline(g, w32, T32, a):
+    """The same Jacobi step on the host (scipy CSR times the [nv, K] state,
+    single thread), a bounded number of steps; relaxations/s."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import ppr_dense as D
+
+    row, col = g.export()
+    nv, ne, K = g.nv, g.ne, T32.shape[1]
+    PT = D.sparse_pt(nv, row, col, w32.astype(np.float64))
+    t = time.perf_counter()
+    X, k = D.ppr_jacobi_sparse(nv, row, col, None, T32, iters=1, PT=PT)
+    dt = time.perf_counter() - t
+    more = int(a.cpu_seconds / max(dt, 1e-3)) - 1
+    if more > 0:
+        t = time.perf_counter()
+        _, k2 = D.ppr_jacobi_sparse(nv, row, col, None, T32, iters=min(more, 20), X0=X, PT=PT)
+        dt += time.perf_counter() - t
+        k += k2
+    return {"value": round(ne * K * k / dt / 1e9, 4), "unit": PPR_UNIT, "cores": 1, "kind": "port",
+            "sample": f"{k} Jacobi steps of the forward solve (all {K} vectors) on the same graph, "
+                      "scipy CSR times the dense state on one thread (matrix build not timed)"}
 
 
 # ----------------------------------------------------------------- reference arm
@@ -451,8 +623,14 @@ def main():
     a = parse()
     R = Ranks()
     try:
-        if a.impl == "reference":
+        if a.impl == "reference" and a.workload == "ppr":
+            out = None if R.rank else {
+                "impl": "reference", "unavailable": "the reference has no personalized PageRank "
+                "or adjoint (its PageRank is the single unweighted vector of the snapshot workload)"}
+        elif a.impl == "reference":
             out = reference_arm(a, R)
+        elif a.workload == "ppr":
+            out = ppr_arm(a, R)
         else:
             out = engine_arm(a, R)
         if R.rank == 0 and out is not None:

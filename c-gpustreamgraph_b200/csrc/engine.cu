@@ -208,6 +208,7 @@ struct sgs_engine {
   bool ktiming = false;
   std::vector<cudaEvent_t> kev;  // 2 per queued launch
   sgs_kernel_stats kst[SGS_K_COUNT]{};
+  uint64_t n_launch = 0;  // this engine's own kernel launches (library sorts/scans excluded)
 
   std::vector<std::unique_ptr<Query>> queries;
   std::vector<std::unique_ptr<Group>> groups;
@@ -303,8 +304,8 @@ struct sgs_engine {
       fail(SGS_ERR_INVALID, "explicit weight mode needs weights");
     {
       CK(cudaMemsetAsync(b_err.p, 0, sizeof(unsigned int), s));
-      k_validate_csr<<<grid_elem(std::max<uint64_t>(ne_in, nv)), 256, 0, s>>>(
-          d_row, d_col, cfg.weight_mode == SGS_W_EXPLICIT ? d_w : nullptr, n, ne_in, b_err.p);
+      { ++n_launch; k_validate_csr<<<grid_elem(std::max<uint64_t>(ne_in, nv)), 256, 0, s>>>(
+          d_row, d_col, cfg.weight_mode == SGS_W_EXPLICIT ? d_w : nullptr, n, ne_in, b_err.p); }
       CK(cudaGetLastError());
       unsigned int herr = 0;
       CK(cudaMemcpyAsync(&herr, b_err.p, sizeof(herr), cudaMemcpyDeviceToHost, s));
@@ -317,16 +318,16 @@ struct sgs_engine {
     slots.ensure(nv);
     live.ensure(nv);
     cap.ensure(nv);
-    k_row_degrees<<<grid_elem(nv), 256, 0, s>>>(d_row, nv, slots.p);
+    { ++n_launch; k_row_degrees<<<grid_elem(nv), 256, 0, s>>>(d_row, nv, slots.p); }
     CK(cudaGetLastError());
     layout_from(slots.p, /*extra=*/0);
     CK(cudaMemcpyAsync(live.p, slots.p, sizeof(uint32_t) * nv, cudaMemcpyDeviceToDevice, s));
     // copy lists
     reset_counters(1);
     FrontierView f0 = fview(0, special(0));
-    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), f0);
+    { ++n_launch; k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), f0); }
     LoadCsrOp op{view(), d_row, d_col, cfg.weight_mode == SGS_W_EXPLICIT ? d_w : nullptr};
-    seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(f0, fview(1, special(1)), op, nullptr);
+    { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(f0, fview(1, special(1)), op, nullptr); }
     CK(cudaGetLastError());
     sync();
     ne = ne_in;
@@ -340,8 +341,8 @@ struct sgs_engine {
   void layout_from(const uint32_t *sz, uint64_t extra) {
     DBuf<uint64_t> scan;
     scan.ensure((size_t)nv + 1);
-    k_layout_caps<<<grid_elem(nv), 256, 0, s>>>(sz, nv, cfg.slack_div, cap.p);
-    k_u32_to_u64<<<grid_elem(nv), 256, 0, s>>>(cap.p, nv, scan.p);
+    { ++n_launch; k_layout_caps<<<grid_elem(nv), 256, 0, s>>>(sz, nv, cfg.slack_div, cap.p); }
+    { ++n_launch; k_u32_to_u64<<<grid_elem(nv), 256, 0, s>>>(cap.p, nv, scan.p); }
     CK(cudaMemsetAsync(scan.p + nv, 0, sizeof(uint64_t), s));
     size_t tb = 0;
     CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, scan.p, scan.p, (int)(nv + 1), s));
@@ -388,7 +389,7 @@ struct sgs_engine {
     }
     arena_cap[0] = cap_d;
     arena_cap[1] = cap_h;
-    k_assign_off<<<grid_elem(nv), 256, 0, s>>>(scan.p, nv, sp, hs[sp], off.p);
+    { ++n_launch; k_assign_off<<<grid_elem(nv), 256, 0, s>>>(scan.p, nv, sp, hs[sp], off.p); }
     unsigned long long tops[2] = {need_d, need_h};
     CK(cudaMemcpyAsync(arena_top.p, tops, sizeof(tops), cudaMemcpyHostToDevice, s));
     ensure_frontier(cap_d + cap_h);
@@ -431,9 +432,9 @@ struct sgs_engine {
     layout_from(slots.p, extra);
     reset_counters(1);
     FrontierView f0 = fview(0, special(0));
-    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), f0);
+    { ++n_launch; k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), f0); }
     CopyBlockOp op{view(), old_off.p, off.p, od.p, ow.p, oh.p, ohw.p};
-    seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(f0, fview(1, special(1)), op, nullptr);
+    { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(f0, fview(1, special(1)), op, nullptr); }
     CK(cudaGetLastError());
     sync();
     ++repacks;
@@ -502,10 +503,10 @@ struct sgs_engine {
         const bool hp = rr >= 1;
         if (ktiming) CK(cudaEventRecord(kev[2 * k], s));
         if (rr == 0 && round0) nvtxRangePushA(round0);
-        group_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
+        { ++n_launch; group_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
             fview(rr, cnt.p + rr), fview(rr + 1, cnt.p + rr + 1), op,
             hp ? fb[(rr - 1) % 3].vtx.p : nullptr, hp ? cnt.p + rr - 1 : nullptr,
-            hp ? gm[(rr - 1) % 3].p : nullptr, b_lane.p, rstat.p + rr);
+            hp ? gm[(rr - 1) % 3].p : nullptr, b_lane.p, rstat.p + rr); }
         if (rr == 0 && round0) nvtxRangePop();
         if (ktiming) CK(cudaEventRecord(kev[2 * k + 1], s));
       }
@@ -522,8 +523,8 @@ struct sgs_engine {
       for (uint32_t k = 0; k < nb; ++k)
         if (h_cnt[k + 1] == 0) {
           const uint32_t z = r + k + 1;  // first empty frontier
-          k_clear_masks<<<grid_elem(nv), 256, 0, s>>>(fb[(z - 1) % 3].vtx.p, cnt.p + z - 1,
-                                                      gm[(z - 1) % 3].p);
+          { ++n_launch; k_clear_masks<<<grid_elem(nv), 256, 0, s>>>(fb[(z - 1) % 3].vtx.p, cnt.p + z - 1,
+                                                      gm[(z - 1) % 3].p); }
           CK(cudaGetLastError());
           converged = true;
           return z;
@@ -533,7 +534,7 @@ struct sgs_engine {
     }
     // not converged: leave the masks clean for the next call
     for (uint32_t f = (r >= 1 ? r - 1 : 0); f <= r; ++f)
-      k_clear_masks<<<grid_elem(nv), 256, 0, s>>>(fb[f % 3].vtx.p, cnt.p + f, gm[f % 3].p);
+      { ++n_launch; k_clear_masks<<<grid_elem(nv), 256, 0, s>>>(fb[f % 3].vtx.p, cnt.p + f, gm[f % 3].p); }
     CK(cudaGetLastError());
     return r;
   }
@@ -555,7 +556,7 @@ struct sgs_engine {
   uint32_t pr_rounds(Query &q, unsigned long long *edge_stat, bool &conv, double &last_l1) {
     GraphView g = view();
     reset_counters(0);
-    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(g, fview(0, cnt.p));
+    { ++n_launch; k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(g, fview(0, cnt.p)); }
     const uint32_t maxr = cfg.max_rounds;
     CK(cudaMemsetAsync(l1.p, 0, sizeof(double) * (maxr + 2), s));
     std::vector<double> hl(maxr + 2);
@@ -571,11 +572,11 @@ struct sgs_engine {
       const uint32_t nb = std::min(rb, maxr - r);
       if (ktiming) ensure_kev(2 * nb);
       for (uint32_t k = 0; k < nb; ++k) {
-        k_pr_absorb<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(g, q.x.p, q.r.p, q.pv.p, cfg.pr_alpha,
-                                                           l1.p + r + k);
+        { ++n_launch; k_pr_absorb<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(g, q.x.p, q.r.p, q.pv.p, cfg.pr_alpha,
+                                                           l1.p + r + k); }
         if (ktiming) CK(cudaEventRecord(kev[2 * k], s));
-        seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, cnt.p), fview(1, cnt.p + 1), op,
-                                                     edge_stat);
+        { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, cnt.p), fview(1, cnt.p + 1), op,
+                                                     edge_stat); }
         if (ktiming) CK(cudaEventRecord(kev[2 * k + 1], s));
       }
       CK(cudaGetLastError());
@@ -626,7 +627,7 @@ struct sgs_engine {
     CK(cudaMemsetAsync(b_stat.p, 0, sizeof(unsigned long long) * 8, s));
     bool conv = false;
     double l1v = 0;
-    k_pr_init<<<grid_elem(nv), 256, 0, s>>>(q.x.p, q.r.p, nv, 1.0 - cfg.pr_alpha);
+    { ++n_launch; k_pr_init<<<grid_elem(nv), 256, 0, s>>>(q.x.p, q.r.p, nv, 1.0 - cfg.pr_alpha); }
     const uint32_t rounds = pr_rounds(q, b_stat.p + 4, conv, l1v);
     CK(cudaEventRecord(ev_q.b, s));
     unsigned long long e = 0;
@@ -650,13 +651,13 @@ struct sgs_engine {
     GraphView g = view();
     CK(cudaEventRecord(ev_q.a, s));
     CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * GMAX, s));
-    k_group_init_lane<Group::S><<<grid_elem(nv), 256, 0, s>>>(G.st.p, G.val.p, nv, l, q.algo, q.source);
+    { ++n_launch; k_group_init_lane<Group::S><<<grid_elem(nv), 256, 0, s>>>(G.st.p, G.val.p, nv, l, q.algo, q.source); }
     reset_counters(0);
     if (q.algo == SGS_CC)
-      k_group_dense<Group::S><<<grid_elem(nv), 256, 0, s>>>(g, G.val.p, 1u << l, G.algo(), gm[0].p,
-                                                            fview(0, cnt.p));
+      { ++n_launch; k_group_dense<Group::S><<<grid_elem(nv), 256, 0, s>>>(g, G.val.p, 1u << l, G.algo(), gm[0].p,
+                                                            fview(0, cnt.p)); }
     else
-      k_group_seed_one<<<1, 32, 0, s>>>(g, q.source, 1u << l, gm[0].p, fview(0, cnt.p));
+      { ++n_launch; k_group_seed_one<<<1, 32, 0, s>>>(g, q.source, 1u << l, gm[0].p, fview(0, cnt.p)); }
     CK(cudaGetLastError());
     bool conv = false;
     const uint32_t rounds = group_relax(G, conv);
@@ -770,11 +771,11 @@ struct sgs_engine {
     CK(cudaMemsetAsync(b_err.p, 0, sizeof(unsigned int), s));
     CK(cudaMemsetAsync(b_stat.p, 0, sizeof(unsigned long long) * 8, s));
     if (ni)
-      k_make_keys<<<grid_elem(ni), 256, 0, s>>>(b_isrc.p, b_idst.p, ni, nv, b_ikeys.p,
-                                                explicit_w ? b_iw.p : nullptr, explicit_w, b_err.p);
+      { ++n_launch; k_make_keys<<<grid_elem(ni), 256, 0, s>>>(b_isrc.p, b_idst.p, ni, nv, b_ikeys.p,
+                                                explicit_w ? b_iw.p : nullptr, explicit_w, b_err.p); }
     if (nd)
-      k_make_keys<<<grid_elem(nd), 256, 0, s>>>(b_dsrc.p, b_ddst.p, nd, nv, b_dkeys.p, nullptr, 0,
-                                                b_err.p);
+      { ++n_launch; k_make_keys<<<grid_elem(nd), 256, 0, s>>>(b_dsrc.p, b_ddst.p, nd, nv, b_dkeys.p, nullptr, 0,
+                                                b_err.p); }
     const int eb = sort_bits();
     size_t tb = 0, t2 = 0, t3 = 0;
     if (nd) CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, b_dkeys.p, b_dkeys_s.p, (int)nd, 0, eb, s));
@@ -789,8 +790,8 @@ struct sgs_engine {
     if (ni) {
       CK(cub::DeviceRadixSort::SortPairs(cub_tmp.p, t2, b_ikeys.p, b_ikeys_s.p,
                                          explicit_w ? b_iw.p : b_isrc.p, b_iw_s.p, (int)ni, 0, eb, s));
-      k_filter_inserts<<<grid_elem(ni), 256, 0, s>>>(b_ikeys_s.p, (uint32_t)ni, b_dkeys_s.p,
-                                                     (uint32_t)nd, b_flag.p);
+      { ++n_launch; k_filter_inserts<<<grid_elem(ni), 256, 0, s>>>(b_ikeys_s.p, (uint32_t)ni, b_dkeys_s.p,
+                                                     (uint32_t)nd, b_flag.p); }
       CK(cub::DeviceSelect::Flagged(cub_tmp.p, t3, b_ikeys_s.p, b_flag.p, b_ikept.p, b_nkept.p,
                                     (int)ni, s));
       if (explicit_w)
@@ -821,8 +822,8 @@ struct sgs_engine {
         Query &q = *qp;
         if (q.algo != SGS_PR) continue;
         PrAmendOp op{g, q.x.p, q.r.p, -cfg.pr_alpha};
-        seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(2)), fview(1, special(3)), op,
-                                                     nullptr);
+        { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(2)), fview(1, special(3)), op,
+                                                     nullptr); }
       }
     }
     // ---- deletion phase: parent-tree invalidation on the old graph, all
@@ -835,9 +836,9 @@ struct sgs_engine {
       CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * GMAX, s));
       CK(cudaMemsetAsync(b_inval.p, 0, sizeof(unsigned long long) * GMAX, s));
       reset_counters(0);
-      k_group_seed_deleted<Group::S><<<grid_elem(nd), 256, 0, s>>>(
+      { ++n_launch; k_group_seed_deleted<Group::S><<<grid_elem(nd), 256, 0, s>>>(
           g, G.st.p, G.val.p, G.used, G.algo(), b_dkeys_s.p, (uint32_t)nd, b_inval.p, gm[0].p,
-          fview(0, cnt.p));
+          fview(0, cnt.p)); }
       CK(cudaGetLastError());
       bool conv = false;
       run_group_rounds(
@@ -877,8 +878,8 @@ struct sgs_engine {
         Query &q = *qp;
         if (q.algo != SGS_PR) continue;
         PrAmendOp op{g, q.x.p, q.r.p, cfg.pr_alpha};
-        seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(2)), fview(1, special(3)), op,
-                                                     nullptr);
+        { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(2)), fview(1, special(3)), op,
+                                                     nullptr); }
       }
       for (auto &qp : queries) {
         Query &q = *qp;
@@ -917,12 +918,12 @@ struct sgs_engine {
       CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * GMAX, s));
       reset_counters(0);
       if (any_inval) {
-        k_group_dense<Group::S><<<grid_elem(nv), 256, 0, s>>>(g, G.val.p, G.used, G.algo(), gm[0].p,
-                                                              fview(0, cnt.p));
+        { ++n_launch; k_group_dense<Group::S><<<grid_elem(nv), 256, 0, s>>>(g, G.val.p, G.used, G.algo(), gm[0].p,
+                                                              fview(0, cnt.p)); }
       } else if (ni) {
-        k_group_relax_inserted<Group::S><<<grid_elem(ni), 256, 0, s>>>(
+        { ++n_launch; k_group_relax_inserted<Group::S><<<grid_elem(ni), 256, 0, s>>>(
             g, G.st.p, G.val.p, G.used, G.algo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr, b_nkept.p,
-            gm[0].p, fview(0, cnt.p), b_lane.p);
+            gm[0].p, fview(0, cnt.p), b_lane.p); }
       }
       CK(cudaGetLastError());
       bool conv = false;
@@ -953,11 +954,11 @@ struct sgs_engine {
     const uint32_t st = ++estamp;
     CK(cudaMemsetAsync(special(2), 0, sizeof(unsigned long long), s));
     if (nd)
-      k_group_heads<<<grid_elem(nd), 256, 0, s>>>(g, b_dkeys_s.p, nullptr, (uint32_t)nd, nullptr,
-                                                  emark.p, st, fview(0, special(2)));
+      { ++n_launch; k_group_heads<<<grid_elem(nd), 256, 0, s>>>(g, b_dkeys_s.p, nullptr, (uint32_t)nd, nullptr,
+                                                  emark.p, st, fview(0, special(2))); }
     if (ni)
-      k_group_heads<<<grid_elem(ni), 256, 0, s>>>(g, b_ikept.p, b_nkept.p, 0, nullptr, emark.p, st,
-                                                  fview(0, special(2)));
+      { ++n_launch; k_group_heads<<<grid_elem(ni), 256, 0, s>>>(g, b_ikept.p, b_nkept.p, 0, nullptr, emark.p, st,
+                                                  fview(0, special(2))); }
     CK(cudaGetLastError());
   }
 
@@ -971,11 +972,11 @@ struct sgs_engine {
     if (nd) {
       CK(cudaMemsetAsync(special(4), 0, sizeof(unsigned long long), s));
       b_gstart.ensure((size_t)nv + 1);
-      k_group_heads<<<grid_elem(nd), 256, 0, s>>>(g, b_dkeys_s.p, nullptr, (uint32_t)nd, b_gstart.p,
-                                                  nullptr, 0, fview(0, special(4)));
+      { ++n_launch; k_group_heads<<<grid_elem(nd), 256, 0, s>>>(g, b_dkeys_s.p, nullptr, (uint32_t)nd, b_gstart.p,
+                                                  nullptr, 0, fview(0, special(4))); }
       TombOp op{g, b_dkeys_s.p, b_gstart.p, (uint32_t)nd};
-      seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(4)), fview(1, special(5)), op,
-                                                   tombs);
+      { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(4)), fview(1, special(5)), op,
+                                                   tombs); }
       CK(cudaGetLastError());
     }
     uint32_t nkept = 0;
@@ -990,7 +991,7 @@ struct sgs_engine {
       c.wbase = wbase.p;
       // dry run: relocation demand per tier
       CK(cudaMemsetAsync(b_stat.p, 0, sizeof(unsigned long long) * 2, s));
-      k_insert_plan<<<grid_elem(ni), 256, 0, s>>>(g, b_ikept.p, b_nkept.p, c, 1, b_stat.p);
+      { ++n_launch; k_insert_plan<<<grid_elem(ni), 256, 0, s>>>(g, b_ikept.p, b_nkept.p, c, 1, b_stat.p); }
       unsigned long long h[2], tops[2];
       CK(cudaMemcpyAsync(h, b_stat.p, sizeof(h), cudaMemcpyDeviceToHost, s));
       CK(cudaMemcpyAsync(tops, arena_top.p, sizeof(tops), cudaMemcpyDeviceToHost, s));
@@ -1013,14 +1014,14 @@ struct sgs_engine {
       c.rl_count64 = rl_count.p;
       CK(cudaMemsetAsync(rl_count.p, 0, sizeof(unsigned long long), s));
       CK(cudaMemsetAsync(b_err.p, 0, sizeof(unsigned int), s));
-      k_insert_plan<<<grid_elem(ni), 256, 0, s>>>(g, b_ikept.p, b_nkept.p, c, 0, nullptr);
-      k_insert_write<<<grid_elem(ni), 256, 0, s>>>(
-          g, b_ikept.p, cfg.weight_mode == SGS_W_EXPLICIT ? b_iw_kept.p : nullptr, b_nkept.p, wbase.p);
+      { ++n_launch; k_insert_plan<<<grid_elem(ni), 256, 0, s>>>(g, b_ikept.p, b_nkept.p, c, 0, nullptr); }
+      { ++n_launch; k_insert_write<<<grid_elem(ni), 256, 0, s>>>(
+          g, b_ikept.p, cfg.weight_mode == SGS_W_EXPLICIT ? b_iw_kept.p : nullptr, b_nkept.p, wbase.p); }
       CK(cudaMemsetAsync(special(6), 0, sizeof(unsigned long long), s));
-      k_reloc_frontier<<<grid_elem(nkept), 256, 0, s>>>(rl_count.p, rl_len.p, fview(0, special(6)));
+      { ++n_launch; k_reloc_frontier<<<grid_elem(nkept), 256, 0, s>>>(rl_count.p, rl_len.p, fview(0, special(6))); }
       RelocCopyOp op{g, rl_from.p, rl_to.p};
-      seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(6)), fview(1, special(7)), op,
-                                                   nullptr);
+      { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(6)), fview(1, special(7)), op,
+                                                   nullptr); }
       CK(cudaGetLastError());
       unsigned int herr = 0;
       unsigned long long hrl = 0;
@@ -1054,9 +1055,9 @@ struct sgs_engine {
     DBuf<uint32_t> tmp;
     tmp.ensure(nv);
     if (field == SGS_FIELD_PARENT)
-      k_group_split<Group::S><<<grid_elem(nv), 256, 0, s>>>(q.grp->st.p, nv, q.lane, nullptr, tmp.p);
+      { ++n_launch; k_group_split<Group::S><<<grid_elem(nv), 256, 0, s>>>(q.grp->st.p, nv, q.lane, nullptr, tmp.p); }
     else if (field == SGS_FIELD_VALUE || field == SGS_FIELD_BUFFER)
-      k_group_split<Group::S><<<grid_elem(nv), 256, 0, s>>>(q.grp->st.p, nv, q.lane, tmp.p, nullptr);
+      { ++n_launch; k_group_split<Group::S><<<grid_elem(nv), 256, 0, s>>>(q.grp->st.p, nv, q.lane, tmp.p, nullptr); }
     else
       fail(SGS_ERR_INVALID, "unknown field");
     CK(cudaMemcpyAsync(out, tmp.p, sizeof(uint32_t) * nv, kind, s));
@@ -1066,10 +1067,10 @@ struct sgs_engine {
   void summary(Query &q, uint64_t out[4]) {
     CK(cudaMemsetAsync(b_stat.p, 0, sizeof(unsigned long long) * 4, s));
     if (q.algo == SGS_PR) {
-      k_summary_pr<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.x.p, nv, (double *)b_stat.p + 1);
+      { ++n_launch; k_summary_pr<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.x.p, nv, (double *)b_stat.p + 1); }
     } else {
-      k_group_summary<Group::S><<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.grp->st.p, nv, q.lane,
-                                                                         b_stat.p);
+      { ++n_launch; k_group_summary<Group::S><<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.grp->st.p, nv, q.lane,
+                                                                         b_stat.p); }
     }
     CK(cudaGetLastError());
     unsigned long long h[4];
@@ -1082,7 +1083,7 @@ struct sgs_engine {
   void export_graph(uint64_t *row, uint32_t *col, uint32_t *w, int mem) {
     DBuf<uint64_t> drow;
     drow.ensure((size_t)nv + 1);
-    k_u32_to_u64<<<grid_elem(nv), 256, 0, s>>>(live.p, nv, drow.p);
+    { ++n_launch; k_u32_to_u64<<<grid_elem(nv), 256, 0, s>>>(live.p, nv, drow.p); }
     CK(cudaMemsetAsync(drow.p + nv, 0, sizeof(uint64_t), s));
     size_t tb = 0;
     CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, drow.p, drow.p, (int)(nv + 1), s));
@@ -1094,10 +1095,10 @@ struct sgs_engine {
     fill.ensure(nv);
     CK(cudaMemsetAsync(fill.p, 0, sizeof(uint32_t) * nv, s));
     reset_counters(0);
-    k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), fview(0, special(0)));
+    { ++n_launch; k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(view(), fview(0, special(0))); }
     ExportOp op{view(), drow.p, dcol.p, w ? dw.p : nullptr, fill.p};
-    seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(0)), fview(1, special(1)), op,
-                                                 nullptr);
+    { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(0)), fview(1, special(1)), op,
+                                                 nullptr); }
     CK(cudaGetLastError());
     const cudaMemcpyKind kind = mem == SGS_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     CK(cudaMemcpyAsync(row, drow.p, sizeof(uint64_t) * (nv + 1), kind, s));
@@ -1121,7 +1122,7 @@ struct sgs_engine {
     DBuf<uint64_t> k1, k2;
     k1.ensure(m);
     k2.ensure(m);
-    k_rmat<<<grid_elem(m), 256, 0, s>>>(scale, m, key, tA, tAB, tABC, 1, k1.p);
+    { ++n_launch; k_rmat<<<grid_elem(m), 256, 0, s>>>(scale, m, key, tA, tAB, tABC, 1, k1.p); }
     size_t tb = 0, tu = 0;
     DBuf<uint32_t> nsel;
     nsel.ensure(1);
@@ -1144,12 +1145,12 @@ struct sgs_engine {
     DBuf<uint32_t> col, w;
     row.ensure((size_t)n + 1);
     col.ensure(hn + 1);
-    k_row_from_sorted<<<grid_elem(n + 1), 256, 0, s>>>(k1.p, nsel.p, n, row.p);
-    k_keys_low<<<grid_elem(hn), 256, 0, s>>>(k1.p, nsel.p, col.p);
+    { ++n_launch; k_row_from_sorted<<<grid_elem(n + 1), 256, 0, s>>>(k1.p, nsel.p, n, row.p); }
+    { ++n_launch; k_keys_low<<<grid_elem(hn), 256, 0, s>>>(k1.p, nsel.p, col.p); }
     if (cfg.weight_mode == SGS_W_EXPLICIT) {
       w.ensure(hn + 1);
       const uint64_t wkey = fin64_host(wseed ^ 0x57454947ull);
-      k_hash_weights<<<grid_elem(hn), 256, 0, s>>>(k1.p, nsel.p, wkey, w.p);
+      { ++n_launch; k_hash_weights<<<grid_elem(hn), 256, 0, s>>>(k1.p, nsel.p, wkey, w.p); }
     }
     CK(cudaGetLastError());
     k1.release();
@@ -1364,6 +1365,7 @@ SGS_API int sgs_get_engine_stats(sgs_engine *e, sgs_engine_stats *out) {
     e->est.nv = e->nv;
     e->est.ne = e->ne;
     e->est.repacks = e->repacks;
+    e->est.kernel_launches = e->n_launch;
     unsigned long long tops[2] = {0, 0};
     if (e->loaded) {
       CK(cudaMemcpyAsync(tops, e->arena_top.p, sizeof(tops), cudaMemcpyDeviceToHost, e->s));

@@ -379,11 +379,53 @@ struct sgs_ppr {
   Buf<double> w, inv_s, pr, pc, t, x, xn, g, y, yn, part, diff;
   Buf<unsigned int> err;
   Adj in, out;  // CSC (forward) and CSR (adjoint, edge gradient)
+  // timing and counters
+  bool timing = false;
+  std::vector<cudaEvent_t> ev;  // 2 per step of a batch (timing on)
+  cudaEvent_t call_ev[2] = {nullptr, nullptr};
+  sgs_ppr_stats st{};
+  uint64_t n_launch = 0;
   ~sgs_ppr() {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    for (cudaEvent_t e : call_ev)
+      if (e) cudaEventDestroy(e);
     if (s) cudaStreamDestroy(s);
+  }
+  void events() {
+    if (!call_ev[0]) {
+      PCK(cudaEventCreate(&call_ev[0]));
+      PCK(cudaEventCreate(&call_ev[1]));
+    }
+    while (ev.size() < 64) {
+      cudaEvent_t e;
+      PCK(cudaEventCreate(&e));
+      ev.push_back(e);
+    }
+  }
+  // begin/end of a public call: device time of everything on the stream
+  void call_begin() {
+    events();
+    st.iters = 0;
+    st.steps_ms = 0.0;
+    st.ms = 0.0;
+    PCK(cudaEventRecord(call_ev[0], s));
+  }
+  void call_end() {
+    PCK(cudaEventRecord(call_ev[1], s));
+    PCK(cudaEventSynchronize(call_ev[1]));
+    float ms = 0.f;
+    PCK(cudaEventElapsedTime(&ms, call_ev[0], call_ev[1]));
+    st.ms = ms;
+    st.kernel_launches = n_launch;
   }
   uint32_t grid() const { return (uint32_t)nsm * 8; }
   void sync() { PCK(cudaStreamSynchronize(s)); }
+  // algorithmic bytes of one Jacobi step with K columns: per edge the 4-B
+  // neighbour id, the 8-B probability and the neighbour's 8K-B row; per
+  // vertex two 8-B offsets and 8K B each of B and x read and out written
+  double step_bytes(uint32_t K) const {
+    return (double)ne * (12.0 + 8.0 * K) + (double)nv * (16.0 + 24.0 * K);
+  }
   cudaMemcpyKind kin(int mem) const {
     return mem == SGS_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   }
@@ -395,7 +437,7 @@ struct sgs_ppr {
     a.ptr = ptr;
     a.nbr = nbr;
     a.poff.ensure((size_t)nv + 1);
-    k_piece_count<<<grid(), THREADS, 0, s>>>(ptr, nv, a.poff.p);
+    { ++n_launch; k_piece_count<<<grid(), THREADS, 0, s>>>(ptr, nv, a.poff.p); }
     size_t tb = 0;
     PCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, a.poff.p, a.poff.p, (int)(nv + 1), s));
     Buf<unsigned char> tmp;
@@ -404,7 +446,7 @@ struct sgs_ppr {
     PCK(cudaMemcpyAsync(&a.npieces, a.poff.p + nv, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     sync();
     a.pv.ensure(a.npieces);
-    k_piece_fill<<<grid(), THREADS, 0, s>>>(a.poff.p, nv, a.pv.p);
+    { ++n_launch; k_piece_fill<<<grid(), THREADS, 0, s>>>(a.poff.p, nv, a.pv.p); }
     PCK(cudaGetLastError());
   }
 
@@ -419,7 +461,7 @@ struct sgs_ppr {
     if (ne) PCK(cudaMemcpyAsync(col.p, c, sizeof(uint32_t) * ne, kin(mem), s));
     err.ensure(1);
     PCK(cudaMemsetAsync(err.p, 0, sizeof(unsigned int), s));
-    k_validate<<<grid(), THREADS, 0, s>>>(row.p, col.p, nv, ne, err.p);
+    { ++n_launch; k_validate<<<grid(), THREADS, 0, s>>>(row.p, col.p, nv, ne, err.p); }
     unsigned int h = 0;
     PCK(cudaMemcpyAsync(&h, err.p, sizeof(h), cudaMemcpyDeviceToHost, s));
     sync();
@@ -435,8 +477,8 @@ struct sgs_ppr {
       csrc.ensure(ne);
       ceid.ensure(ne);
       crow.ensure((size_t)nv + 1);
-      k_edge_src<<<grid(), THREADS, 0, s>>>(row.p, nv, src.p);
-      k_iota<<<grid(), THREADS, 0, s>>>(eid.p, ne);
+      { ++n_launch; k_edge_src<<<grid(), THREADS, 0, s>>>(row.p, nv, src.p); }
+      { ++n_launch; k_iota<<<grid(), THREADS, 0, s>>>(eid.p, ne); }
       int bits = 1;
       while (bits < 32 && (1ull << bits) < nv) ++bits;
       size_t tb = 0;
@@ -446,8 +488,8 @@ struct sgs_ppr {
       tmp.ensure(tb);
       PCK(cub::DeviceRadixSort::SortPairs(tmp.p, tb, col.p, dst_s.p, eid.p, ceid.p, (int)ne, 0,
                                           bits, s));
-      k_csc_rows<<<grid(), THREADS, 0, s>>>(dst_s.p, ne, nv, crow.p);
-      k_gather_u32<<<grid(), THREADS, 0, s>>>(src.p, ceid.p, ne, csrc.p);
+      { ++n_launch; k_csc_rows<<<grid(), THREADS, 0, s>>>(dst_s.p, ne, nv, crow.p); }
+      { ++n_launch; k_gather_u32<<<grid(), THREADS, 0, s>>>(src.p, ceid.p, ne, csrc.p); }
       PCK(cudaGetLastError());
       sync();
     }
@@ -465,8 +507,8 @@ struct sgs_ppr {
     w.ensure(ne);
     if (ne) PCK(cudaMemcpyAsync(w.p, wt, sizeof(double) * ne, kin(mem), s));
     PCK(cudaMemsetAsync(err.p, 0, sizeof(unsigned int), s));
-    k_row_probs<<<grid(), THREADS, 0, s>>>(row.p, nv, w.p, inv_s.p, pr.p, err.p);
-    k_csc_probs<<<grid(), THREADS, 0, s>>>(pr.p, ceid.p, ne, pc.p);
+    { ++n_launch; k_row_probs<<<grid(), THREADS, 0, s>>>(row.p, nv, w.p, inv_s.p, pr.p, err.p); }
+    { ++n_launch; k_csc_probs<<<grid(), THREADS, 0, s>>>(pr.p, ceid.p, ne, pc.p); }
     PCK(cudaGetLastError());
     unsigned int h = 0;
     PCK(cudaMemcpyAsync(&h, err.p, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -477,8 +519,14 @@ struct sgs_ppr {
   template <int LPE, int CPL>
   void launch_step(const Adj &a, const double *p, uint32_t K, double alpha, double c,
                    const double *B, const double *xin, double *xout, double *d) {
-    k_ppr_step<LPE, CPL><<<grid(), THREADS, 0, s>>>(a.ptr, a.nbr, p, nv, a.pv.p, a.poff.p,
-                                                    a.npieces, K, alpha, c, B, xin, xout, part.p, d);
+    { ++n_launch; k_ppr_step<LPE, CPL><<<grid(), THREADS, 0, s>>>(a.ptr, a.nbr, p, nv, a.pv.p, a.poff.p,
+                                                    a.npieces, K, alpha, c, B, xin, xout, part.p, d); }
+  }
+
+  template <int L>
+  void launch_grad(uint32_t K, double alpha, const double *Y, double *dst) {
+    { ++n_launch; k_ppr_edge_grad<L><<<grid(), THREADS, 0, s>>>(row.p, col.p, inv_s.p, nv, out.pv.p, out.poff.p,
+                                                  out.npieces, K, alpha, x.p, Y, g.p, dst); }
   }
 
   // One Jacobi step xin -> xout along `a` with probabilities p.
@@ -494,8 +542,8 @@ struct sgs_ppr {
       default: launch_step<32, 2>(a, p, K, alpha, c, B, xin, xout, d); break;
     }
     if (a.npieces)
-      k_ppr_finalize<<<grid(), THREADS, 0, s>>>(a.pv.p, a.poff.p, a.npieces, K, alpha, c, B, xin,
-                                                xout, part.p, d);
+      { ++n_launch; k_ppr_finalize<<<grid(), THREADS, 0, s>>>(a.pv.p, a.poff.p, a.npieces, K, alpha, c, B, xin,
+                                                xout, part.p, d); }
   }
 
   // Jacobi steps (cur -> nxt, swap) until one step changes the state by
@@ -509,13 +557,22 @@ struct sgs_ppr {
       const uint32_t nb = std::min<uint32_t>(batch, max_iter - it);
       PCK(cudaMemsetAsync(diff.p, 0, sizeof(double) * nb, s));
       for (uint32_t b = 0; b < nb; ++b) {
+        if (timing) PCK(cudaEventRecord(ev[2 * b], s));
         stepf(cur, nxt, diff.p + b);
+        if (timing) PCK(cudaEventRecord(ev[2 * b + 1], s));
         std::swap(cur, nxt);
       }
       PCK(cudaGetLastError());
       PCK(cudaMemcpyAsync(hd, diff.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
       sync();
+      if (timing)
+        for (uint32_t b = 0; b < nb; ++b) {
+          float ms = 0.f;
+          PCK(cudaEventElapsedTime(&ms, ev[2 * b], ev[2 * b + 1]));
+          st.steps_ms += ms;
+        }
       it += nb;
+      st.iters = (int32_t)it;
       for (uint32_t b = 0; b < nb; ++b)
         if (hd[b] < tol) return (int)it;
       batch = std::min<uint32_t>(batch * 2, 32);
@@ -531,7 +588,7 @@ struct sgs_ppr {
     xn.ensure(n);
     part.ensure((uint64_t)std::max(in.npieces, out.npieces) * K);
     PCK(cudaMemcpyAsync(t.p, T, sizeof(double) * n, kin(mem), s));
-    k_scale<<<grid(), THREADS, 0, s>>>(t.p, 1.0 - alpha, n, x.p);
+    { ++n_launch; k_scale<<<grid(), THREADS, 0, s>>>(t.p, 1.0 - alpha, n, x.p); }
     double *cur = x.p, *nxt = xn.p;
     const int it = iterate(
         [&](double *a, double *b, double *d) { step(in, pc.p, K, alpha, 1.0 - alpha, t.p, a, b, d); },
@@ -564,19 +621,14 @@ struct sgs_ppr {
         tmp.ensure(ne);
         dst = tmp.p;
       }
-      const int lpe = lanes_per_edge(K);
-#define SGS_GRAD(L)                                                                              \
-  k_ppr_edge_grad<L><<<grid(), THREADS, 0, s>>>(row.p, col.p, inv_s.p, nv, out.pv.p, out.poff.p, \
-                                                out.npieces, K, alpha, x.p, cur, g.p, dst)
-      switch (lpe) {
-        case 1: SGS_GRAD(1); break;
-        case 2: SGS_GRAD(2); break;
-        case 4: SGS_GRAD(4); break;
-        case 8: SGS_GRAD(8); break;
-        case 16: SGS_GRAD(16); break;
-        default: SGS_GRAD(32); break;
+      switch (lanes_per_edge(K)) {
+        case 1: launch_grad<1>(K, alpha, cur, dst); break;
+        case 2: launch_grad<2>(K, alpha, cur, dst); break;
+        case 4: launch_grad<4>(K, alpha, cur, dst); break;
+        case 8: launch_grad<8>(K, alpha, cur, dst); break;
+        case 16: launch_grad<16>(K, alpha, cur, dst); break;
+        default: launch_grad<32>(K, alpha, cur, dst); break;
       }
-#undef SGS_GRAD
       PCK(cudaGetLastError());
       if (mem == SGS_MEM_HOST) PCK(cudaMemcpyAsync(gw, dst, sizeof(double) * ne, kout(mem), s));
       sync();
@@ -588,7 +640,7 @@ struct sgs_ppr {
         tmp.ensure(n);
         dst = tmp.p;
       }
-      k_scale<<<grid(), THREADS, 0, s>>>(cur, 1.0 - alpha, n, dst);
+      { ++n_launch; k_scale<<<grid(), THREADS, 0, s>>>(cur, 1.0 - alpha, n, dst); }
       PCK(cudaGetLastError());
       if (mem == SGS_MEM_HOST) PCK(cudaMemcpyAsync(gT, dst, sizeof(double) * n, kout(mem), s));
       sync();
@@ -685,6 +737,27 @@ SGS_API int sgs_ppr_info(sgs_ppr *p, uint32_t *nv, uint64_t *ne) {
   return SGS_OK;
 }
 
+SGS_API int sgs_ppr_timing(sgs_ppr *p, int enable) {
+  if (!p) {
+    sgs::set_last_error("null argument");
+    return SGS_ERR_INVALID;
+  }
+  p->timing = enable != 0;
+  return SGS_OK;
+}
+
+SGS_API int sgs_ppr_get_stats(sgs_ppr *p, sgs_ppr_stats *out) {
+  if (!p || !out) {
+    sgs::set_last_error("null argument");
+    return SGS_ERR_INVALID;
+  }
+  p->st.pieces_in = p->in.npieces;
+  p->st.pieces_out = p->out.npieces;
+  p->st.kernel_launches = p->n_launch;
+  *out = p->st;
+  return SGS_OK;
+}
+
 SGS_API int sgs_ppr_export(sgs_ppr *p, uint64_t *row, uint32_t *col, int mem) {
   if (!p || !row || !col) {
     sgs::set_last_error("null argument");
@@ -708,7 +781,10 @@ SGS_API int sgs_ppr_forward(sgs_ppr *p, const double *w, const double *T, uint32
   return pguard([&] {
     PCK(cudaSetDevice(p->dev));
     p->set_weights(w, mem);
+    p->call_begin();
+    p->st.bytes_alg_step = p->step_bytes(K);
     const int it = p->forward(T, K, alpha, tol, max_iter, X, mem);
+    p->call_end();
     if (iters) *iters = it;
     if (it < 0) throw PprFail{SGS_ERR_NOCONV, "PPR forward did not converge"};
   });
@@ -725,7 +801,10 @@ SGS_API int sgs_ppr_backward(sgs_ppr *p, const double *w, const double *X, const
   return pguard([&] {
     PCK(cudaSetDevice(p->dev));
     p->set_weights(w, mem);
+    p->call_begin();
+    p->st.bytes_alg_step = p->step_bytes(K);
     const int it = p->backward(X, G, K, alpha, tol, max_iter, gw, gT, mem);
+    p->call_end();
     if (iters) *iters = it;
     if (it < 0) throw PprFail{SGS_ERR_NOCONV, "PPR adjoint did not converge"};
   });

@@ -49,7 +49,8 @@ EXPORTS = [
     "sgs_query_summary", "sgs_gen_update_stream", "sgs_hash_weights",
     "sgs_read_edge_list", "sgs_read_stream_sizes", "sgs_read_update_file", "sgs_free",
     "sgs_ppr_create_csr", "sgs_ppr_create", "sgs_ppr_destroy", "sgs_ppr_info",
-    "sgs_ppr_export", "sgs_ppr_forward", "sgs_ppr_backward",
+    "sgs_ppr_export", "sgs_ppr_forward", "sgs_ppr_backward", "sgs_ppr_timing",
+    "sgs_ppr_get_stats",
 ]
 
 K_GROUP, K_GROUP_INVAL, K_PR_PUSH = range(3)
@@ -109,6 +110,7 @@ class EngineStats(C.Structure):
         ("repacks", C.c_uint64),
         ("last_apply_ms", C.c_double),
         ("last_batch_ms", C.c_double),
+        ("kernel_launches", C.c_uint64),
     ]
 
     def as_dict(self):
@@ -130,6 +132,22 @@ class KernelStats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class PprStats(C.Structure):
+    _fields_ = [
+        ("iters", C.c_int32),
+        ("pieces_in", C.c_uint32),
+        ("pieces_out", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("ms", C.c_double),
+        ("steps_ms", C.c_double),
+        ("bytes_alg_step", C.c_double),
+        ("kernel_launches", C.c_uint64),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
 _lib = None
@@ -181,6 +199,8 @@ def lib():
     L.sgs_ppr_export.argtypes = [vp, vp, vp, i32]
     L.sgs_ppr_forward.argtypes = [vp, vp, vp, u32, dbl, dbl, u32, vp, C.POINTER(i32), i32]
     L.sgs_ppr_backward.argtypes = [vp, vp, vp, vp, u32, dbl, dbl, u32, vp, vp, C.POINTER(i32), i32]
+    L.sgs_ppr_timing.argtypes = [vp, i32]
+    L.sgs_ppr_get_stats.argtypes = [vp, C.POINTER(PprStats)]
     for name in EXPORTS:
         if name not in ("sgs_version", "sgs_last_error", "sgs_config_default",
                         "sgs_hash_weights", "sgs_free"):
@@ -526,6 +546,15 @@ class Ppr:
         col = np.empty(max(self.ne, 1), np.uint32)
         _check(lib().sgs_ppr_export(self.h, _ptr(row), _ptr(col), MEM_HOST))
         return row, col[: self.ne]
+
+    def timing(self, enable=True):
+        """Per-step CUDA events (steps_ms in :meth:`stats`)."""
+        _check(lib().sgs_ppr_timing(self.h, int(enable)))
+
+    def stats(self):
+        st = PprStats()
+        _check(lib().sgs_ppr_get_stats(self.h, C.byref(st)))
+        return st.as_dict()
 
     def _tol(self, tol, K):
         return 1e-13 * self.nv * K if tol is None else float(tol)

@@ -119,6 +119,8 @@ typedef struct sgs_engine_stats {
   uint64_t repacks;           /* arena repacks so far                      */
   double last_apply_ms;       /* device time of the last graph update      */
   double last_batch_ms;       /* device time of the whole last snapshot    */
+  uint64_t kernel_launches;   /* the engine's own kernel launches so far
+                                 (CUB sorts and scans not counted)         */
 } sgs_engine_stats;
 
 /* Per-kernel-class timing of the relaxation launches (CUDA events on the
@@ -289,6 +291,23 @@ SGS_API int sgs_ppr_backward(sgs_ppr *p, const double *w, const double *X,
                              const double *G, uint32_t K, double alpha,
                              double tol, uint32_t max_iter, double *gw,
                              double *gT, int *iters, int mem);
+/* Device timing of the last forward/backward call (CUDA events on the
+ * handle's stream).  steps_ms is filled only while sgs_ppr_timing is on
+ * (events around every Jacobi step).  bytes_alg_step = algorithmic bytes of
+ * one step: per edge the 4-B neighbour id, 8-B probability and 8K-B neighbour
+ * row; per vertex 16 B of offsets and 24K B of state (B, x read; out written). */
+typedef struct sgs_ppr_stats {
+  int32_t iters;             /* Jacobi steps of the last call              */
+  uint32_t pieces_in;        /* work pieces of hub vertices, CSC and CSR   */
+  uint32_t pieces_out;
+  uint32_t reserved;
+  double ms;                 /* device time of the whole last call         */
+  double steps_ms;           /* device time of its Jacobi steps            */
+  double bytes_alg_step;
+  uint64_t kernel_launches;  /* own kernel launches since the handle was made */
+} sgs_ppr_stats;
+SGS_API int sgs_ppr_timing(sgs_ppr *p, int enable);
+SGS_API int sgs_ppr_get_stats(sgs_ppr *p, sgs_ppr_stats *out);
 
 #ifdef __cplusplus
 }

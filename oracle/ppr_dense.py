@@ -81,3 +81,35 @@ def ppr_grad_autograd(nv, row, col, w, T, G, alpha=0.85):
     L = (X * torch.from_numpy(np.asarray(G, np.float64).reshape(nv, -1))).sum()
     L.backward()
     return X.detach().numpy(), wt.grad.numpy(), Tt.grad.numpy()
+
+
+def sparse_pt(nv, row, col, w):
+    """P^T as a scipy CSR matrix."""
+    import scipy.sparse as sp
+
+    w = np.asarray(w, np.float64)
+    src = _src(nv, row)
+    s = np.bincount(src, weights=w, minlength=nv)
+    inv = np.where(s > 0, 1.0 / np.where(s > 0, s, 1.0), 0.0)
+    return sp.csr_matrix((w * inv[src], (col.astype(np.int64), src)), shape=(nv, nv))
+
+
+def ppr_jacobi_sparse(nv, row, col, w, T, alpha=0.85, iters=None, tol=None, X0=None, PT=None):
+    """The same Jacobi iteration the GPU runs, X <- (1 - alpha) T + alpha P^T X,
+    on the CPU with a scipy CSR matrix (single thread): for the timed CPU
+    baseline.  Runs `iters` steps, or until the L1 step change is below tol.
+    Returns (X, steps)."""
+    if PT is None:
+        PT = sparse_pt(nv, row, col, w)
+    T = np.asarray(T, np.float64).reshape(nv, -1)
+    B = (1.0 - alpha) * T
+    X = B.copy() if X0 is None else X0
+    k = 0
+    while iters is None or k < iters:
+        Xn = B + alpha * (PT @ X)
+        k += 1
+        d = float(np.abs(Xn - X).sum())
+        X = Xn
+        if tol is not None and d < tol:
+            break
+    return X, k

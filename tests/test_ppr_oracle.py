@@ -72,3 +72,10 @@ def test_closed_gradient_finite_differences():
     dT = rng.standard_normal(T.shape)
     fd = (L(w, T + h * dT) - L(w, T - h * dT)) / (2 * h)
     assert abs(fd - (gT * dT).sum()) <= 1e-6 * max(abs(fd), 1e-12)
+
+
+def test_sparse_jacobi_port_matches_dense():
+    nv, row, col, w, T, _ = _case(8, 3, 3)
+    X, k = D.ppr_jacobi_sparse(nv, row, col, w, T, tol=1e-14)
+    assert k > 10
+    assert np.allclose(X, D.ppr_dense(nv, row, col, w, T), rtol=1e-11, atol=1e-14)
