@@ -33,6 +33,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -214,7 +215,7 @@ __device__ __forceinline__ void gather_rows(const uint32_t *__restrict__ nbr,
 // partial sums to part[piece][K]) and [npieces, npieces + nv) (light vertices:
 // out[v,k] = c B[v,k] + alpha sum p x, |out - x| added to *diff).
 template <int LPE, int CPL>
-__global__ void __launch_bounds__(THREADS)
+__global__ void __launch_bounds__(THREADS, CPL == 1 ? 8 : 6)
     k_ppr_step(const uint64_t *__restrict__ ptr, const uint32_t *__restrict__ nbr,
                const double *__restrict__ p, uint32_t nv, const uint32_t *__restrict__ pv,
                const uint32_t *__restrict__ poff, uint32_t npieces, uint32_t K, double alpha,
@@ -419,6 +420,18 @@ struct sgs_ppr {
     st.kernel_launches = n_launch;
   }
   uint32_t grid() const { return (uint32_t)nsm * 8; }
+  // One wave: every block resident at once, so the grid-stride split of the
+  // work items has no second partial wave.
+  std::map<const void *, uint32_t> rgrid_cache;
+  uint32_t rgrid(const void *f) {
+    auto it = rgrid_cache.find(f);
+    if (it != rgrid_cache.end()) return it->second;
+    int b = 0;
+    PCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, THREADS, 0));
+    const uint32_t g = (uint32_t)nsm * (uint32_t)std::max(b, 1);
+    rgrid_cache[f] = g;
+    return g;
+  }
   void sync() { PCK(cudaStreamSynchronize(s)); }
   // algorithmic bytes of one Jacobi step with K columns: per edge the 4-B
   // neighbour id, the 8-B probability and the neighbour's 8K-B row; per
@@ -519,13 +532,13 @@ struct sgs_ppr {
   template <int LPE, int CPL>
   void launch_step(const Adj &a, const double *p, uint32_t K, double alpha, double c,
                    const double *B, const double *xin, double *xout, double *d) {
-    { ++n_launch; k_ppr_step<LPE, CPL><<<grid(), THREADS, 0, s>>>(a.ptr, a.nbr, p, nv, a.pv.p, a.poff.p,
+    { ++n_launch; k_ppr_step<LPE, CPL><<<rgrid((const void *)k_ppr_step<LPE, CPL>), THREADS, 0, s>>>(a.ptr, a.nbr, p, nv, a.pv.p, a.poff.p,
                                                     a.npieces, K, alpha, c, B, xin, xout, part.p, d); }
   }
 
   template <int L>
   void launch_grad(uint32_t K, double alpha, const double *Y, double *dst) {
-    { ++n_launch; k_ppr_edge_grad<L><<<grid(), THREADS, 0, s>>>(row.p, col.p, inv_s.p, nv, out.pv.p, out.poff.p,
+    { ++n_launch; k_ppr_edge_grad<L><<<rgrid((const void *)k_ppr_edge_grad<L>), THREADS, 0, s>>>(row.p, col.p, inv_s.p, nv, out.pv.p, out.poff.p,
                                                   out.npieces, K, alpha, x.p, Y, g.p, dst); }
   }
 
@@ -542,7 +555,7 @@ struct sgs_ppr {
       default: launch_step<32, 2>(a, p, K, alpha, c, B, xin, xout, d); break;
     }
     if (a.npieces)
-      { ++n_launch; k_ppr_finalize<<<grid(), THREADS, 0, s>>>(a.pv.p, a.poff.p, a.npieces, K, alpha, c, B, xin,
+      { ++n_launch; k_ppr_finalize<<<rgrid((const void *)k_ppr_finalize), THREADS, 0, s>>>(a.pv.p, a.poff.p, a.npieces, K, alpha, c, B, xin,
                                                 xout, part.p, d); }
   }
 
