@@ -28,6 +28,7 @@
 #include "../../include/sgs.h"
 #include "sgs_group.cuh"
 #include "sgs_kernels.cuh"
+#include "sgs_wide.cuh"
 
 using namespace sgs;
 
@@ -104,19 +105,28 @@ struct Frontier {
   DBuf<uint32_t> ustart;
 };
 
-// A group: up to GMAX integer queries sharing one edge stream (sgs_group.cuh).
+// A group: integer queries sharing one edge stream.  Narrow groups (width
+// GMAX = 4, sgs_group.cuh) keep a vertex's lanes in one 32-B sector and the
+// lanes of a slot in a thread's registers; wide groups (width 64,
+// sgs_wide.cuh) keep a vertex's lanes in one 512-B row with a warp's threads
+// covering them.
 struct Group {
-  static constexpr int S = GMAX;
-  DBuf<unsigned long long> st;  // [nv * S] packed (value, parent)
-  DBuf<uint32_t> val;           // [nv * S] value mirror (read-side filter)
-  uint32_t used = 0;            // lanes in use
-  uint32_t algo_packed = 0;     // 8 bits per lane
-  uint64_t inval[GMAX] = {};    // resets per lane in the last deletion phase
+  int width = GMAX;             // GMAX or WLANES
+  DBuf<unsigned long long> st;  // [nv * width] packed (value, parent)
+  DBuf<uint32_t> val;           // [nv * width] value mirror (read-side filter)
+  uint64_t used = 0;            // lanes in use
+  uint32_t algo_packed = 0;     // narrow: 8 bits per lane
+  uint64_t sssp = 0, cc = 0;    // lanes per algorithm (both widths)
+  uint64_t inval[WLANES] = {};  // resets per lane in the last deletion phase
+  bool wide() const { return width == WLANES; }
   LaneAlgo algo() const { return LaneAlgo{algo_packed}; }
-  bool any_sssp(uint32_t lanes) const {
-    for (int q = 0; q < GMAX; ++q)
-      if ((lanes >> q & 1u) && ((algo_packed >> (8 * q)) & 0xFF) == A_SSSP) return true;
-    return false;
+  WideAlgo walgo() const { return WideAlgo{sssp, cc}; }
+  bool any_sssp(uint64_t lanes) const { return (lanes & sssp) != 0; }
+  void set_lane(int l, int a) {
+    if (!wide()) algo_packed = (algo_packed & ~(0xFFu << (8 * l))) | ((uint32_t)a << (8 * l));
+    const uint64_t b = 1ull << l;
+    sssp = a == A_SSSP ? sssp | b : sssp & ~b;
+    cc = a == A_CC ? cc | b : cc & ~b;
   }
 };
 
@@ -179,6 +189,7 @@ struct sgs_engine {
   // frontier scratch
   Frontier fb[3];                          // rotating frontier buffers
   DBuf<uint32_t> gm[3];                    // rotating group lane masks
+  DBuf<unsigned long long> wm[3];          // the same for wide groups (u64)
   uint32_t ucap = 0;
   static constexpr uint32_t kSpecial = 8;  // extra counter slots at the end
   DBuf<unsigned long long> cnt;            // [max_rounds + 2 + kSpecial]
@@ -187,8 +198,9 @@ struct sgs_engine {
   uint32_t estamp = 1;
   DBuf<double> l1;                         // PR per-round L1
   DBuf<unsigned long long> rstat;          // per-round instance-edge counts
-  DBuf<unsigned long long> b_lane;         // [GMAX] per-lane edge counts
-  DBuf<unsigned long long> b_inval;        // [GMAX] per-lane resets
+  DBuf<unsigned long long> b_lane;         // [WLANES] per-lane edge counts
+  DBuf<unsigned long long> b_inval;        // [WLANES] per-lane resets
+  DBuf<uint32_t> b_seed;                   // sources and lanes of new wide lanes
 
   // batch scratch
   DBuf<uint32_t> b_isrc, b_idst, b_iw, b_dsrc, b_ddst;
@@ -275,9 +287,9 @@ struct sgs_engine {
     rl_count.ensure(1);
     l1.ensure(cfg.max_rounds + 2);
     rstat.ensure(cfg.max_rounds + 2);
-    b_lane.ensure(GMAX);
-    b_inval.ensure(GMAX);
-    if (cfg.group_size < 1 || cfg.group_size > GMAX) cfg.group_size = GMAX;
+    b_lane.ensure(WLANES);
+    b_inval.ensure(WLANES);
+    if (cfg.group_size < 1 || cfg.group_size > WLANES) cfg.group_size = GMAX;
     ev_batch.init();
     ev_apply.init();
     ev_q.init();
@@ -406,6 +418,10 @@ struct sgs_engine {
     for (int i = 0; i < 3; ++i) {
       gm[i].ensure(nv);
       CK(cudaMemsetAsync(gm[i].p, 0, sizeof(uint32_t) * nv, s));
+      if (wm[i].p) {
+        wm[i].ensure(nv);
+        CK(cudaMemsetAsync(wm[i].p, 0, sizeof(unsigned long long) * nv, s));
+      }
       fb[i].vtx.ensure((size_t)nv + 1);
       fb[i].len.ensure((size_t)nv + 1);
       fb[i].ebase.ensure((size_t)nv + 1);
@@ -486,6 +502,39 @@ struct sgs_engine {
   template <class MakeOp>
   uint32_t run_group_rounds(MakeOp make_op, bool &converged, int kind, double per_slot,
                             const char *round0 = nullptr) {
+    return run_rounds(
+        [&](uint32_t rr) {
+          auto op = make_op(gm[rr % 3].p, gm[(rr + 1) % 3].p);
+          const bool hp = rr >= 1;
+          { ++n_launch; group_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
+              fview(rr, cnt.p + rr), fview(rr + 1, cnt.p + rr + 1), op,
+              hp ? fb[(rr - 1) % 3].vtx.p : nullptr, hp ? cnt.p + rr - 1 : nullptr,
+              hp ? gm[(rr - 1) % 3].p : nullptr, b_lane.p, rstat.p + rr); }
+        },
+        false, converged, kind, per_slot, round0);
+  }
+
+  // The same for a wide group op (wide_map, u64 masks in wm).
+  template <class Op>
+  uint32_t run_wide_rounds(const Op &op, bool &converged, int kind, double per_slot,
+                           unsigned long long *lane_changes, const char *round0 = nullptr) {
+    GraphView g = view();
+    return run_rounds(
+        [&](uint32_t rr) {
+          const bool hp = rr >= 1;
+          { ++n_launch; wide_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
+              g, fview(rr, cnt.p + rr), fview(rr + 1, cnt.p + rr + 1), op, wm[rr % 3].p,
+              wm[(rr + 1) % 3].p, hp ? fb[(rr - 1) % 3].vtx.p : nullptr,
+              hp ? cnt.p + rr - 1 : nullptr, hp ? wm[(rr - 1) % 3].p : nullptr, b_lane.p,
+              lane_changes, rstat.p + rr); }
+        },
+        true, converged, kind, per_slot, round0);
+  }
+
+  // Round loop shared by both group widths: `launch(rr)` queues round rr.
+  template <class Launch>
+  uint32_t run_rounds(Launch launch, bool wide, bool &converged, int kind, double per_slot,
+                      const char *round0) {
     const uint32_t maxr = cfg.max_rounds;
     uint32_t r = 0, rb = 2;
     converged = false;
@@ -499,14 +548,9 @@ struct sgs_engine {
       if (ktiming) ensure_kev(2 * nb);
       for (uint32_t k = 0; k < nb; ++k) {
         const uint32_t rr = r + k;
-        auto op = make_op(gm[rr % 3].p, gm[(rr + 1) % 3].p);
-        const bool hp = rr >= 1;
         if (ktiming) CK(cudaEventRecord(kev[2 * k], s));
         if (rr == 0 && round0) nvtxRangePushA(round0);
-        { ++n_launch; group_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
-            fview(rr, cnt.p + rr), fview(rr + 1, cnt.p + rr + 1), op,
-            hp ? fb[(rr - 1) % 3].vtx.p : nullptr, hp ? cnt.p + rr - 1 : nullptr,
-            hp ? gm[(rr - 1) % 3].p : nullptr, b_lane.p, rstat.p + rr); }
+        launch(rr);
         if (rr == 0 && round0) nvtxRangePop();
         if (ktiming) CK(cudaEventRecord(kev[2 * k + 1], s));
       }
@@ -523,8 +567,7 @@ struct sgs_engine {
       for (uint32_t k = 0; k < nb; ++k)
         if (h_cnt[k + 1] == 0) {
           const uint32_t z = r + k + 1;  // first empty frontier
-          { ++n_launch; k_clear_masks<<<grid_elem(nv), 256, 0, s>>>(fb[(z - 1) % 3].vtx.p, cnt.p + z - 1,
-                                                      gm[(z - 1) % 3].p); }
+          clear_masks(wide, z - 1);
           CK(cudaGetLastError());
           converged = true;
           return z;
@@ -533,19 +576,39 @@ struct sgs_engine {
       rb = std::min<uint32_t>(rb * 2, 16);
     }
     // not converged: leave the masks clean for the next call
-    for (uint32_t f = (r >= 1 ? r - 1 : 0); f <= r; ++f)
-      { ++n_launch; k_clear_masks<<<grid_elem(nv), 256, 0, s>>>(fb[f % 3].vtx.p, cnt.p + f, gm[f % 3].p); }
+    for (uint32_t f = (r >= 1 ? r - 1 : 0); f <= r; ++f) clear_masks(wide, f);
     CK(cudaGetLastError());
     return r;
+  }
+
+  // Masks of the frontier of round f (buffer f % 3, counter cnt[f]).
+  void clear_masks(bool wide, uint32_t f) {
+    if (wide)
+      { ++n_launch; k_clear_masks64<<<grid_elem(nv), 256, 0, s>>>(fb[f % 3].vtx.p, cnt.p + f, wm[f % 3].p); }
+    else
+      { ++n_launch; k_clear_masks<<<grid_elem(nv), 256, 0, s>>>(fb[f % 3].vtx.p, cnt.p + f, gm[f % 3].p); }
+  }
+
+  void ensure_wide_masks() {
+    for (int i = 0; i < 3; ++i)
+      if (!wm[i].p || wm[i].n < nv) {
+        wm[i].ensure(nv);
+        CK(cudaMemsetAsync(wm[i].p, 0, sizeof(unsigned long long) * nv, s));
+      }
   }
 
   // Relaxation rounds for the lanes whose frontier is in buffer 0.
   uint32_t group_relax(Group &G, bool &conv, const char *round0 = nullptr) {
     GraphView g = view();
+    if (G.wide()) {
+      const bool anyw = G.sssp && cfg.weight_mode == SGS_W_EXPLICIT;
+      WideRelaxOp op{G.st.p, G.val.p, G.walgo()};
+      return run_wide_rounds(op, conv, SGS_K_WIDE, anyw ? 8.0 : 4.0, nullptr, round0);
+    }
     const uint32_t anyw = G.any_sssp(G.used | 0xF) && cfg.weight_mode == SGS_W_EXPLICIT;
     return run_group_rounds(
         [&](uint32_t *mi, uint32_t *mo) {
-          return GroupRelaxOp<Group::S>{g, G.st.p, G.val.p, mi, mo, G.algo(), anyw};
+          return GroupRelaxOp<GMAX>{g, G.st.p, G.val.p, mi, mo, G.algo(), anyw};
         },
         conv, SGS_K_GROUP, anyw ? 8.0 : 4.0, round0);
   }
@@ -605,8 +668,8 @@ struct sgs_engine {
   // Per-lane stats of every query of a group after a group phase.
   void lane_stats(Group &G, uint32_t rounds, bool conv, float ms, const uint64_t *extra_edges,
                   const uint64_t *inval) {
-    unsigned long long le[GMAX];
-    CK(cudaMemcpyAsync(le, b_lane.p, sizeof(le), cudaMemcpyDeviceToHost, s));
+    unsigned long long le[WLANES];
+    CK(cudaMemcpyAsync(le, b_lane.p, sizeof(unsigned long long) * G.width, cudaMemcpyDeviceToHost, s));
     sync();
     for (auto &q : queries) {
       if (q->grp != &G) continue;
@@ -644,20 +707,47 @@ struct sgs_engine {
     q.stats.invalidated = 0;
   }
 
-  // Static convergence of one new lane (InitGraph + Start for that query).
-  void start_lane(Query &q) {
-    Group &G = *q.grp;
-    const int l = q.lane;
+  // Static convergence of the new lanes `fresh` of a group, all together
+  // (InitGraph + Start for each of those queries): CC lanes start from a
+  // dense frontier, BFS/SSSP lanes from their sources, then one round loop.
+  void start_lanes(Group &G, uint64_t fresh, const std::vector<Query *> &qs) {
     GraphView g = view();
     CK(cudaEventRecord(ev_q.a, s));
-    CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * GMAX, s));
-    { ++n_launch; k_group_init_lane<Group::S><<<grid_elem(nv), 256, 0, s>>>(G.st.p, G.val.p, nv, l, q.algo, q.source); }
+    CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * WLANES, s));
     reset_counters(0);
-    if (q.algo == SGS_CC)
-      { ++n_launch; k_group_dense<Group::S><<<grid_elem(nv), 256, 0, s>>>(g, G.val.p, 1u << l, G.algo(), gm[0].p,
-                                                            fview(0, cnt.p)); }
-    else
-      { ++n_launch; k_group_seed_one<<<1, 32, 0, s>>>(g, q.source, 1u << l, gm[0].p, fview(0, cnt.p)); }
+    const uint64_t fresh_cc = fresh & G.cc;
+    if (G.wide()) {
+      ensure_wide_masks();
+      { ++n_launch; k_wide_init_lanes<<<grid_elem((uint64_t)nv * 32), 256, 0, s>>>(G.st.p, G.val.p, nv, fresh, G.cc); }
+      if (fresh_cc)
+        { ++n_launch; k_wide_dense<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(g, G.val.p, fresh_cc, G.cc, wm[0].p,
+                                                               fview(0, cnt.p)); }
+      std::vector<uint32_t> src, lane;
+      for (Query *q : qs)
+        if (q->algo != SGS_CC) {
+          src.push_back(q->source);
+          lane.push_back((uint32_t)q->lane);
+        }
+      if (!src.empty()) {
+        b_seed.ensure(2 * src.size());
+        CK(cudaMemcpyAsync(b_seed.p, src.data(), sizeof(uint32_t) * src.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(b_seed.p + src.size(), lane.data(), sizeof(uint32_t) * lane.size(),
+                           cudaMemcpyHostToDevice, s));
+        { ++n_launch; k_wide_seed_sources<<<grid_elem(src.size()), 256, 0, s>>>(
+            g, G.st.p, G.val.p, b_seed.p, b_seed.p + src.size(), (uint32_t)src.size(), wm[0].p,
+            fview(0, cnt.p)); }
+      }
+    } else {
+      for (Query *q : qs)
+        { ++n_launch; k_group_init_lane<GMAX><<<grid_elem(nv), 256, 0, s>>>(G.st.p, G.val.p, nv, q->lane, q->algo,
+                                                                q->source); }
+      if (fresh_cc)
+        { ++n_launch; k_group_dense<GMAX><<<grid_elem(nv), 256, 0, s>>>(g, G.val.p, (uint32_t)fresh_cc, G.algo(),
+                                                            gm[0].p, fview(0, cnt.p)); }
+      for (Query *q : qs)
+        if (q->algo != SGS_CC)
+          { ++n_launch; k_group_seed_one<<<1, 32, 0, s>>>(g, q->source, 1u << q->lane, gm[0].p, fview(0, cnt.p)); }
+    }
     CK(cudaGetLastError());
     bool conv = false;
     const uint32_t rounds = group_relax(G, conv);
@@ -665,56 +755,90 @@ struct sgs_engine {
     sync();
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, ev_q.a, ev_q.b));
-    unsigned long long le[GMAX];
-    CK(cudaMemcpyAsync(le, b_lane.p, sizeof(le), cudaMemcpyDeviceToHost, s));
+    unsigned long long le[WLANES];
+    CK(cudaMemcpyAsync(le, b_lane.p, sizeof(unsigned long long) * G.width, cudaMemcpyDeviceToHost, s));
     sync();
-    q.stats.edges_traversed = le[l];
-    q.stats.edges_total += le[l];
-    q.stats.rounds = rounds;
-    q.stats.converged = conv ? 1 : 0;
-    q.stats.ms = ms;
-    q.stats.invalidated = 0;
+    for (Query *q : qs) {
+      const int l = q->lane;
+      q->stats.edges_traversed = le[l];
+      q->stats.edges_total += le[l];
+      q->stats.rounds = rounds;
+      q->stats.converged = conv ? 1 : 0;
+      q->stats.ms = ms;
+      q->stats.invalidated = 0;
+    }
+    if (!conv) fail(SGS_ERR_NOCONV, "round limit reached before convergence");
   }
 
   int add_query(int algo, uint32_t source) {
+    int id = 0;
+    add_queries(1, &algo, &source, &id);
+    return id;
+  }
+
+  // Registers n queries and brings them to their static fixed points; the
+  // BFS/SSSP/CC ones fill free lanes of groups of cfg.group_size lanes
+  // (narrow groups up to 4 lanes, wide groups above) and every group that
+  // received lanes converges them in one pass.
+  void add_queries(uint32_t n, const int *algos, const uint32_t *sources, int *ids) {
     if (!loaded) fail(SGS_ERR_STATE, "no graph loaded");
-    if (algo < 0 || algo > 3) fail(SGS_ERR_INVALID, "unknown algorithm");
-    auto q = std::make_unique<Query>();
-    q->id = next_qid++;
-    q->algo = algo;
-    q->source = std::min(source, nv - 1);
-    if (algo == SGS_PR) {
-      q->x.ensure(nv);
-      q->r.ensure(nv);
-      q->pv.ensure(nv);
-    } else {
-      // first group with a free lane among the first group_size lanes
-      const uint32_t full = (1u << cfg.group_size) - 1u;
-      Group *G = nullptr;
-      for (auto &gp : groups)
-        if ((gp->used & full) != full) { G = gp.get(); break; }
-      if (!G) {
-        auto ng = std::make_unique<Group>();
-        ng->st.ensure((size_t)nv * Group::S);
-        ng->val.ensure((size_t)nv * Group::S);
-        G = ng.get();
-        groups.push_back(std::move(ng));
+    for (uint32_t i = 0; i < n; ++i)
+      if (algos[i] < 0 || algos[i] > 3) fail(SGS_ERR_INVALID, "unknown algorithm");
+    const bool wide = cfg.group_size > (uint32_t)GMAX;
+    const uint64_t full = cfg.group_size >= 64 ? ~0ull : (1ull << cfg.group_size) - 1ull;
+    std::vector<Query *> added;
+    std::vector<std::pair<Group *, uint64_t>> touched;
+    for (uint32_t i = 0; i < n; ++i) {
+      auto q = std::make_unique<Query>();
+      q->id = next_qid++;
+      q->algo = algos[i];
+      q->source = std::min(sources[i], nv - 1);
+      if (q->algo == SGS_PR) {
+        q->x.ensure(nv);
+        q->r.ensure(nv);
+        q->pv.ensure(nv);
+      } else {
+        Group *G = nullptr;
+        for (auto &gp : groups) {
+          if (gp->wide() != wide) continue;
+          uint64_t pend = 0;
+          for (auto &t : touched)
+            if (t.first == gp.get()) pend = t.second;
+          if (((gp->used | pend) & full) != full) { G = gp.get(); break; }
+        }
+        if (!G) {
+          auto ng = std::make_unique<Group>();
+          ng->width = wide ? WLANES : GMAX;
+          ng->st.ensure((size_t)nv * ng->width);
+          ng->val.ensure((size_t)nv * ng->width);
+          G = ng.get();
+          groups.push_back(std::move(ng));
+        }
+        uint64_t pend = 0;
+        size_t ti = touched.size();
+        for (size_t k = 0; k < touched.size(); ++k)
+          if (touched[k].first == G) { pend = touched[k].second; ti = k; }
+        if (ti == touched.size()) touched.push_back({G, 0});
+        int l = 0;
+        while ((G->used | pend) >> l & 1ull) ++l;
+        G->set_lane(l, q->algo);
+        touched[ti].second |= 1ull << l;
+        q->grp = G;
+        q->lane = l;
       }
-      int l = 0;
-      while (G->used >> l & 1u) ++l;
-      G->algo_packed = (G->algo_packed & ~(0xFFu << (8 * l))) | ((uint32_t)algo << (8 * l));
-      q->grp = G;
-      q->lane = l;
+      ids[i] = q->id;
+      added.push_back(q.get());
+      queries.push_back(std::move(q));
     }
-    Query &ref = *q;
-    queries.push_back(std::move(q));
-    if (algo == SGS_PR) {
-      start_pr(ref);
-    } else {
-      start_lane(ref);
-      ref.grp->used |= 1u << ref.lane;
+    for (Query *q : added)
+      if (q->algo == SGS_PR) start_pr(*q);
+    for (auto &t : touched) {
+      std::vector<Query *> qs;
+      for (Query *q : added)
+        if (q->grp == t.first) qs.push_back(q);
+      start_lanes(*t.first, t.second, qs);
+      t.first->used |= t.second;
     }
-    return ref.id;
   }
 
   void remove_query(int qid) {
@@ -722,7 +846,7 @@ struct sgs_engine {
       if (queries[i]->id == qid) {
         sync();
         Query &q = *queries[i];
-        if (q.grp) q.grp->used &= ~(1u << q.lane);
+        if (q.grp) q.grp->used &= ~(1ull << q.lane);
         queries.erase(queries.begin() + i);
         for (size_t j = 0; j < groups.size(); ++j)
           if (groups[j]->used == 0) {
@@ -809,7 +933,7 @@ struct sgs_engine {
     for (auto &q : queries) any_pr |= q->algo == SGS_PR;
     const size_t ng = groups.size();
     std::vector<float> gms(ng, 0.f);
-    std::vector<std::array<uint64_t, GMAX>> gedges(ng), ginval(ng);
+    std::vector<std::array<uint64_t, WLANES>> gedges(ng), ginval(ng);
     for (size_t i = 0; i < ng; ++i) {
       gedges[i].fill(0);
       ginval[i].fill(0);
@@ -833,29 +957,38 @@ struct sgs_engine {
       Group &G = *groups[i];
       if (!G.used) continue;
       CK(cudaEventRecord(ev_q.a, s));
-      CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * GMAX, s));
-      CK(cudaMemsetAsync(b_inval.p, 0, sizeof(unsigned long long) * GMAX, s));
+      CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * WLANES, s));
+      CK(cudaMemsetAsync(b_inval.p, 0, sizeof(unsigned long long) * WLANES, s));
       reset_counters(0);
-      { ++n_launch; k_group_seed_deleted<Group::S><<<grid_elem(nd), 256, 0, s>>>(
-          g, G.st.p, G.val.p, G.used, G.algo(), b_dkeys_s.p, (uint32_t)nd, b_inval.p, gm[0].p,
-          fview(0, cnt.p)); }
-      CK(cudaGetLastError());
       bool conv = false;
-      run_group_rounds(
-          [&](uint32_t *mi, uint32_t *mo) {
-            return GroupInvalidateOp<Group::S>{g, G.st.p, G.val.p, mi, mo, G.algo(), b_inval.p};
-          },
-          conv, SGS_K_GROUP_INVAL, 4.0);
+      if (G.wide()) {
+        { ++n_launch; k_wide_seed_deleted<<<grid_elem(nd), 256, 0, s>>>(
+            g, G.st.p, G.val.p, G.used, G.cc, b_dkeys_s.p, (uint32_t)nd, b_inval.p, wm[0].p,
+            fview(0, cnt.p)); }
+        CK(cudaGetLastError());
+        WideInvalidateOp op{G.st.p, G.val.p, WideAlgo{0ull, G.cc}};  // no weights needed
+        run_wide_rounds(op, conv, SGS_K_WIDE_INVAL, 4.0, b_inval.p);
+      } else {
+        { ++n_launch; k_group_seed_deleted<GMAX><<<grid_elem(nd), 256, 0, s>>>(
+            g, G.st.p, G.val.p, (uint32_t)G.used, G.algo(), b_dkeys_s.p, (uint32_t)nd, b_inval.p, gm[0].p,
+            fview(0, cnt.p)); }
+        CK(cudaGetLastError());
+        run_group_rounds(
+            [&](uint32_t *mi, uint32_t *mo) {
+              return GroupInvalidateOp<GMAX>{g, G.st.p, G.val.p, mi, mo, G.algo(), b_inval.p};
+            },
+            conv, SGS_K_GROUP_INVAL, 4.0);
+      }
       if (!conv) fail(SGS_ERR_NOCONV, "invalidation did not converge");
       CK(cudaEventRecord(ev_q.b, s));
-      unsigned long long hv[GMAX], he[GMAX];
-      CK(cudaMemcpyAsync(hv, b_inval.p, sizeof(hv), cudaMemcpyDeviceToHost, s));
-      CK(cudaMemcpyAsync(he, b_lane.p, sizeof(he), cudaMemcpyDeviceToHost, s));
+      unsigned long long hv[WLANES], he[WLANES];
+      CK(cudaMemcpyAsync(hv, b_inval.p, sizeof(unsigned long long) * G.width, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(he, b_lane.p, sizeof(unsigned long long) * G.width, cudaMemcpyDeviceToHost, s));
       sync();
       float ms = 0;
       CK(cudaEventElapsedTime(&ms, ev_q.a, ev_q.b));
       gms[i] += ms;
-      for (int q = 0; q < GMAX; ++q) {
+      for (int q = 0; q < G.width; ++q) {
         ginval[i][q] = hv[q];
         gedges[i][q] = he[q];
         G.inval[q] = hv[q];
@@ -913,17 +1046,25 @@ struct sgs_engine {
       if (!G.used) continue;
       Range rg("sgs:repair");
       bool any_inval = false;
-      for (int q = 0; q < GMAX; ++q) any_inval |= (G.used >> q & 1u) && ginval[i][q] > 0;
+      for (int q = 0; q < G.width; ++q) any_inval |= (G.used >> q & 1ull) && ginval[i][q] > 0;
       CK(cudaEventRecord(ev_q.a, s));
-      CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * GMAX, s));
+      CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * WLANES, s));
       reset_counters(0);
-      if (any_inval) {
-        { ++n_launch; k_group_dense<Group::S><<<grid_elem(nv), 256, 0, s>>>(g, G.val.p, G.used, G.algo(), gm[0].p,
-                                                              fview(0, cnt.p)); }
+      if (G.wide()) {
+        if (any_inval)
+          { ++n_launch; k_wide_dense<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(g, G.val.p, G.used, G.cc, wm[0].p,
+                                                                 fview(0, cnt.p)); }
+        else if (ni)
+          { ++n_launch; k_wide_relax_inserted<<<grid_elem(ni), 256, 0, s>>>(
+              g, G.st.p, G.val.p, G.used, G.walgo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr,
+              b_nkept.p, wm[0].p, fview(0, cnt.p), b_lane.p); }
+      } else if (any_inval) {
+        { ++n_launch; k_group_dense<GMAX><<<grid_elem(nv), 256, 0, s>>>(g, G.val.p, (uint32_t)G.used, G.algo(),
+                                                            gm[0].p, fview(0, cnt.p)); }
       } else if (ni) {
-        { ++n_launch; k_group_relax_inserted<Group::S><<<grid_elem(ni), 256, 0, s>>>(
-            g, G.st.p, G.val.p, G.used, G.algo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr, b_nkept.p,
-            gm[0].p, fview(0, cnt.p), b_lane.p); }
+        { ++n_launch; k_group_relax_inserted<GMAX><<<grid_elem(ni), 256, 0, s>>>(
+            g, G.st.p, G.val.p, (uint32_t)G.used, G.algo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr,
+            b_nkept.p, gm[0].p, fview(0, cnt.p), b_lane.p); }
       }
       CK(cudaGetLastError());
       bool conv = false;
@@ -1054,12 +1195,14 @@ struct sgs_engine {
     }
     DBuf<uint32_t> tmp;
     tmp.ensure(nv);
-    if (field == SGS_FIELD_PARENT)
-      { ++n_launch; k_group_split<Group::S><<<grid_elem(nv), 256, 0, s>>>(q.grp->st.p, nv, q.lane, nullptr, tmp.p); }
-    else if (field == SGS_FIELD_VALUE || field == SGS_FIELD_BUFFER)
-      { ++n_launch; k_group_split<Group::S><<<grid_elem(nv), 256, 0, s>>>(q.grp->st.p, nv, q.lane, tmp.p, nullptr); }
-    else
+    if (field != SGS_FIELD_PARENT && field != SGS_FIELD_VALUE && field != SGS_FIELD_BUFFER)
       fail(SGS_ERR_INVALID, "unknown field");
+    uint32_t *vo = field == SGS_FIELD_PARENT ? nullptr : tmp.p;
+    uint32_t *po = field == SGS_FIELD_PARENT ? tmp.p : nullptr;
+    if (q.grp->wide())
+      { ++n_launch; k_group_split<WLANES><<<grid_elem(nv), 256, 0, s>>>(q.grp->st.p, nv, q.lane, vo, po); }
+    else
+      { ++n_launch; k_group_split<GMAX><<<grid_elem(nv), 256, 0, s>>>(q.grp->st.p, nv, q.lane, vo, po); }
     CK(cudaMemcpyAsync(out, tmp.p, sizeof(uint32_t) * nv, kind, s));
     sync();
   }
@@ -1069,8 +1212,12 @@ struct sgs_engine {
     if (q.algo == SGS_PR) {
       { ++n_launch; k_summary_pr<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.x.p, nv, (double *)b_stat.p + 1); }
     } else {
-      { ++n_launch; k_group_summary<Group::S><<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.grp->st.p, nv, q.lane,
-                                                                         b_stat.p); }
+      if (q.grp->wide())
+        { ++n_launch; k_group_summary<WLANES><<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.grp->st.p, nv, q.lane,
+                                                                          b_stat.p); }
+      else
+        { ++n_launch; k_group_summary<GMAX><<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.grp->st.p, nv, q.lane,
+                                                                        b_stat.p); }
     }
     CK(cudaGetLastError());
     unsigned long long h[4];
@@ -1328,6 +1475,18 @@ SGS_API int sgs_query_add(sgs_engine *e, int algo, uint32_t source, int *qid) {
     CK(cudaSetDevice(e->dev));
     *qid = e->add_query(algo, source);
     if (!e->find(*qid).stats.converged) fail(SGS_ERR_NOCONV, "round limit reached before convergence");
+  });
+}
+
+SGS_API int sgs_query_add_many(sgs_engine *e, uint32_t n, const int *algos, const uint32_t *sources,
+                               int *qids) {
+  if (!e || (n && (!algos || !sources || !qids))) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    if (n == 0) return;
+    e->add_queries(n, algos, sources, qids);
+    for (uint32_t i = 0; i < n; ++i)
+      if (!e->find(qids[i]).stats.converged) fail(SGS_ERR_NOCONV, "round limit reached before convergence");
   });
 }
 

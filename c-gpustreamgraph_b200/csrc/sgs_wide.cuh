@@ -1,0 +1,416 @@
+// sgs_wide.cuh -- wide query groups: up to 64 BFS / SSSP / CC queries (any
+// sources, uneven frontiers) relaxed together over one edge stream.
+//
+// Layout: st[v * 64 + q] u64 packed (value << 32 | parent) and the u32 value
+// mirror val[v * 64 + q], so the 64 lanes of one vertex are one contiguous
+// row (512 B / 256 B).  Lane masks are u64 per vertex in three rotating
+// buffers, with the same protocol as the narrow groups (sgs_group.cuh): round
+// r reads mask r%3, writes (r+1)%3 and clears the previous frontier's masks,
+// and the thread whose atomicOr turns a mask non-zero appends the vertex.
+//
+// Mapping: a warp walks 32 consecutive edge slots of the frontier at a time
+// (one coalesced id read), then relaxes them one by one with the warp's
+// threads covering the lanes -- thread t owns lanes t and t + 32 -- so every
+// destination row is read with two coalesced 128-B requests and lanes that
+// are not active at the source issue no load at all.  This is the batched
+// form of the single-query relaxation (hybrid_sssp.cu:97-118 min relaxation,
+// hybrid_cc.cu:96-110 label propagation) and of the parent-tree reset
+// (reset_del_edges / SyncPushDDB_del, driver.cuh:398-430, :1985-2031).
+#pragma once
+#include "sgs_device.cuh"
+#include "sgs_segmap.cuh"
+
+namespace sgs {
+
+constexpr int WLANES = 64;
+constexpr int WCHUNK = 256;  // entries staged per chunk by wide_map
+
+// Lane algorithms of a wide group as bit masks (a lane in neither is BFS).
+struct WideAlgo {
+  uint64_t sssp;
+  uint64_t cc;
+};
+
+__device__ __forceinline__ uint64_t ballot64(bool lo, bool hi) {
+  const uint32_t a = __ballot_sync(0xFFFFFFFFu, lo);
+  const uint32_t b = __ballot_sync(0xFFFFFFFFu, hi);
+  return (uint64_t)a | ((uint64_t)b << 32);
+}
+
+__device__ __forceinline__ void clear_prev_masks64(const uint32_t *vtx, const unsigned long long *cnt,
+                                                   unsigned long long *mask) {
+  if (!cnt) return;
+  const uint32_t n = (uint32_t)(__ldcg(cnt) >> CNT_SHIFT);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    mask[__ldcg(&vtx[i])] = 0ull;
+}
+
+// Relaxation of one lane: candidate from the source value, strict
+// improvement through the packed word, mirror lowered after it.
+struct WideRelaxOp {
+  static constexpr bool kNeedsSourceValues = true;
+  unsigned long long *st;
+  uint32_t *val;
+  WideAlgo algo;
+  // is_sssp / is_cc: this lane's algorithm; vu: the lane's value at u.
+  __device__ __forceinline__ bool lane(uint32_t u, uint32_t v, uint32_t w, uint32_t vu, int q,
+                                       bool is_sssp, bool is_cc) const {
+    uint32_t cand;
+    if (is_cc) {
+      cand = vu;
+    } else {
+      if (vu == INF32) return false;
+      const uint64_t nd = (uint64_t)vu + (is_sssp ? w : 1u);
+      if (nd >= INF32) return false;
+      cand = (uint32_t)nd;
+    }
+    const uint64_t idx = (uint64_t)v * WLANES + q;
+    if (cand >= __ldcg(&val[idx])) return false;
+    const unsigned long long old = atomicMin(&st[idx], ((unsigned long long)cand << 32) | u);
+    if (cand < (uint32_t)(old >> 32)) {
+      atomicMin(&val[idx], cand);
+      return true;
+    }
+    return false;
+  }
+};
+
+// Parent-tree reset of one lane: a child whose parent is u is reset once
+// (CAS on the packed word), the mirror with it; resets are counted per lane.
+struct WideInvalidateOp {
+  static constexpr bool kNeedsSourceValues = false;
+  unsigned long long *st;
+  uint32_t *val;
+  WideAlgo algo;
+  __device__ __forceinline__ bool lane(uint32_t u, uint32_t v, uint32_t, uint32_t, int q, bool,
+                                       bool is_cc) const {
+    const uint64_t idx = (uint64_t)v * WLANES + q;
+    const unsigned long long cu = __ldcg(&st[idx]);
+    if ((uint32_t)cu != u) return false;
+    const unsigned long long rst = is_cc ? (((unsigned long long)v << 32) | INF32) : ~0ull;
+    if (atomicCAS(&st[idx], cu, rst) != cu) return false;
+    val[idx] = is_cc ? v : INF32;
+    return true;
+  }
+};
+
+// Load-balanced map for wide ops: CTAs take ranges of 2048-slot units of
+// the frontier's edge space (as seg_map / group_map); entries are staged in
+// shared memory, then each warp takes 32 consecutive slots per step.  Per
+// lane counts: the CTA that holds an entry's first slot adds live[v] for
+// every lane of its mask ((query, edge) pairs relaxed); lane_changes counts
+// the lanes changed (resets for the invalidation op).
+template <class Op>
+__global__ void __launch_bounds__(RELAX_THREADS)
+    wide_map(GraphView g, FrontierView in, FrontierView out, Op op,
+             const unsigned long long *m_in, unsigned long long *m_out, const uint32_t *prev_vtx,
+             const unsigned long long *prev_cnt, unsigned long long *prev_mask,
+             unsigned long long *lane_edges, unsigned long long *lane_changes,
+             unsigned long long *edge_stat) {
+  constexpr int GC = WCHUNK;
+  __shared__ uint64_t s_eb[GC + 1];
+  __shared__ uint64_t s_off[GC];
+  __shared__ unsigned long long s_mask[GC];
+  __shared__ uint32_t s_len[GC];
+  __shared__ uint32_t s_vtx[GC];
+  __shared__ unsigned long long s_lane[WLANES];
+  __shared__ unsigned long long s_chg[WLANES];
+  clear_prev_masks64(prev_vtx, prev_cnt, prev_mask);
+  const int t = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  constexpr int NW = RELAX_THREADS / 32;
+  if (threadIdx.x < WLANES) {
+    s_lane[threadIdx.x] = 0;
+    s_chg[threadIdx.x] = 0;
+  }
+  const bool sssp0 = op.algo.sssp >> t & 1ull, sssp1 = op.algo.sssp >> (t + 32) & 1ull;
+  const bool cc0 = op.algo.cc >> t & 1ull, cc1 = op.algo.cc >> (t + 32) & 1ull;
+  unsigned long long acc0 = 0, acc1 = 0, chg0 = 0, chg1 = 0;
+  const uint64_t packed = __ldcg((const unsigned long long *)in.counter);
+  const uint32_t n = (uint32_t)(packed >> CNT_SHIFT);
+  const uint64_t T = packed & EDGE_MASK;
+  const uint64_t nunits = (T + UNIT - 1) / UNIT;
+  const uint64_t ub = (uint64_t)blockIdx.x * nunits / gridDim.x;
+  const uint64_t ue = (uint64_t)(blockIdx.x + 1) * nunits / gridDim.x;
+  __syncthreads();
+  if (n != 0 && ub < ue) {
+    const uint64_t E0 = ub * UNIT;
+    const uint64_t E1 = min(ue * (uint64_t)UNIT, T);
+    uint32_t s = __ldcg(&in.ustart[ub]);
+    for (;;) {
+      __syncthreads();
+      for (int h = threadIdx.x; h < GC; h += RELAX_THREADS) {
+        const uint32_t idx = s + h;
+        const uint64_t eb = idx < n ? __ldcg((const unsigned long long *)&in.ebase[idx]) : T;
+        s_eb[h] = eb;
+        s_mask[h] = 0ull;
+        if (h == 0) {
+          const uint32_t j = s + GC;
+          s_eb[GC] = j < n ? __ldcg((const unsigned long long *)&in.ebase[j]) : T;
+        }
+        if (idx < n && eb < E1) {
+          const uint32_t v = __ldcg(&in.vtx[idx]);
+          s_vtx[h] = v;
+          s_len[h] = __ldcg(&in.len[idx]);
+          s_off[h] = g.off[v];
+          s_mask[h] = __ldcg(&m_in[v]);
+        }
+      }
+      __syncthreads();
+      // per-lane (query, edge) counts of the entries whose first slot is ours
+      for (int h = warp * 32; h < GC; h += RELAX_THREADS) {
+        const uint32_t idx = s + h + t;
+        const uint64_t eb = s_eb[h + t];
+        const bool own = idx < n && eb >= E0 && eb < E1;
+        const uint32_t l = own ? g.live[s_vtx[h + t]] : 0u;
+        const unsigned long long m = own ? s_mask[h + t] : 0ull;
+#pragma unroll 4
+        for (int i = 0; i < 32; ++i) {
+          const uint32_t li = __shfl_sync(0xFFFFFFFFu, l, i);
+          const unsigned long long mi = __shfl_sync(0xFFFFFFFFu, m, i);
+          acc0 += (mi >> t & 1ull) ? li : 0u;
+          acc1 += (mi >> (t + 32) & 1ull) ? li : 0u;
+        }
+      }
+      const uint64_t lo = max(E0, s_eb[0]);
+      const uint64_t hi = min(E1, s_eb[GC]);
+      for (uint64_t base = lo + (uint64_t)warp * 32; base < hi; base += (uint64_t)NW * 32) {
+        const uint64_t e = base + t;
+        bool ok = false;
+        int le = 0;
+        uint32_t v = 0, w = 1;
+        if (e < hi) {
+          int l = 0, r = GC - 1;
+          while (l < r) {
+            const int m = (l + r + 1) >> 1;
+            if (s_eb[m] <= e) l = m;
+            else r = m - 1;
+          }
+          const uint32_t j = (uint32_t)(e - s_eb[l]);
+          if (j < s_len[l]) {
+            le = l;
+            v = __ldcg(adj_ptr(g, s_off[l]) + j);
+            ok = v != SGS_TOMB;
+            if (ok && op.algo.sssp && s_mask[l] & op.algo.sssp)
+              w = g.wmode == W_EXPLICIT ? __ldcg(wgt_ptr(g, s_off[l]) + j)
+                  : g.wmode == W_SYNTH  ? (s_vtx[l] + v) % 128u + 1u
+                                        : 1u;
+          }
+        }
+        bool want = false;
+        int cur = -1;
+        uint32_t vu0 = INF32, vu1 = INF32;
+        const uint32_t okb = __ballot_sync(0xFFFFFFFFu, ok);
+        for (uint32_t rem = okb; rem; rem &= rem - 1) {
+          const int i = __ffs(rem) - 1;
+          const int li = __shfl_sync(0xFFFFFFFFu, le, i);
+          const uint32_t vi = __shfl_sync(0xFFFFFFFFu, v, i);
+          const uint32_t wi = __shfl_sync(0xFFFFFFFFu, w, i);
+          const uint32_t u = s_vtx[li];
+          const unsigned long long mk = s_mask[li];
+          const bool a0 = mk >> t & 1ull, a1 = mk >> (t + 32) & 1ull;
+          if (Op::kNeedsSourceValues && li != cur) {
+            cur = li;
+            const uint32_t *row = op.val + (uint64_t)u * WLANES;
+            vu0 = a0 ? __ldcg(row + t) : INF32;
+            vu1 = a1 ? __ldcg(row + t + 32) : INF32;
+          }
+          const bool c0 = a0 && op.lane(u, vi, wi, vu0, t, sssp0, cc0);
+          const bool c1 = a1 && op.lane(u, vi, wi, vu1, t + 32, sssp1, cc1);
+          chg0 += c0;
+          chg1 += c1;
+          const unsigned long long bits = ballot64(c0, c1);
+          if (bits && t == i && g.slots[vi])
+            want = atomicOr(&m_out[vi], bits) == 0ull;
+        }
+        frontier_append(out, want, v, want ? g.slots[v] : 0u);
+      }
+      if (s_eb[GC] >= E1 || s + GC >= n) break;
+      s += GC;
+    }
+  }
+  // per-lane sums (thread t holds lanes t and t + 32): shared, then 64
+  // global atomics per CTA
+  atomicAdd(&s_lane[t], acc0);
+  atomicAdd(&s_lane[t + 32], acc1);
+  atomicAdd(&s_chg[t], chg0);
+  atomicAdd(&s_chg[t + 32], chg1);
+  __syncthreads();
+  if (threadIdx.x < WLANES) {
+    const unsigned long long x = s_lane[threadIdx.x], c = s_chg[threadIdx.x];
+    if (x) {
+      if (lane_edges) atomicAdd(&lane_edges[threadIdx.x], x);
+      if (edge_stat) atomicAdd(edge_stat, x);
+    }
+    if (c && lane_changes) atomicAdd(&lane_changes[threadIdx.x], c);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Frontier builders and per-lane helpers
+// ---------------------------------------------------------------------------
+
+// Initial state of the lanes in `lanes` on every vertex: CC lanes v's own id,
+// the others unreached; one warp per vertex row.
+__global__ void k_wide_init_lanes(unsigned long long *st, uint32_t *val, uint32_t nv,
+                                  unsigned long long lanes, unsigned long long cc) {
+  const int t = threadIdx.x & 31;
+  const uint32_t nwarp = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < nv; v += nwarp) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int q = t + 32 * h;
+      if (!(lanes >> q & 1ull)) continue;
+      const bool c = cc >> q & 1ull;
+      const uint64_t idx = (uint64_t)v * WLANES + q;
+      st[idx] = c ? (((unsigned long long)v << 32) | INF32) : ~0ull;
+      val[idx] = c ? v : INF32;
+    }
+  }
+}
+
+// Sources of new BFS/SSSP lanes: value 0 at the source, mask bit set, the
+// source appended once.  One thread per new lane.
+__global__ void k_wide_seed_sources(GraphView g, unsigned long long *st, uint32_t *val,
+                                    const uint32_t *src, const uint32_t *lane, uint32_t n,
+                                    unsigned long long *m_out, FrontierView out) {
+  for (uint32_t b = blockIdx.x * blockDim.x; b < n; b += gridDim.x * blockDim.x) {
+    const uint32_t i = b + threadIdx.x;
+    bool want = false;
+    uint32_t v = 0, d = 0;
+    if (i < n) {
+      v = src[i];
+      const uint32_t q = lane[i];
+      const uint64_t idx = (uint64_t)v * WLANES + q;
+      st[idx] = (unsigned long long)INF32;  // value 0, no parent
+      val[idx] = 0u;
+      d = g.slots[v];
+      want = d && atomicOr(&m_out[v], 1ull << q) == 0ull;
+    }
+    frontier_append(out, want, v, d);
+  }
+}
+
+// Every vertex with a non-empty block; mask = lanes of `lanes` whose value is
+// finite there (CC lanes always).  A warp reads 32 rows, one per step, and
+// appends the 32 vertices together.
+__global__ void k_wide_dense(GraphView g, const uint32_t *val, unsigned long long lanes,
+                             unsigned long long cc, unsigned long long *m_out, FrontierView out) {
+  const int t = threadIdx.x & 31;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const bool l0 = lanes >> t & 1ull, l1 = lanes >> (t + 32) & 1ull;
+  const bool c0 = cc >> t & 1ull, c1 = cc >> (t + 32) & 1ull;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < g.nv; b += stride) {
+    const uint64_t base = b + (threadIdx.x & ~31u);
+    const uint32_t myv = (uint32_t)(base + t);
+    const uint32_t myd = myv < g.nv ? g.slots[myv] : 0u;
+    bool want = false;
+    uint32_t dm = __ballot_sync(0xFFFFFFFFu, myd != 0u);
+    for (; dm; dm &= dm - 1) {
+      const int i = __ffs(dm) - 1;
+      const uint32_t v = (uint32_t)(base + i);
+      const uint32_t *row = val + (uint64_t)v * WLANES;
+      const bool f0 = l0 && (c0 || __ldcg(row + t) != INF32);
+      const bool f1 = l1 && (c1 || __ldcg(row + t + 32) != INF32);
+      const unsigned long long m = ballot64(f0, f1);
+      if (t == i && m) {
+        m_out[v] = m;
+        want = true;
+      }
+    }
+    frontier_append_block(out, want, myv, want ? myd : 0u);
+  }
+}
+
+// Deletion seeds: deleted (u,v) whose lane-q parent of v is u reset lane q.
+// A warp handles 32 deleted edges, one per step.
+__global__ void k_wide_seed_deleted(GraphView g, unsigned long long *st, uint32_t *val,
+                                    unsigned long long lanes, unsigned long long cc,
+                                    const uint64_t *keys, uint32_t n, unsigned long long *inval,
+                                    unsigned long long *m_out, FrontierView out) {
+  const int t = threadIdx.x & 31;
+  const bool l0 = lanes >> t & 1ull, l1 = lanes >> (t + 32) & 1ull;
+  const bool c0 = cc >> t & 1ull, c1 = cc >> (t + 32) & 1ull;
+  WideInvalidateOp op{st, val, WideAlgo{0, cc}};
+  unsigned long long r0 = 0, r1 = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < n; b += stride) {
+    const uint64_t base = b + (threadIdx.x & ~31u);
+    const uint64_t mi = base + t;
+    const uint64_t key = mi < n ? keys[mi] : 0ull;
+    bool want = false;
+    uint32_t okm = __ballot_sync(0xFFFFFFFFu, mi < n);
+    for (; okm; okm &= okm - 1) {
+      const int i = __ffs(okm) - 1;
+      const uint64_t k = __shfl_sync(0xFFFFFFFFu, (unsigned long long)key, i);
+      const uint32_t u = (uint32_t)(k >> 32), v = (uint32_t)k;
+      const bool x0 = l0 && op.lane(u, v, 0, 0, t, false, c0);
+      const bool x1 = l1 && op.lane(u, v, 0, 0, t + 32, false, c1);
+      r0 += x0;
+      r1 += x1;
+      const unsigned long long bits = ballot64(x0, x1);
+      if (bits && t == i && g.slots[v]) want = atomicOr(&m_out[v], bits) == 0ull;
+    }
+    const uint32_t v = (uint32_t)key;
+    frontier_append(out, want, v, want ? g.slots[v] : 0u);
+  }
+  if (r0) atomicAdd(&inval[t], r0);
+  if (r1) atomicAdd(&inval[t + 32], r1);
+}
+
+// Insert-only fast path: relax just the kept inserted edges in the lanes of
+// `lanes`; each inserted edge counts once per lane.
+__global__ void k_wide_relax_inserted(GraphView g, unsigned long long *st, uint32_t *val,
+                                      unsigned long long lanes, WideAlgo algo,
+                                      const uint64_t *keys, const uint32_t *w,
+                                      const uint32_t *n_ptr, unsigned long long *m_out,
+                                      FrontierView out, unsigned long long *lane_edges) {
+  const uint32_t n = *n_ptr;
+  const int t = threadIdx.x & 31;
+  const bool l0 = lanes >> t & 1ull, l1 = lanes >> (t + 32) & 1ull;
+  const bool s0 = algo.sssp >> t & 1ull, s1 = algo.sssp >> (t + 32) & 1ull;
+  const bool c0 = algo.cc >> t & 1ull, c1 = algo.cc >> (t + 32) & 1ull;
+  WideRelaxOp op{st, val, algo};
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint32_t counted = 0;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < n; b += stride) {
+    const uint64_t base = b + (threadIdx.x & ~31u);
+    const uint64_t mi = base + t;
+    const uint64_t key = mi < n ? keys[mi] : 0ull;
+    uint32_t wt = 1u;
+    if (mi < n) {
+      const uint32_t u = (uint32_t)(key >> 32), v = (uint32_t)key;
+      wt = g.wmode == W_EXPLICIT ? w[mi] : g.wmode == W_SYNTH ? (u + v) % 128u + 1u : 1u;
+      ++counted;
+    }
+    bool want = false;
+    uint32_t okm = __ballot_sync(0xFFFFFFFFu, mi < n);
+    for (; okm; okm &= okm - 1) {
+      const int i = __ffs(okm) - 1;
+      const uint64_t k = __shfl_sync(0xFFFFFFFFu, (unsigned long long)key, i);
+      const uint32_t wi = __shfl_sync(0xFFFFFFFFu, wt, i);
+      const uint32_t u = (uint32_t)(k >> 32), v = (uint32_t)k;
+      const uint32_t *row = val + (uint64_t)u * WLANES;
+      const uint32_t vu0 = l0 ? __ldcg(row + t) : INF32;
+      const uint32_t vu1 = l1 ? __ldcg(row + t + 32) : INF32;
+      const bool x0 = l0 && op.lane(u, v, wi, vu0, t, s0, c0);
+      const bool x1 = l1 && op.lane(u, v, wi, vu1, t + 32, s1, c1);
+      const unsigned long long bits = ballot64(x0, x1);
+      if (bits && t == i && g.slots[v]) want = atomicOr(&m_out[v], bits) == 0ull;
+    }
+    const uint32_t v = (uint32_t)key;
+    frontier_append(out, want, v, want ? g.slots[v] : 0u);
+  }
+  const uint32_t c = warp_sum(counted);
+  if (t == 0 && c) {
+    for (int q = 0; q < WLANES; ++q)
+      if (lanes >> q & 1ull) atomicAdd(&lane_edges[q], (unsigned long long)c);
+  }
+}
+
+__global__ void k_clear_masks64(const uint32_t *vtx, const unsigned long long *cnt,
+                                unsigned long long *mask) {
+  clear_prev_masks64(vtx, cnt, mask);
+}
+
+}  // namespace sgs

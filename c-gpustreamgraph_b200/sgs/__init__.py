@@ -43,7 +43,7 @@ ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of memory",
 EXPORTS = [
     "sgs_version", "sgs_last_error", "sgs_config_default", "sgs_create",
     "sgs_destroy", "sgs_load_csr", "sgs_load_edge_list", "sgs_load_rmat",
-    "sgs_query_add", "sgs_query_remove", "sgs_apply_batch", "sgs_gather",
+    "sgs_query_add", "sgs_query_add_many", "sgs_query_remove", "sgs_apply_batch", "sgs_gather",
     "sgs_get_query_stats", "sgs_get_engine_stats", "sgs_graph_export",
     "sgs_synchronize", "sgs_kernel_timing", "sgs_get_kernel_stats",
     "sgs_query_summary", "sgs_gen_update_stream", "sgs_hash_weights",
@@ -53,8 +53,9 @@ EXPORTS = [
     "sgs_ppr_get_stats",
 ]
 
-K_GROUP, K_GROUP_INVAL, K_PR_PUSH = range(3)
-KERNEL_KINDS = {"group_relax": K_GROUP, "group_invalidate": K_GROUP_INVAL, "pr_push": K_PR_PUSH}
+K_GROUP, K_GROUP_INVAL, K_PR_PUSH, K_WIDE, K_WIDE_INVAL = range(5)
+KERNEL_KINDS = {"group_relax": K_GROUP, "group_invalidate": K_GROUP_INVAL, "pr_push": K_PR_PUSH,
+                "wide_relax": K_WIDE, "wide_invalidate": K_WIDE_INVAL}
 
 
 class SgsError(RuntimeError):
@@ -172,6 +173,7 @@ def lib():
     L.sgs_load_edge_list.argtypes = [vp, u32, u64, vp, vp, vp, i32]
     L.sgs_load_rmat.argtypes = [vp, u32, u32, u64, dbl, dbl, dbl, u64]
     L.sgs_query_add.argtypes = [vp, i32, u32, C.POINTER(i32)]
+    L.sgs_query_add_many.argtypes = [vp, u32, vp, vp, vp]
     L.sgs_query_remove.argtypes = [vp, i32]
     L.sgs_apply_batch.argtypes = [vp, vp, vp, vp, u64, vp, vp, u64, i32]
     L.sgs_gather.argtypes = [vp, i32, i32, vp, i32]
@@ -371,6 +373,22 @@ class Engine:
         q = Query(self, qid.value, algo, source)
         self._queries[qid.value] = q
         return q
+
+    def add_queries(self, specs):
+        """Registers many queries at once: specs = [(algo, source), ...].  The
+        BFS/SSSP/CC ones share group lanes and converge together."""
+        specs = [(ALGOS[a] if isinstance(a, str) else int(a), int(src)) for a, src in specs]
+        n = len(specs)
+        algos = np.array([a for a, _ in specs], np.int32)
+        srcs = np.array([x for _, x in specs], np.uint32)
+        ids = np.zeros(max(n, 1), np.int32)
+        _check(lib().sgs_query_add_many(self.h, n, _ptr(algos), _ptr(srcs), _ptr(ids)))
+        out = []
+        for i, (a, src) in enumerate(specs):
+            q = Query(self, int(ids[i]), a, src)
+            self._queries[q.qid] = q
+            out.append(q)
+        return out
 
     def remove_query(self, q):
         _check(lib().sgs_query_remove(self.h, q.qid if isinstance(q, Query) else q))

@@ -93,7 +93,9 @@ typedef struct sgs_config {
   uint32_t slack_div;     /* per-block slack: cap = deg + deg/slack_div + 2 */
   double arena_headroom;  /* extra arena fraction for relocated blocks    */
   uint32_t group_size;    /* BFS/SSSP/CC queries relaxed together per edge
-                             pass (1..4); 1 = one query per pass            */
+                             pass: 1..4 (narrow groups: lanes in one 32-B
+                             sector) or 5..64 (wide groups: one 512-B row
+                             per vertex, a warp's threads over the lanes) */
 } sgs_config;
 
 typedef struct sgs_query_stats {
@@ -132,7 +134,9 @@ typedef struct sgs_engine_stats {
 #define SGS_K_GROUP 0        /* BFS/SSSP/CC relaxation of a query group   */
 #define SGS_K_GROUP_INVAL 1  /* parent-tree invalidation of a query group */
 #define SGS_K_PR_PUSH 2      /* PageRank residual push                    */
-#define SGS_K_COUNT 3
+#define SGS_K_WIDE 3         /* relaxation of a wide query group          */
+#define SGS_K_WIDE_INVAL 4   /* parent-tree invalidation of a wide group  */
+#define SGS_K_COUNT 5
 typedef struct sgs_kernel_stats {
   uint64_t launches;
   uint64_t slots;      /* positions walked (edges incl. tombstones)          */
@@ -172,6 +176,12 @@ SGS_API int sgs_load_rmat(sgs_engine *e, uint32_t scale, uint32_t edge_factor,
 /* Registers a query and runs it to convergence on the current graph
  * (InitGraph + Start).  source is clamped to [0, nv-1] as the samples do. */
 SGS_API int sgs_query_add(sgs_engine *e, int algo, uint32_t source, int *qid);
+/* Batched form (no reference counterpart; the reference runs one source per
+ * engine): registers n queries at once; the BFS/SSSP/CC ones fill group lanes
+ * and each group that received lanes converges all of them in one pass, so
+ * many sources share every edge read.  qids[i] receives the i-th id. */
+SGS_API int sgs_query_add_many(sgs_engine *e, uint32_t n, const int *algos,
+                               const uint32_t *sources, int *qids);
 SGS_API int sgs_query_remove(sgs_engine *e, int qid);
 
 /* One snapshot: applies the batch to the graph and brings every registered

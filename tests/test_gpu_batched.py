@@ -1,0 +1,140 @@
+"""Batched multi-source queries: wide groups of up to 64 BFS / SSSP / CC
+lanes (group_size 5..64) and sgs_query_add_many, through the C ABI.
+
+Every lane must equal its own single-source run (group_size=1) and the CPU
+oracle -- values bit-exact, parents valid tight trees -- at the static start
+and after every snapshot (deletes and inserts, insert-only and delete-only
+batches), with lanes joining and leaving, several groups, a partly filled
+group, and the out-of-HBM tier."""
+import numpy as np
+import pytest
+
+import oracle as O
+import sgs
+from test_gpu_parity import Mirror, check_query
+
+pytestmark = pytest.mark.gpu
+
+
+def _specs(nv, n_bfs, n_sssp, n_cc, seed):
+    rng = np.random.default_rng(seed)
+    srcs = rng.integers(0, nv, n_bfs + n_sssp)
+    out = [(sgs.BFS, int(s)) for s in srcs[:n_bfs]]
+    out += [(sgs.SSSP, int(s)) for s in srcs[n_bfs:]]
+    out += [(sgs.CC, 0)] * n_cc
+    rng.shuffle(out)
+    return out
+
+
+def _stream(nv, row, col, seed, k, n, wseed):
+    i_s, i_d, d_s, d_d = O.gen_updates(nv, row, col, seed, k * n, k * n)
+    iw = np.array([O.weight_of(wseed, u, v) for u, v in zip(i_s, i_d)], np.uint32)
+    return i_s, i_d, iw, d_s, d_d
+
+
+@pytest.mark.parametrize("gs", [64, 17])
+def test_wide_group_static_and_snapshots(gs):
+    nv, row, col = O.rmat_csr(12, 16, 5)
+    w = O.weights(nv, row, col, 2, 0)
+    specs = _specs(nv, 28, 30, 6, gs)
+    i_s, i_d, iw, d_s, d_d = _stream(nv, row, col, 8, 3, 1000, 2)
+    with sgs.Engine(group_size=gs) as e:
+        e.load_csr(nv, row, col, w)
+        qs = e.add_queries(specs)
+        m = Mirror(nv, row, col, w)
+        for q in qs:
+            check_query(q, m, sgs.W_EXPLICIT)
+            assert q.stats()["converged"] == 1
+        for k in range(3):
+            sl = slice(k * 1000, (k + 1) * 1000)
+            e.apply_batch(i_s[sl], i_d[sl], iw[sl], d_s[sl], d_d[sl])
+            m.apply(i_s[sl], i_d[sl], iw[sl], d_s[sl], d_d[sl])
+            for q in qs:
+                check_query(q, m, sgs.W_EXPLICIT)
+
+
+def test_wide_lanes_equal_single_source_runs():
+    """Each lane of a 64-lane group equals the same query run alone
+    (group_size=1), value for value, through three snapshots."""
+    nv, row, col = O.rmat_csr(12, 16, 9)
+    w = O.weights(nv, row, col, 4, 0)
+    specs = _specs(nv, 20, 20, 4, 3)
+    i_s, i_d, iw, d_s, d_d = _stream(nv, row, col, 17, 3, 800, 4)
+    res = {}
+    for gs in (1, 64):
+        with sgs.Engine(group_size=gs) as e:
+            e.load_csr(nv, row, col, w)
+            qs = e.add_queries(specs)
+            out = [[q.value() for q in qs]]
+            for k in range(3):
+                sl = slice(k * 800, (k + 1) * 800)
+                e.apply_batch(i_s[sl], i_d[sl], iw[sl], d_s[sl], d_d[sl])
+                out.append([q.value() for q in qs])
+            res[gs] = out
+    for k in range(4):
+        for a, b in zip(res[1][k], res[64][k]):
+            assert np.array_equal(a, b)
+
+
+def test_several_groups_join_leave_and_one_sided_batches():
+    nv, row, col = O.rmat_csr(11, 16, 2)
+    w = O.weights(nv, row, col, 6, 0)
+    specs = _specs(nv, 60, 60, 10, 11)  # 130 lanes: three groups, the last partly filled
+    i_s, i_d, iw, d_s, d_d = _stream(nv, row, col, 5, 4, 600, 6)
+    e0 = np.empty(0, np.uint32)
+    with sgs.Engine(group_size=64) as e:
+        e.load_csr(nv, row, col, w)
+        qs = e.add_queries(specs)
+        m = Mirror(nv, row, col, w)
+        for k in range(4):
+            sl = slice(k * 600, (k + 1) * 600)
+            if k == 1:  # insert-only batch
+                args = (i_s[sl], i_d[sl], iw[sl], e0, e0)
+            elif k == 2:  # delete-only batch; lanes leave and new ones join first
+                for q in qs[::7]:
+                    e.remove_query(q)
+                keep = [q for i, q in enumerate(qs) if i % 7]
+                qs = keep + e.add_queries(_specs(nv, 5, 5, 1, 99))
+                args = (e0, e0, e0, d_s[sl], d_d[sl])
+            else:
+                args = (i_s[sl], i_d[sl], iw[sl], d_s[sl], d_d[sl])
+            e.apply_batch(*args)
+            m.apply(*args)
+            for q in qs:
+                check_query(q, m, sgs.W_EXPLICIT)
+
+
+@pytest.mark.parametrize("wmode", [sgs.W_SYNTH, sgs.W_UNIT])
+def test_wide_group_weight_modes_and_host_tier(wmode):
+    nv, row, col = O.rmat_csr(12, 16, 4)
+    specs = _specs(nv, 10, 20, 2, 5)
+    i_s, i_d, _, d_s, d_d = _stream(nv, row, col, 3, 2, 700, 1)
+    with sgs.Engine(group_size=64, weight_mode=wmode, hbm_budget_gb=0.0002, segments=64) as e:
+        e.load_csr(nv, row, col, None)
+        assert e.engine_stats()["hbm_resident_vertices"] < nv
+        qs = e.add_queries(specs)
+        m = Mirror(nv, row, col, None)
+        for q in qs:
+            check_query(q, m, wmode)
+        for k in range(2):
+            sl = slice(k * 700, (k + 1) * 700)
+            e.apply_batch(i_s[sl], i_d[sl], None, d_s[sl], d_d[sl])
+            m.apply(i_s[sl], i_d[sl], None, d_s[sl], d_d[sl])
+            for q in qs:
+                check_query(q, m, wmode)
+
+
+def test_add_many_narrow_groups_and_pagerank():
+    """sgs_query_add_many with narrow groups (group_size 4) and a PageRank
+    query in the same call."""
+    nv, row, col = O.rmat_csr(11, 16, 7)
+    w = O.weights(nv, row, col, 1, 0)
+    specs = _specs(nv, 5, 5, 1, 2) + [(sgs.PR, 0)]
+    with sgs.Engine(group_size=4) as e:
+        e.load_csr(nv, row, col, w)
+        qs = e.add_queries(specs)
+        m = Mirror(nv, row, col, w)
+        for q in qs:
+            check_query(q, m, sgs.W_EXPLICIT)
+        with pytest.raises(sgs.SgsError):
+            e.add_queries([(7, 0)])
