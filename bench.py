@@ -57,9 +57,17 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="snapshot", choices=["snapshot", "ppr"],
+    ap.add_argument("--workload", default="snapshot", choices=["snapshot", "ppr", "batched"],
                     help="snapshot: incremental SSSP/BFS/CC (the headline); ppr: weighted "
-                         "personalized PageRank forward + adjoint")
+                         "personalized PageRank forward + adjoint; batched: 256 BFS + 256 SSSP "
+                         "queries kept up to date together")
+    ap.add_argument("--batched-scale", type=int, default=22)
+    ap.add_argument("--batched-bfs", type=int, default=256)
+    ap.add_argument("--batched-sssp", type=int, default=256)
+    ap.add_argument("--batched-updates", type=int, default=100_000)
+    ap.add_argument("--group-size", type=int, default=64)
+    ap.add_argument("--plain-sample", type=int, default=32,
+                    help="batched workload: queries of the sample run one per edge pass")
     ap.add_argument("--ppr-scale", type=int, default=22)
     ap.add_argument("--ppr-vectors", type=int, default=64)
     ap.add_argument("--ppr-seeds", type=int, default=32)
@@ -387,6 +395,181 @@ def cpu_baseline(e, a):
             "parts": {k: {"edges": int(v[0]), "s": round(v[1], 3)} for k, v in parts.items()}}
 
 
+# ----------------------------------------------------------------- batched arm
+BATCHED_METRIC = ("GTEPS per snapshot, batched multi-source ({nb} BFS + {ns} SSSP, R-MAT s{scale}, "
+                  "{upd} updates/snapshot)")
+
+
+def largest_wcc_sources(nv, row, col, n, seed):
+    """n distinct vertices uniform from the largest weakly connected
+    component (scipy's connected components on the exported CSR)."""
+    import scipy.sparse as sp
+    import scipy.sparse.csgraph as cg
+
+    A = sp.csr_matrix((np.ones(len(col), np.int8), col.astype(np.int64), row.astype(np.int64)),
+                      shape=(nv, nv))
+    _, lab = cg.connected_components(A, directed=True, connection="weak")
+    big = int(np.argmax(np.bincount(lab)))
+    cand = np.nonzero(lab == big)[0]
+    rng = np.random.default_rng(seed)
+    return rng.choice(cand, n, replace=False).astype(np.uint32), len(cand)
+
+
+def run_snapshots(e, queries, batches, dev_of, warmup, steps):
+    """Applies warm-up then timed snapshots (device-resident batches);
+    returns (lane-edges traversed, device ms) over the timed ones."""
+    edges, ms = 0, 0.0
+    for k in range(warmup + steps):
+        isrc, idst, iw, dsrc, ddst, half = dev_of(batches[k])
+        e.apply_batch_ptr(isrc.data_ptr(), idst.data_ptr(), iw.data_ptr(), half,
+                          dsrc.data_ptr(), ddst.data_ptr(), half, 1)
+        if k >= warmup:
+            edges += sum(q.stats()["edges_traversed"] for q in queries)
+            ms += e.engine_stats()["last_batch_ms"]
+    return edges, ms
+
+
+def batched_arm(a, R):
+    """N1: 256 BFS + 256 SSSP queries with sources uniform from the largest
+    WCC, kept up to date over snapshots.  value = (query, edge) relaxations
+    of all queries per second of device time (batched: group_size 64).  The
+    plain figure runs a sample of the same sources one query per edge pass
+    (group_size 1) over the same snapshots."""
+    import torch
+
+    import sgs
+
+    dev = torch.device("cuda", R.local)
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    e = sgs.Engine(device=R.local, weight_mode=sgs.W_EXPLICIT, group_size=a.group_size)
+    e.load_rmat(a.batched_scale, a.edge_factor, a.seed, 0.57, 0.19, 0.19, wseed=a.seed)
+    nv = int(e.engine_stats()["nv"])
+    row, col, _ = e.export()
+    nq = a.batched_bfs + a.batched_sssp
+    srcs, wcc = largest_wcc_sources(nv, row, col, nq, a.seed)
+    specs = [(sgs.BFS, int(x)) for x in srcs[:a.batched_bfs]] + \
+            [(sgs.SSSP, int(x)) for x in srcs[a.batched_bfs:]]
+    half = a.batched_updates // 2
+    nb = a.warmup + a.steps + (0 if a.no_e2e else a.steps)
+    i_s, i_d, d_s, d_d = sgs.gen_update_stream(nv, row, col, a.seed * 1000003, nb * half, nb * half)
+    i_w = sgs.hash_weights(a.seed, i_s, i_d)
+    del row, col
+    batches = [tuple(x[k * half:(k + 1) * half] for x in (i_s, i_d, i_w, d_s, d_d)) for k in range(nb)]
+    dev_b = {}
+
+    def dev_of(b):
+        key = id(b)
+        if key not in dev_b:
+            dev_b[key] = [torch.from_numpy(x.view(np.int32)).to(dev) for x in b] + [half]
+        return dev_b[key]
+
+    t_gen = time.time() - t0
+    # static start of all queries together
+    e.synchronize()
+    ts = time.perf_counter()
+    qs = e.add_queries(specs)
+    e.synchronize()
+    static_s = time.perf_counter() - ts
+    static_edges = sum(q.stats()["edges_traversed"] for q in qs)
+    static_ms = sum(q.stats()["ms"] for q in qs[::a.group_size])
+    # ---------------- timed snapshots
+    e.kernel_timing(True)
+    clocks = Clocks(R.local)
+    R.barrier()
+    torch.cuda.synchronize()
+    l0 = e.engine_stats()["kernel_launches"]
+    clocks.start()
+    w0 = time.perf_counter()
+    edges, dev_ms = run_snapshots(e, qs, batches, dev_of, a.warmup, a.steps)
+    torch.cuda.synchronize()
+    R.barrier()
+    wall_ms = (time.perf_counter() - w0) * 1e3
+    clk = clocks.stop()
+    launches = int(e.engine_stats()["kernel_launches"] - l0)
+    kst = e.kernel_stats()
+    e.kernel_timing(False)
+    # ---------------- e2e: pinned host batches + every query's summary read back
+    e2e = None
+    if not a.no_e2e:
+        pinned = []
+        for k in range(a.warmup + a.steps, nb):
+            ps = []
+            for x in batches[k]:
+                t = torch.empty(len(x), dtype=torch.int32, pin_memory=True)
+                t.numpy()[:] = x.view(np.int32)
+                ps.append(t)
+            pinned.append(ps)
+        R.barrier()
+        e_edges, e_ms, out_b = 0, 0.0, 0
+        for ps in pinned:
+            t1 = time.perf_counter()
+            e.apply_batch_ptr(*(x.data_ptr() for x in ps[:3]), half, ps[3].data_ptr(), ps[4].data_ptr(),
+                              half, sgs.MEM_HOST)
+            sums = [q.summary() for q in qs]
+            e_ms += (time.perf_counter() - t1) * 1e3
+            out_b = sum(x.nbytes for x in sums)
+            e_edges += sum(q.stats()["edges_traversed"] for q in qs)
+        e_ms = R.max(e_ms)
+        e2e = {"value": round(R.sum(e_edges) / (e_ms * 1e6), 3), "unit": UNIT,
+               "h2d_bytes_per_step": half * 5 * 4, "d2h_bytes_per_step": int(out_b),
+               "ms_per_step": round(e_ms / a.steps, 2)}
+    # ---------------- self check at full size: incremental == from scratch for a few lanes
+    chk = {}
+    for q in qs[:: max(1, nq // 4)][:4]:
+        f = e.add_query(q.algo, q.source)
+        chk[f"{'bfs' if q.algo == sgs.BFS else 'sssp'}:{q.source}"] = bool(
+            np.array_equal(q.summary()[:3], f.summary()[:3]))
+        e.remove_query(f)
+    e.close()
+    # ---------------- plain: a sample of the same sources, one query per pass
+    plain = None
+    if a.plain_sample > 0:
+        k = min(a.plain_sample, nq)
+        sample = specs[:k // 2] + specs[a.batched_bfs:a.batched_bfs + (k - k // 2)]
+        p = sgs.Engine(device=R.local, weight_mode=sgs.W_EXPLICIT, group_size=1)
+        p.load_rmat(a.batched_scale, a.edge_factor, a.seed, 0.57, 0.19, 0.19, wseed=a.seed)
+        pq = p.add_queries(sample)
+        pe, pms = run_snapshots(p, pq, batches, dev_of, a.warmup, a.steps)
+        p.close()
+        plain = {"queries": k, "gteps": round(pe / (pms * 1e6), 3),
+                 "ms_per_snapshot_per_query": round(pms / a.steps / k, 3),
+                 "note": "same snapshots, each query its own edge pass (group_size 1)"}
+    T = R.max(dev_ms)
+    value = R.sum(edges) / (T * 1e6)
+    peak, peak_src = measured_peak_hbm()
+    dom = max(kst, key=lambda kk: kst[kk]["ms"])
+    kd = kst[dom]
+    achieved = kd["bytes_alg"] / (kd["ms"] * 1e-3) / 1e9 if kd["ms"] > 0 else 0.0
+    roof = {"bound": "hbm", "kernel": f"wide_map ({dom})" if dom.startswith("wide") else dom,
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "peak_source": peak_src, "traffic": None, "launches": kd["launches"],
+            "avg_launch_ms": round(kd["ms"] / max(kd["launches"], 1), 4),
+            "alg_bytes_per_launch": kd["bytes_alg"] / max(kd["launches"], 1)}
+    out = {
+        "metric": BATCHED_METRIC.format(nb=a.batched_bfs, ns=a.batched_sssp, scale=a.batched_scale,
+                                        upd=a.batched_updates),
+        "value": round(value, 3), "unit": UNIT, "n_gpus": R.world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": round(T / a.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (device R-MAT, seeded weights and update stream; sources from the largest WCC)",
+        "config": {"workload": f"{a.batched_bfs} BFS + {a.batched_sssp} SSSP queries, R-MAT scale "
+                               f"{a.batched_scale} ef {a.edge_factor} seed {a.seed}, {a.batched_updates} "
+                               f"updates/snapshot (50/50), group_size {a.group_size}",
+                   "nv": nv, "largest_wcc": int(wcc),
+                   "l2": "inputs larger than L2 (per-group state %.1f GB)" % (nv * 64 * 12 / 1e9),
+                   "parallelism": "replicas" if R.world > 1 else "single GPU"},
+        "e2e": e2e, "gpu_launches": launches, "roofline": roof, "clocks": clk,
+        "wall_ms_timed": round(wall_ms, 2),
+        "static_start": {"queries": nq, "gteps": round(static_edges / (static_ms * 1e6), 3),
+                         "device_ms": round(static_ms, 2), "wall_s": round(static_s, 3)},
+        "plain": plain, "selfcheck_incremental_eq_static": chk, "gen_s": round(t_gen, 2),
+        "kernel_stats": {kk: {k2: (round(v2, 4) if isinstance(v2, float) else v2) for k2, v2 in v.items()}
+                         for kk, v in kst.items()},
+    }
+    return out
+
+
 # ----------------------------------------------------------------- PPR adjoint arm
 PPR_METRIC = ("PPR forward+adjoint relaxations/s (weighted personalized PageRank, R-MAT s{scale}, "
               "{K} vectors x {seeds} seeds, loss on {targets} targets)")
@@ -628,9 +811,13 @@ def main():
                 "impl": "reference", "unavailable": "the reference has no personalized PageRank "
                 "or adjoint (its PageRank is the single unweighted vector of the snapshot workload)"}
         elif a.impl == "reference":
+            if a.workload == "batched":
+                a.scale, a.updates = a.batched_scale, a.batched_updates
             out = reference_arm(a, R)
         elif a.workload == "ppr":
             out = ppr_arm(a, R)
+        elif a.workload == "batched":
+            out = batched_arm(a, R)
         else:
             out = engine_arm(a, R)
         if R.rank == 0 and out is not None:

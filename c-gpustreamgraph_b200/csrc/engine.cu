@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -118,6 +119,7 @@ struct Group {
   uint32_t algo_packed = 0;     // narrow: 8 bits per lane
   uint64_t sssp = 0, cc = 0;    // lanes per algorithm (both widths)
   uint64_t inval[WLANES] = {};  // resets per lane in the last deletion phase
+  DBuf<uint32_t> ibits;         // bitmap of vertices reset in the last deletion phase
   bool wide() const { return width == WLANES; }
   LaneAlgo algo() const { return LaneAlgo{algo_packed}; }
   WideAlgo walgo() const { return WideAlgo{sssp, cc}; }
@@ -501,40 +503,50 @@ struct sgs_engine {
   // frontier are cleared at the end, so all mask buffers are zero again.
   template <class MakeOp>
   uint32_t run_group_rounds(MakeOp make_op, bool &converged, int kind, double per_slot,
-                            const char *round0 = nullptr) {
+                            const char *round0 = nullptr,
+                            const std::function<void()> *after0 = nullptr) {
     return run_rounds(
-        [&](uint32_t rr) {
-          auto op = make_op(gm[rr % 3].p, gm[(rr + 1) % 3].p);
-          const bool hp = rr >= 1;
-          { ++n_launch; group_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
-              fview(rr, cnt.p + rr), fview(rr + 1, cnt.p + rr + 1), op,
-              hp ? fb[(rr - 1) % 3].vtx.p : nullptr, hp ? cnt.p + rr - 1 : nullptr,
-              hp ? gm[(rr - 1) % 3].p : nullptr, b_lane.p, rstat.p + rr); }
-        },
-        false, converged, kind, per_slot, round0);
+        [&](uint32_t rr) { launch_group(rr, make_op(rr, gm[rr % 3].p, gm[(rr + 1) % 3].p)); },
+        false, converged, kind, per_slot, round0, after0);
   }
 
-  // The same for a wide group op (wide_map, u64 masks in wm).
-  template <class Op>
-  uint32_t run_wide_rounds(const Op &op, bool &converged, int kind, double per_slot,
-                           unsigned long long *lane_changes, const char *round0 = nullptr) {
-    GraphView g = view();
+  // The same for a wide group op (wide_map, u64 masks in wm); `op0` for
+  // round 0, `op` for the others.
+  template <class Op0, class Op>
+  uint32_t run_wide_rounds(const Op0 &op0, const Op &op, bool &converged, int kind, double per_slot,
+                           unsigned long long *lane_changes, const char *round0 = nullptr,
+                           const std::function<void()> *after0 = nullptr) {
     return run_rounds(
         [&](uint32_t rr) {
-          const bool hp = rr >= 1;
-          { ++n_launch; wide_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
-              g, fview(rr, cnt.p + rr), fview(rr + 1, cnt.p + rr + 1), op, wm[rr % 3].p,
-              wm[(rr + 1) % 3].p, hp ? fb[(rr - 1) % 3].vtx.p : nullptr,
-              hp ? cnt.p + rr - 1 : nullptr, hp ? wm[(rr - 1) % 3].p : nullptr, b_lane.p,
-              lane_changes, rstat.p + rr); }
+          if (rr == 0) launch_wide(rr, op0, lane_changes);
+          else launch_wide(rr, op, lane_changes);
         },
-        true, converged, kind, per_slot, round0);
+        true, converged, kind, per_slot, round0, after0);
+  }
+
+  template <class Op>
+  void launch_wide(uint32_t rr, const Op &op, unsigned long long *lane_changes) {
+    const bool hp = rr >= 1;
+    { ++n_launch; wide_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
+        view(), fview(rr, cnt.p + rr), fview(rr + 1, cnt.p + rr + 1), op, wm[rr % 3].p,
+        wm[(rr + 1) % 3].p, hp ? fb[(rr - 1) % 3].vtx.p : nullptr,
+        hp ? cnt.p + rr - 1 : nullptr, hp ? wm[(rr - 1) % 3].p : nullptr, b_lane.p,
+        lane_changes, rstat.p + rr); }
+  }
+
+  template <class Op>
+  void launch_group(uint32_t rr, const Op &op) {
+    const bool hp = rr >= 1;
+    { ++n_launch; group_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
+        fview(rr, cnt.p + rr), fview(rr + 1, cnt.p + rr + 1), op,
+        hp ? fb[(rr - 1) % 3].vtx.p : nullptr, hp ? cnt.p + rr - 1 : nullptr,
+        hp ? gm[(rr - 1) % 3].p : nullptr, b_lane.p, rstat.p + rr); }
   }
 
   // Round loop shared by both group widths: `launch(rr)` queues round rr.
   template <class Launch>
   uint32_t run_rounds(Launch launch, bool wide, bool &converged, int kind, double per_slot,
-                      const char *round0) {
+                      const char *round0, const std::function<void()> *after0 = nullptr) {
     const uint32_t maxr = cfg.max_rounds;
     uint32_t r = 0, rb = 2;
     converged = false;
@@ -552,6 +564,7 @@ struct sgs_engine {
         if (rr == 0 && round0) nvtxRangePushA(round0);
         launch(rr);
         if (rr == 0 && round0) nvtxRangePop();
+        if (rr == 0 && after0) (*after0)();
         if (ktiming) CK(cudaEventRecord(kev[2 * k + 1], s));
       }
       CK(cudaGetLastError());
@@ -597,20 +610,29 @@ struct sgs_engine {
       }
   }
 
-  // Relaxation rounds for the lanes whose frontier is in buffer 0.
-  uint32_t group_relax(Group &G, bool &conv, const char *round0 = nullptr) {
+  // Relaxation rounds for the lanes whose frontier is in buffer 0.  With
+  // `only0` (wide groups), round 0 relaxes only edges into vertices of that
+  // bitmap; `after0` runs right after round 0 (it may append to frontier 1).
+  uint32_t group_relax(Group &G, bool &conv, const char *round0 = nullptr,
+                       const uint32_t *only0 = nullptr,
+                       const std::function<void()> *after0 = nullptr) {
     GraphView g = view();
     if (G.wide()) {
       const bool anyw = G.sssp && cfg.weight_mode == SGS_W_EXPLICIT;
-      WideRelaxOp op{G.st.p, G.val.p, G.walgo()};
-      return run_wide_rounds(op, conv, SGS_K_WIDE, anyw ? 8.0 : 4.0, nullptr, round0);
+      WideRelaxOp<> op{G.st.p, G.val.p, G.walgo()};
+      WideRelaxOp<true> op0{G.st.p, G.val.p, G.walgo()};
+      op0.only = only0;
+      if (only0)
+        return run_wide_rounds(op0, op, conv, SGS_K_WIDE, anyw ? 8.0 : 4.0, nullptr, round0, after0);
+      return run_wide_rounds(op, op, conv, SGS_K_WIDE, anyw ? 8.0 : 4.0, nullptr, round0, after0);
     }
     const uint32_t anyw = G.any_sssp(G.used | 0xF) && cfg.weight_mode == SGS_W_EXPLICIT;
-    return run_group_rounds(
-        [&](uint32_t *mi, uint32_t *mo) {
-          return GroupRelaxOp<GMAX>{g, G.st.p, G.val.p, mi, mo, G.algo(), anyw};
+    return run_rounds(
+        [&](uint32_t rr) {
+          uint32_t *mi = gm[rr % 3].p, *mo = gm[(rr + 1) % 3].p;
+          launch_group(rr, GroupRelaxOp<GMAX>{g, G.st.p, G.val.p, mi, mo, G.algo(), anyw});
         },
-        conv, SGS_K_GROUP, anyw ? 8.0 : 4.0, round0);
+        false, conv, SGS_K_GROUP, anyw ? 8.0 : 4.0, round0, after0);
   }
 
   // PageRank rounds over the static frontier of all non-empty blocks:
@@ -960,22 +982,28 @@ struct sgs_engine {
       CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * WLANES, s));
       CK(cudaMemsetAsync(b_inval.p, 0, sizeof(unsigned long long) * WLANES, s));
       reset_counters(0);
+      if (G.wide()) {
+        const size_t nw = (size_t)nv / 32 + 1;
+        G.ibits.ensure(nw);
+        CK(cudaMemsetAsync(G.ibits.p, 0, sizeof(uint32_t) * nw, s));
+      }
       bool conv = false;
       if (G.wide()) {
         { ++n_launch; k_wide_seed_deleted<<<grid_elem(nd), 256, 0, s>>>(
-            g, G.st.p, G.val.p, G.used, G.cc, b_dkeys_s.p, (uint32_t)nd, b_inval.p, wm[0].p,
+            g, G.st.p, G.val.p, G.used, G.cc, b_dkeys_s.p, (uint32_t)nd, b_inval.p, G.ibits.p, wm[0].p,
             fview(0, cnt.p)); }
         CK(cudaGetLastError());
         WideInvalidateOp op{G.st.p, G.val.p, WideAlgo{0ull, G.cc}};  // no weights needed
-        run_wide_rounds(op, conv, SGS_K_WIDE_INVAL, 4.0, b_inval.p);
+        op.mark = G.ibits.p;
+        run_wide_rounds(op, op, conv, SGS_K_WIDE_INVAL, 4.0, b_inval.p);
       } else {
         { ++n_launch; k_group_seed_deleted<GMAX><<<grid_elem(nd), 256, 0, s>>>(
-            g, G.st.p, G.val.p, (uint32_t)G.used, G.algo(), b_dkeys_s.p, (uint32_t)nd, b_inval.p, gm[0].p,
-            fview(0, cnt.p)); }
+            g, G.st.p, G.val.p, (uint32_t)G.used, G.algo(), b_dkeys_s.p, (uint32_t)nd, b_inval.p,
+            nullptr, gm[0].p, fview(0, cnt.p)); }
         CK(cudaGetLastError());
         run_group_rounds(
-            [&](uint32_t *mi, uint32_t *mo) {
-              return GroupInvalidateOp<GMAX>{g, G.st.p, G.val.p, mi, mo, G.algo(), b_inval.p};
+            [&](uint32_t, uint32_t *mi, uint32_t *mo) {
+              return GroupInvalidateOp<GMAX>{g, G.st.p, G.val.p, mi, mo, G.algo(), b_inval.p, nullptr};
             },
             conv, SGS_K_GROUP_INVAL, 4.0);
       }
@@ -1038,9 +1066,18 @@ struct sgs_engine {
         if (!conv) fail(SGS_ERR_NOCONV, "round limit reached before convergence");
       }
     }
-    // ---- add phase per group: re-push from every reached vertex of every
-    // lane when some lane was invalidated (SyncPushDDBAll), else relax only
-    // the inserted edges; then rounds to convergence
+    // ---- add phase per group.  After an invalidation the reference re-pushes
+    // from every reached vertex (SyncPushDDBAll), and so do narrow groups.
+    // In a wide group that first round visits the same edges but relaxes
+    // only those into vertices reset in this snapshot (bitmap G.ibits), and
+    // the kept inserted edges are relaxed right after it: before the repair,
+    // every other edge (u,v) already satisfies value(u) + w >= value(v) -- u
+    // kept a value that was valid on the old graph, v kept its own, and the
+    // edge existed -- so these two sets hold every violated edge.  Later
+    // rounds are unrestricted, so the fixed point is the same.  (For a narrow
+    // group the 16-B state row costs no more than the bitmap probe, so the
+    // restriction does not pay.)  Without invalidation only the inserted
+    // edges are relaxed.  Then rounds to convergence.
     for (size_t i = 0; i < ng; ++i) {
       Group &G = *groups[i];
       if (!G.used) continue;
@@ -1067,8 +1104,22 @@ struct sgs_engine {
             b_nkept.p, gm[0].p, fview(0, cnt.p), b_lane.p); }
       }
       CK(cudaGetLastError());
+      // inserted edges after the restricted round 0, into its output frontier
+      const std::function<void()> ins_after0 = [&] {
+        if (G.wide())
+          { ++n_launch; k_wide_relax_inserted<<<grid_elem(ni), 256, 0, s>>>(
+              g, G.st.p, G.val.p, G.used, G.walgo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr,
+              b_nkept.p, wm[1].p, fview(1, cnt.p + 1), b_lane.p); }
+        else
+          { ++n_launch; k_group_relax_inserted<GMAX><<<grid_elem(ni), 256, 0, s>>>(
+              g, G.st.p, G.val.p, (uint32_t)G.used, G.algo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr,
+              b_nkept.p, gm[1].p, fview(1, cnt.p + 1), b_lane.p); }
+      };
       bool conv = false;
-      const uint32_t rounds = group_relax(G, conv, any_inval ? "sgs:sweep" : nullptr);
+      const uint32_t rounds =
+          any_inval && G.wide() ? group_relax(G, conv, "sgs:sweep", G.ibits.p, ni ? &ins_after0 : nullptr)
+          : any_inval           ? group_relax(G, conv, "sgs:sweep")
+                                : group_relax(G, conv);
       CK(cudaEventRecord(ev_q.b, s));
       sync();
       float ms = 0;

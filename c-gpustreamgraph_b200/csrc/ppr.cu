@@ -170,13 +170,14 @@ __global__ void k_csc_probs(const double *pr, const uint32_t *ceid, uint64_t ne,
     pc[i] = pr[ceid[i]];
 }
 
-// acc[j] += sum_{i in [b,e)} p[i] x[nbr[i], kb + j LPE] for this lane's
-// neighbour group eg (neighbours b+eg, b+eg+NEG, ...), four neighbours deep.
+// Narrow rows (K < 32): each lane group loads its own neighbours' ids,
+// probabilities and rows, four neighbours deep (neighbours b+eg, b+eg+NEG, ...).
 template <int LPE, int CPL>
-__device__ __forceinline__ void gather_rows(const uint32_t *__restrict__ nbr,
-                                            const double *__restrict__ p, uint64_t b, uint64_t e,
-                                            int eg, uint32_t kb, uint32_t K,
-                                            const double *__restrict__ x, double (&acc)[CPL]) {
+__device__ __forceinline__ void gather_rows_direct(const uint32_t *__restrict__ nbr,
+                                                   const double *__restrict__ p, uint64_t b,
+                                                   uint64_t e, int eg, uint32_t kb, uint32_t K,
+                                                   const double *__restrict__ x,
+                                                   double (&acc)[CPL]) {
   constexpr int NEG = 32 / LPE;
   uint64_t i = b + eg;
   for (; i + 3 * NEG < e; i += 4 * NEG) {
@@ -211,11 +212,55 @@ __device__ __forceinline__ void gather_rows(const uint32_t *__restrict__ nbr,
   }
 }
 
+// acc[j] += sum_{i in [b,e)} p[i] x[nbr[i], kb + j LPE] for this lane's
+// neighbour group eg.  Neighbour ids and probabilities come 32 at a time in
+// one coalesced load per warp and are handed to the lane groups by shuffles
+// (group eg takes neighbours eg, eg + NEG, ...), so the only dependent load
+// per neighbour is its row; DEPTH neighbours per group are in flight at once.
+template <int LPE, int CPL>
+__device__ __forceinline__ void gather_rows(const uint32_t *__restrict__ nbr,
+                                            const double *__restrict__ p, uint64_t b, uint64_t e,
+                                            int lane, int eg, uint32_t kb, uint32_t K,
+                                            const double *__restrict__ x, double (&acc)[CPL]) {
+  constexpr int NEG = 32 / LPE;
+  constexpr int DEPTH = LPE < 4 ? LPE : 4;
+  for (uint64_t c = b; c < e; c += 32) {
+    const uint32_t cnt = e - c < 32 ? (uint32_t)(e - c) : 32u;
+    const uint32_t mu = (uint32_t)lane < cnt ? __ldg(nbr + c + lane) : 0u;
+    const double mp = (uint32_t)lane < cnt ? __ldg(p + c + lane) : 0.0;
+#pragma unroll 1
+    for (int r0 = 0; r0 < LPE && (uint32_t)(NEG * r0) < cnt; r0 += DEPTH) {
+      uint32_t u[DEPTH];
+      double pp[DEPTH];
+      bool ok[DEPTH];
+#pragma unroll
+      for (int q = 0; q < DEPTH; ++q) {
+        const int jn = eg + NEG * (r0 + q);  // < 32
+        u[q] = __shfl_sync(0xFFFFFFFFu, mu, jn);
+        pp[q] = __shfl_sync(0xFFFFFFFFu, mp, jn);
+        ok[q] = (uint32_t)jn < cnt;
+      }
+      double xv[DEPTH][CPL];
+#pragma unroll
+      for (int q = 0; q < DEPTH; ++q)
+#pragma unroll
+        for (int jj = 0; jj < CPL; ++jj) {
+          const uint32_t k = kb + jj * LPE;
+          xv[q][jj] = ok[q] && k < K ? __ldg(x + (uint64_t)u[q] * K + k) : 0.0;
+        }
+#pragma unroll
+      for (int q = 0; q < DEPTH; ++q)
+#pragma unroll
+        for (int jj = 0; jj < CPL; ++jj) acc[jj] = fma(pp[q], xv[q][jj], acc[jj]);
+    }
+  }
+}
+
 // One Jacobi step over the work items [0, npieces) (pieces of heavy vertices:
 // partial sums to part[piece][K]) and [npieces, npieces + nv) (light vertices:
 // out[v,k] = c B[v,k] + alpha sum p x, |out - x| added to *diff).
 template <int LPE, int CPL>
-__global__ void __launch_bounds__(THREADS, CPL == 1 ? 8 : 6)
+__global__ void __launch_bounds__(THREADS, LPE == 32 ? 1 : 8)
     k_ppr_step(const uint64_t *__restrict__ ptr, const uint32_t *__restrict__ nbr,
                const double *__restrict__ p, uint32_t nv, const uint32_t *__restrict__ pv,
                const uint32_t *__restrict__ poff, uint32_t npieces, uint32_t K, double alpha,
@@ -225,7 +270,10 @@ __global__ void __launch_bounds__(THREADS, CPL == 1 ? 8 : 6)
   const int sub = lane % LPE, eg = lane / LPE;
   double dsum = 0.0;
   const uint32_t items = npieces + nv;
-  for (uint32_t wi = warp_id(); wi < items; wi += num_warps()) {
+  const uint32_t W = num_warps();
+  uint64_t pb = 0, pe = 0;  // bounds of this warp's next light vertex, loaded ahead
+  bool have = false;
+  for (uint32_t wi = warp_id(); wi < items; wi += W) {
     uint32_t v;
     uint64_t b, e;
     const bool piece = wi < npieces;
@@ -235,15 +283,30 @@ __global__ void __launch_bounds__(THREADS, CPL == 1 ? 8 : 6)
       e = min(b + PIECE, ptr[v + 1]);
     } else {
       v = wi - npieces;
-      b = ptr[v];
-      e = ptr[v + 1];
+      if (have) {
+        b = pb;
+        e = pe;
+      } else {
+        b = ptr[v];
+        e = ptr[v + 1];
+      }
+      if constexpr (LPE == 32) {  // the narrow forms have no registers to spare
+        have = wi + W < items;
+        if (have) {
+          pb = ptr[v + W];
+          pe = ptr[v + W + 1];
+        }
+      }
       if (e - b > PIECE) continue;  // summed by its pieces
     }
     for (uint32_t k0 = 0; k0 < K; k0 += LPE * CPL) {
       double acc[CPL];
 #pragma unroll
       for (int j = 0; j < CPL; ++j) acc[j] = 0.0;
-      gather_rows<LPE, CPL>(nbr, p, b, e, eg, k0 + sub, K, x, acc);
+      if constexpr (LPE == 32)
+        gather_rows<LPE, CPL>(nbr, p, b, e, lane, eg, k0 + sub, K, x, acc);
+      else
+        gather_rows_direct<LPE, CPL>(nbr, p, b, e, eg, k0 + sub, K, x, acc);
 #pragma unroll
       for (int j = 0; j < CPL; ++j)
 #pragma unroll

@@ -93,6 +93,16 @@ __device__ __forceinline__ uint32_t edge_weight(const GraphView &g, uint64_t o,
   return 1u;
 }
 
+// Vertex bitmaps (one bit per vertex): `only` restricts a relaxation round to
+// destinations whose bit is set; `mark` records vertices reset by the
+// parent-tree invalidation.
+__device__ __forceinline__ bool bit_at(const uint32_t *bm, uint32_t v) {
+  return __ldcg(&bm[v >> 5]) >> (v & 31) & 1u;
+}
+__device__ __forceinline__ void bit_set(uint32_t *bm, uint32_t v) {
+  atomicOr(&bm[v >> 5], 1u << (v & 31));
+}
+
 // Warp-aggregated append of (v, d) into a frontier.  Must be called by all 32
 // lanes of a converged warp; `want` selects the lanes that append.  One packed
 // 64-bit atomicAdd per warp reserves the slots and the edge range together.

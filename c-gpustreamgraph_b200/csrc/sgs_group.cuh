@@ -149,6 +149,7 @@ struct GroupInvalidateOp {
   uint32_t *m_out;
   LaneAlgo algo;
   unsigned long long *inval;  // [GMAX] per-lane reset counts
+  uint32_t *mark;             // bitmap of reset vertices (may be null)
   __device__ __forceinline__ Payload load(uint32_t v) const {
     Payload p;
     p.off = g.off[v];
@@ -184,6 +185,7 @@ struct GroupInvalidateOp {
           atomicAdd(&inval[q], 1ull);
         }
       }
+      if (bits && mark) bit_set(mark, dst[k]);
       if (bits && g.slots[dst[k]] && atomicOr(&m_out[dst[k]], bits) == 0u) app |= 1u << k;
     }
     return app;
@@ -345,7 +347,8 @@ __global__ void k_group_seed_one(GraphView g, uint32_t v, uint32_t bits, uint32_
 template <int S>
 __global__ void k_group_seed_deleted(GraphView g, unsigned long long *st, uint32_t *val, uint32_t lanes,
                                      LaneAlgo algo, const uint64_t *keys, uint32_t n,
-                                     unsigned long long *inval, uint32_t *m_out, FrontierView out) {
+                                     unsigned long long *inval, uint32_t *mark, uint32_t *m_out,
+                                     FrontierView out) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < n; b += stride) {
     const uint64_t i = b + threadIdx.x;
@@ -371,6 +374,7 @@ __global__ void k_group_seed_deleted(GraphView g, unsigned long long *st, uint32
         }
       }
       if (bits) {
+        if (mark) bit_set(mark, v);
         d = g.slots[v];
         want = d && atomicOr(&m_out[v], bits) == 0u;
       }
@@ -379,8 +383,9 @@ __global__ void k_group_seed_deleted(GraphView g, unsigned long long *st, uint32
   }
 }
 
-// Insert-only fast path: relax just the kept inserted edges in the selected
-// lanes.
+// Relaxes just the kept inserted edges in the selected lanes: the whole
+// repair of an insert-only batch, and the inserted-edge half of the repair
+// after an invalidation (the other half is the restricted first round).
 template <int S>
 __global__ void k_group_relax_inserted(GraphView g, unsigned long long *st, uint32_t *val, uint32_t lanes,
                                        LaneAlgo algo, const uint64_t *keys, const uint32_t *w,

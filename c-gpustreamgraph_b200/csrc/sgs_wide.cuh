@@ -47,14 +47,27 @@ __device__ __forceinline__ void clear_prev_masks64(const uint32_t *vtx, const un
 
 // Relaxation of one lane: candidate from the source value, strict
 // improvement through the packed word, mirror lowered after it.
+template <bool Restrict = false>
 struct WideRelaxOp {
   static constexpr bool kNeedsSourceValues = true;
+  static constexpr bool kRestrict = Restrict;
+  using Pre = uint32_t;
   unsigned long long *st;
   uint32_t *val;
   WideAlgo algo;
+  const uint32_t *only = nullptr;  // restrict to destinations in this bitmap
+  uint32_t *mark = nullptr;
+  // the destination's current value (loaded ahead of the decision)
+  __device__ __forceinline__ Pre pre(uint32_t v, int q) const {
+    return __ldcg(&val[(uint64_t)v * WLANES + q]);
+  }
   // is_sssp / is_cc: this lane's algorithm; vu: the lane's value at u.
   __device__ __forceinline__ bool lane(uint32_t u, uint32_t v, uint32_t w, uint32_t vu, int q,
                                        bool is_sssp, bool is_cc) const {
+    return fin(u, v, w, vu, q, is_sssp, is_cc, pre(v, q));
+  }
+  __device__ __forceinline__ bool fin(uint32_t u, uint32_t v, uint32_t w, uint32_t vu, int q,
+                                      bool is_sssp, bool is_cc, Pre cur) const {
     uint32_t cand;
     if (is_cc) {
       cand = vu;
@@ -64,8 +77,8 @@ struct WideRelaxOp {
       if (nd >= INF32) return false;
       cand = (uint32_t)nd;
     }
+    if (cand >= cur) return false;
     const uint64_t idx = (uint64_t)v * WLANES + q;
-    if (cand >= __ldcg(&val[idx])) return false;
     const unsigned long long old = atomicMin(&st[idx], ((unsigned long long)cand << 32) | u);
     if (cand < (uint32_t)(old >> 32)) {
       atomicMin(&val[idx], cand);
@@ -79,13 +92,23 @@ struct WideRelaxOp {
 // (CAS on the packed word), the mirror with it; resets are counted per lane.
 struct WideInvalidateOp {
   static constexpr bool kNeedsSourceValues = false;
+  static constexpr bool kRestrict = false;
+  using Pre = unsigned long long;
   unsigned long long *st;
   uint32_t *val;
   WideAlgo algo;
-  __device__ __forceinline__ bool lane(uint32_t u, uint32_t v, uint32_t, uint32_t, int q, bool,
-                                       bool is_cc) const {
+  const uint32_t *only = nullptr;
+  uint32_t *mark = nullptr;  // bitmap of reset vertices
+  __device__ __forceinline__ Pre pre(uint32_t v, int q) const {
+    return __ldcg(&st[(uint64_t)v * WLANES + q]);
+  }
+  __device__ __forceinline__ bool lane(uint32_t u, uint32_t v, uint32_t w, uint32_t vu, int q,
+                                       bool is_sssp, bool is_cc) const {
+    return fin(u, v, w, vu, q, is_sssp, is_cc, pre(v, q));
+  }
+  __device__ __forceinline__ bool fin(uint32_t u, uint32_t v, uint32_t, uint32_t, int q, bool,
+                                      bool is_cc, Pre cu) const {
     const uint64_t idx = (uint64_t)v * WLANES + q;
-    const unsigned long long cu = __ldcg(&st[idx]);
     if ((uint32_t)cu != u) return false;
     const unsigned long long rst = is_cc ? (((unsigned long long)v << 32) | INF32) : ~0ull;
     if (atomicCAS(&st[idx], cu, rst) != cu) return false;
@@ -101,7 +124,7 @@ struct WideInvalidateOp {
 // every lane of its mask ((query, edge) pairs relaxed); lane_changes counts
 // the lanes changed (resets for the invalidation op).
 template <class Op>
-__global__ void __launch_bounds__(RELAX_THREADS)
+__global__ void __launch_bounds__(RELAX_THREADS, 3)
     wide_map(GraphView g, FrontierView in, FrontierView out, Op op,
              const unsigned long long *m_in, unsigned long long *m_out, const uint32_t *prev_vtx,
              const unsigned long long *prev_cnt, unsigned long long *prev_mask,
@@ -191,6 +214,7 @@ __global__ void __launch_bounds__(RELAX_THREADS)
             le = l;
             v = __ldcg(adj_ptr(g, s_off[l]) + j);
             ok = v != SGS_TOMB;
+            if constexpr (Op::kRestrict) ok = ok && bit_at(op.only, v);
             if (ok && op.algo.sssp && s_mask[l] & op.algo.sssp)
               w = g.wmode == W_EXPLICIT ? __ldcg(wgt_ptr(g, s_off[l]) + j)
                   : g.wmode == W_SYNTH  ? (s_vtx[l] + v) % 128u + 1u
@@ -198,30 +222,55 @@ __global__ void __launch_bounds__(RELAX_THREADS)
           }
         }
         bool want = false;
-        int cur = -1;
-        uint32_t vu0 = INF32, vu1 = INF32;
-        const uint32_t okb = __ballot_sync(0xFFFFFFFFu, ok);
-        for (uint32_t rem = okb; rem; rem &= rem - 1) {
-          const int i = __ffs(rem) - 1;
-          const int li = __shfl_sync(0xFFFFFFFFu, le, i);
-          const uint32_t vi = __shfl_sync(0xFFFFFFFFu, v, i);
-          const uint32_t wi = __shfl_sync(0xFFFFFFFFu, w, i);
-          const uint32_t u = s_vtx[li];
-          const unsigned long long mk = s_mask[li];
-          const bool a0 = mk >> t & 1ull, a1 = mk >> (t + 32) & 1ull;
-          if (Op::kNeedsSourceValues && li != cur) {
-            cur = li;
-            const uint32_t *row = op.val + (uint64_t)u * WLANES;
-            vu0 = a0 ? __ldcg(row + t) : INF32;
-            vu1 = a1 ? __ldcg(row + t + 32) : INF32;
+        // four edges per step: their destination rows (and source rows) are
+        // all requested before any decision, so a warp keeps 16 loads per
+        // thread in flight instead of waiting once per edge
+        constexpr int D = 4;
+        uint32_t rem = __ballot_sync(0xFFFFFFFFu, ok);
+        while (rem) {
+          int ii[D], li[D];
+          uint32_t vi[D], wi[D], uu[D];
+          bool a0[D], a1[D];
+#pragma unroll
+          for (int q = 0; q < D; ++q) {
+            ii[q] = rem ? __ffs(rem) - 1 : -1;
+            rem = rem ? rem & (rem - 1) : 0u;
+            const int src = ii[q] < 0 ? 0 : ii[q];
+            li[q] = __shfl_sync(0xFFFFFFFFu, le, src);
+            vi[q] = __shfl_sync(0xFFFFFFFFu, v, src);
+            wi[q] = __shfl_sync(0xFFFFFFFFu, w, src);
+            uu[q] = s_vtx[li[q]];
+            const unsigned long long mk = ii[q] < 0 ? 0ull : s_mask[li[q]];
+            a0[q] = mk >> t & 1ull;
+            a1[q] = mk >> (t + 32) & 1ull;
           }
-          const bool c0 = a0 && op.lane(u, vi, wi, vu0, t, sssp0, cc0);
-          const bool c1 = a1 && op.lane(u, vi, wi, vu1, t + 32, sssp1, cc1);
-          chg0 += c0;
-          chg1 += c1;
-          const unsigned long long bits = ballot64(c0, c1);
-          if (bits && t == i && g.slots[vi])
-            want = atomicOr(&m_out[vi], bits) == 0ull;
+          typename Op::Pre c0[D], c1[D];
+          uint32_t vu0[D], vu1[D];
+#pragma unroll
+          for (int q = 0; q < D; ++q) {
+            c0[q] = a0[q] ? op.pre(vi[q], t) : typename Op::Pre(0);
+            c1[q] = a1[q] ? op.pre(vi[q], t + 32) : typename Op::Pre(0);
+            vu0[q] = INF32;
+            vu1[q] = INF32;
+            if (Op::kNeedsSourceValues) {
+              // a stale (higher) source value is harmless: a source that
+              // improves during this round is appended and pushes again
+              const uint32_t *row = op.val + (uint64_t)uu[q] * WLANES;
+              if (a0[q]) vu0[q] = __ldg(row + t);
+              if (a1[q]) vu1[q] = __ldg(row + t + 32);
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < D; ++q) {
+            const bool x0 = a0[q] && op.fin(uu[q], vi[q], wi[q], vu0[q], t, sssp0, cc0, c0[q]);
+            const bool x1 = a1[q] && op.fin(uu[q], vi[q], wi[q], vu1[q], t + 32, sssp1, cc1, c1[q]);
+            chg0 += x0;
+            chg1 += x1;
+            const unsigned long long bits = ballot64(x0, x1);
+            if (bits && t == ii[q] && op.mark) bit_set(op.mark, vi[q]);
+            if (bits && t == ii[q] && g.slots[vi[q]])
+              want = atomicOr(&m_out[vi[q]], bits) == 0ull;
+          }
         }
         frontier_append(out, want, v, want ? g.slots[v] : 0u);
       }
@@ -327,7 +376,7 @@ __global__ void k_wide_dense(GraphView g, const uint32_t *val, unsigned long lon
 __global__ void k_wide_seed_deleted(GraphView g, unsigned long long *st, uint32_t *val,
                                     unsigned long long lanes, unsigned long long cc,
                                     const uint64_t *keys, uint32_t n, unsigned long long *inval,
-                                    unsigned long long *m_out, FrontierView out) {
+                                    uint32_t *mark, unsigned long long *m_out, FrontierView out) {
   const int t = threadIdx.x & 31;
   const bool l0 = lanes >> t & 1ull, l1 = lanes >> (t + 32) & 1ull;
   const bool c0 = cc >> t & 1ull, c1 = cc >> (t + 32) & 1ull;
@@ -349,6 +398,7 @@ __global__ void k_wide_seed_deleted(GraphView g, unsigned long long *st, uint32_
       r0 += x0;
       r1 += x1;
       const unsigned long long bits = ballot64(x0, x1);
+      if (bits && t == i) bit_set(mark, v);
       if (bits && t == i && g.slots[v]) want = atomicOr(&m_out[v], bits) == 0ull;
     }
     const uint32_t v = (uint32_t)key;
@@ -370,7 +420,7 @@ __global__ void k_wide_relax_inserted(GraphView g, unsigned long long *st, uint3
   const bool l0 = lanes >> t & 1ull, l1 = lanes >> (t + 32) & 1ull;
   const bool s0 = algo.sssp >> t & 1ull, s1 = algo.sssp >> (t + 32) & 1ull;
   const bool c0 = algo.cc >> t & 1ull, c1 = algo.cc >> (t + 32) & 1ull;
-  WideRelaxOp op{st, val, algo};
+  WideRelaxOp<> op{st, val, algo};
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   uint32_t counted = 0;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < n; b += stride) {
