@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="snapshot", choices=["snapshot", "ppr", "batched"],
+    ap.add_argument("--workload", default="snapshot", choices=["snapshot", "ppr", "batched", "served"],
                     help="snapshot: incremental SSSP/BFS/CC (the headline); ppr: weighted "
                          "personalized PageRank forward + adjoint; batched: 256 BFS + 256 SSSP "
                          "queries kept up to date together")
@@ -66,6 +66,11 @@ def parse():
     ap.add_argument("--batched-sssp", type=int, default=256)
     ap.add_argument("--batched-updates", type=int, default=100_000)
     ap.add_argument("--group-size", type=int, default=64)
+    ap.add_argument("--served-scale", type=int, default=26)
+    ap.add_argument("--served-seconds", type=float, default=30.0)
+    ap.add_argument("--served-rate", type=float, default=6.0, help="requests per second (Poisson)")
+    ap.add_argument("--served-budget-gb", type=float, default=16.0)
+    ap.add_argument("--slots", type=int, default=16)
     ap.add_argument("--plain-sample", type=int, default=32,
                     help="batched workload: queries of the sample run one per edge pass")
     ap.add_argument("--ppr-scale", type=int, default=22)
@@ -570,6 +575,136 @@ def batched_arm(a, R):
     return out
 
 
+# ----------------------------------------------------------------- served arm
+SERVED_METRIC = ("GTEPS served (R-MAT s{scale}, {budget} GB HBM budget, Poisson {rate}/s: update "
+                 "batches log-uniform 1k-1M and PR/BFS/SSSP queries)")
+
+
+def served_trace(nv, row, col, a):
+    """Poisson arrivals over --served-seconds: half update batches (size
+    log-uniform in [1k, 1M], half inserts of new edges, half deletes of
+    existing ones, from the seeded stream generator), half one-shot queries
+    (2 % PR, 49 % BFS, 49 % SSSP) from uniform random sources.  A PageRank
+    from scratch at scale 26 needs about 200 full passes to guarantee
+    L-inf <= 1e-6, several seconds, hence the small share."""
+    import sgs
+
+    rng = np.random.default_rng(a.seed + 26)
+    t, arrivals = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / a.served_rate)
+        if t > a.served_seconds:
+            break
+        arrivals.append(t)
+    kinds = rng.random(len(arrivals)) < 0.5
+    sizes = np.exp(rng.uniform(np.log(1e3), np.log(1e6), len(arrivals))).astype(np.int64)
+    n_upd = int(kinds.sum())
+    half = [int(x) // 2 for x in sizes[kinds]]
+    tot = int(sum(half))
+    i_s, i_d, d_s, d_d = sgs.gen_update_stream(nv, row, col, a.seed * 7919, tot, tot)
+    i_w = sgs.hash_weights(a.seed, i_s, i_d)
+    reqs, off, u = [], 0, 0
+    for k, t in enumerate(arrivals):
+        if kinds[k]:
+            h = half[u]
+            sl = slice(off, off + h)
+            off += h
+            u += 1
+            reqs.append({"kind": "update", "arrival_s": t, "ins_src": i_s[sl], "ins_dst": i_d[sl],
+                         "ins_w": i_w[sl], "del_src": d_s[sl], "del_dst": d_d[sl]})
+        else:
+            x = rng.random()
+            algo = sgs.PR if x < 0.02 else sgs.BFS if x < 0.51 else sgs.SSSP
+            reqs.append({"kind": "query", "algo": algo, "source": int(rng.integers(0, nv)), "arrival_s": t})
+    return reqs, n_upd
+
+
+def served_arm(a, R):
+    """N2: a served loop (sgs_serve) on one GPU: requests arrive on the wall
+    clock, updates are applied in order, queries are admitted together up to
+    --slots per step.  value = edges traversed by all requests / busy time of
+    the loop (host wall clock, host->device copies of the batches and the
+    result reads included), with p50/p99 latency per request kind."""
+    import torch
+
+    import sgs
+
+    dev = torch.device("cuda", R.local)
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    e = sgs.Engine(device=R.local, weight_mode=sgs.W_EXPLICIT, hbm_budget_gb=a.served_budget_gb,
+                   group_size=4)
+    e.load_rmat(a.served_scale, a.edge_factor, a.seed, 0.57, 0.19, 0.19, wseed=a.seed)
+    st0 = e.engine_stats()
+    nv = int(st0["nv"])
+    row, col, _ = e.export()
+    reqs, n_upd = served_trace(nv, row, col, a)
+    del row, col
+    t_gen = time.time() - t0
+    # warm-up: a few requests of each kind outside the trace
+    warm = [{"kind": "query", "algo": alg, "source": 1, "arrival_s": 0.0} for alg in (sgs.BFS, sgs.SSSP, sgs.PR)]
+    e.serve(warm, slots=a.slots, realtime=False)
+    clocks = Clocks(R.local)
+    R.barrier()
+    torch.cuda.synchronize()
+    l0 = e.engine_stats()["kernel_launches"]
+    clocks.start()
+    w0 = time.perf_counter()
+    res = e.serve(reqs, slots=a.slots, realtime=True)
+    wall = time.perf_counter() - w0
+    clk = clocks.stop()
+    launches = int(e.engine_stats()["kernel_launches"] - l0)
+    st = e.engine_stats()
+    e.close()
+    ok = [c["status"] == 0 for c in res]
+    # busy time: union of the steps' [start, done] intervals
+    steps = sorted({(c["start_s"], c["done_s"]) for c in res})
+    busy, last = 0.0, -1.0
+    for s0, s1 in steps:
+        s0 = max(s0, last)
+        if s1 > s0:
+            busy += s1 - s0
+        last = max(last, s1)
+    edges = sum(c["edges"] for c in res)
+
+    def pct(kind, algo=None):
+        lat = [c["latency_s"] * 1e3 for c, r in zip(res, reqs)
+               if r["kind"] == kind and (algo is None or r.get("algo") == algo)]
+        if not lat:
+            return None
+        return {"n": len(lat), "p50_ms": round(float(np.percentile(lat, 50)), 2),
+                "p99_ms": round(float(np.percentile(lat, 99)), 2), "max_ms": round(max(lat), 2)}
+
+    qb = [c["batch"] for c, r in zip(res, reqs) if r["kind"] == "query"]
+    value = edges / busy / 1e9 if busy > 0 else 0.0
+    h2d = sum((len(r["ins_src"]) * 3 + len(r["del_src"]) * 2) * 4 for r in reqs if r["kind"] == "update")
+    out = {
+        "metric": SERVED_METRIC.format(scale=a.served_scale, budget=a.served_budget_gb, rate=a.served_rate),
+        "value": round(R.sum(value), 3), "unit": UNIT, "n_gpus": R.world, "steps": len(reqs),
+        "warmup": len(warm), "ms_per_step": round(busy * 1e3 / max(len(reqs), 1), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (device R-MAT, seeded update stream, Poisson arrivals)",
+        "config": {"workload": f"served loop, R-MAT scale {a.served_scale} ef {a.edge_factor} seed {a.seed}, "
+                               f"HBM budget {a.served_budget_gb} GB, {a.served_seconds} s of Poisson "
+                               f"arrivals at {a.served_rate}/s, slots {a.slots}, group_size 4",
+                   "nv": nv, "ne_initial": int(st0["ne"]), "ne_final": int(st["ne"]),
+                   "hbm_resident_fraction": st["hbm_resident_vertices"] / max(nv, 1),
+                   "requests": len(reqs), "updates": n_upd, "queries": len(reqs) - n_upd,
+                   "parallelism": "replicas" if R.world > 1 else "single GPU"},
+        "latency": {"update": pct("update"), "query": pct("query"), "bfs": pct("query", sgs.BFS),
+                    "sssp": pct("query", sgs.SSSP), "pr": pct("query", sgs.PR)},
+        "query_batch": {"mean": round(float(np.mean(qb)), 2) if qb else 0, "max": int(max(qb)) if qb else 0},
+        "failed": int(len(res) - sum(ok)),
+        "busy_s": round(busy, 3), "wall_s": round(wall, 3), "utilisation": round(busy / wall, 3),
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d / max(len(reqs), 1)),
+                "d2h_bytes_per_step": 32, "note": "the served loop is end to end: host batches in, "
+                                                  "summaries out, wall clock"},
+        "gpu_launches": launches, "clocks": clk, "gen_s": round(t_gen, 2),
+        "roofline": None,
+    }
+    return out
+
+
 # ----------------------------------------------------------------- PPR adjoint arm
 PPR_METRIC = ("PPR forward+adjoint relaxations/s (weighted personalized PageRank, R-MAT s{scale}, "
               "{K} vectors x {seeds} seeds, loss on {targets} targets)")
@@ -806,7 +941,11 @@ def main():
     a = parse()
     R = Ranks()
     try:
-        if a.impl == "reference" and a.workload == "ppr":
+        if a.impl == "reference" and a.workload == "served":
+            out = None if R.rank else {
+                "impl": "reference", "unavailable": "the reference has no request loop (its drivers "
+                "run one source through a fixed snapshot list)"}
+        elif a.impl == "reference" and a.workload == "ppr":
             out = None if R.rank else {
                 "impl": "reference", "unavailable": "the reference has no personalized PageRank "
                 "or adjoint (its PageRank is the single unweighted vector of the snapshot workload)"}
@@ -818,6 +957,8 @@ def main():
             out = ppr_arm(a, R)
         elif a.workload == "batched":
             out = batched_arm(a, R)
+        elif a.workload == "served":
+            out = served_arm(a, R)
         else:
             out = engine_arm(a, R)
         if R.rank == 0 and out is not None:

@@ -831,8 +831,26 @@ struct sgs_engine {
         if (!G) {
           auto ng = std::make_unique<Group>();
           ng->width = wide ? WLANES : GMAX;
-          ng->st.ensure((size_t)nv * ng->width);
-          ng->val.ensure((size_t)nv * ng->width);
+          for (int attempt = 0;; ++attempt) {
+            try {
+              ng->st.ensure((size_t)nv * ng->width);
+              ng->val.ensure((size_t)nv * ng->width);
+              break;
+            } catch (const SgsError &f) {
+              // out of memory: drop pooled empty groups (not pending here) once
+              bool freed = false;
+              if (f.code == SGS_ERR_OOM && attempt == 0)
+                for (size_t j = groups.size(); j-- > 0;) {
+                  bool pend = false;
+                  for (auto &t : touched) pend |= t.first == groups[j].get();
+                  if (groups[j]->used == 0 && !pend) {
+                    groups.erase(groups.begin() + j);
+                    freed = true;
+                  }
+                }
+              if (!freed) throw;
+            }
+          }
           G = ng.get();
           groups.push_back(std::move(ng));
         }
@@ -863,6 +881,17 @@ struct sgs_engine {
     }
   }
 
+  // Frees the state of groups without lanes in use; true if any was freed.
+  bool release_empty_groups() {
+    bool any = false;
+    for (size_t j = groups.size(); j-- > 0;)
+      if (groups[j]->used == 0) {
+        groups.erase(groups.begin() + j);
+        any = true;
+      }
+    return any;
+  }
+
   void remove_query(int qid) {
     for (size_t i = 0; i < queries.size(); ++i)
       if (queries[i]->id == qid) {
@@ -870,12 +899,9 @@ struct sgs_engine {
         Query &q = *queries[i];
         if (q.grp) q.grp->used &= ~(1ull << q.lane);
         queries.erase(queries.begin() + i);
-        for (size_t j = 0; j < groups.size(); ++j)
-          if (groups[j]->used == 0) {
-            bool ref = false;
-            for (auto &o : queries) ref |= o->grp == groups[j].get();
-            if (!ref) { groups.erase(groups.begin() + j); break; }
-          }
+        // an empty group keeps its state arrays for the next queries (a
+        // serving loop admits and retires queries all the time); they are
+        // released when an allocation would fail (release_empty_groups)
         return;
       }
     fail(SGS_ERR_INVALID, "unknown query id");
@@ -1134,6 +1160,9 @@ struct sgs_engine {
     CK(cudaEventElapsedTime(&bms, ev_batch.a, ev_batch.b));
     est.last_apply_ms = ams;
     est.last_batch_ms = bms;
+    uint64_t edges = 0;
+    for (auto &q : queries) edges += q->stats.edges_traversed;
+    est.last_batch_edges = edges;
   }
 
   // Union of the distinct sources of the sorted deletes and kept inserts, with

@@ -50,7 +50,7 @@ EXPORTS = [
     "sgs_read_edge_list", "sgs_read_stream_sizes", "sgs_read_update_file", "sgs_free",
     "sgs_ppr_create_csr", "sgs_ppr_create", "sgs_ppr_destroy", "sgs_ppr_info",
     "sgs_ppr_export", "sgs_ppr_forward", "sgs_ppr_backward", "sgs_ppr_timing",
-    "sgs_ppr_get_stats",
+    "sgs_ppr_get_stats", "sgs_serve",
 ]
 
 K_GROUP, K_GROUP_INVAL, K_PR_PUSH, K_WIDE, K_WIDE_INVAL = range(5)
@@ -112,6 +112,7 @@ class EngineStats(C.Structure):
         ("last_apply_ms", C.c_double),
         ("last_batch_ms", C.c_double),
         ("kernel_launches", C.c_uint64),
+        ("last_batch_edges", C.c_uint64),
     ]
 
     def as_dict(self):
@@ -133,6 +134,27 @@ class KernelStats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+REQ_QUERY, REQ_UPDATE = 0, 1
+
+
+class Request(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int), ("algo", C.c_int), ("source", C.c_uint32), ("reserved", C.c_uint32),
+        ("arrival_s", C.c_double), ("value_out", C.c_void_p), ("parent_out", C.c_void_p),
+        ("ins_src", C.c_void_p), ("ins_dst", C.c_void_p), ("ins_w", C.c_void_p),
+        ("del_src", C.c_void_p), ("del_dst", C.c_void_p),
+        ("n_ins", C.c_uint64), ("n_del", C.c_uint64),
+    ]
+
+
+class Completion(C.Structure):
+    _fields_ = [
+        ("status", C.c_int), ("batch", C.c_uint32), ("version", C.c_uint64),
+        ("start_s", C.c_double), ("done_s", C.c_double),
+        ("summary", C.c_uint64 * 4), ("edges", C.c_uint64),
+    ]
 
 
 class PprStats(C.Structure):
@@ -202,6 +224,7 @@ def lib():
     L.sgs_ppr_forward.argtypes = [vp, vp, vp, u32, dbl, dbl, u32, vp, C.POINTER(i32), i32]
     L.sgs_ppr_backward.argtypes = [vp, vp, vp, vp, u32, dbl, dbl, u32, vp, vp, C.POINTER(i32), i32]
     L.sgs_ppr_timing.argtypes = [vp, i32]
+    L.sgs_serve.argtypes = [vp, C.POINTER(Request), u32, u32, i32, C.POINTER(Completion)]
     L.sgs_ppr_get_stats.argtypes = [vp, C.POINTER(PprStats)]
     for name in EXPORTS:
         if name not in ("sgs_version", "sgs_last_error", "sgs_config_default",
@@ -389,6 +412,50 @@ class Engine:
             self._queries[q.qid] = q
             out.append(q)
         return out
+
+    def serve(self, requests, slots=0, realtime=True):
+        """Runs sgs_serve over a trace.  requests: dicts with kind "query"
+        (algo, source, arrival_s, optional value_out / parent_out numpy
+        buffers) or "update" (ins_src, ins_dst, ins_w, del_src, del_dst,
+        arrival_s).  Returns one dict per request."""
+        n = len(requests)
+        arr = (Request * max(n, 1))()
+        keep = []
+        for i, r in enumerate(requests):
+            q = arr[i]
+            q.arrival_s = float(r.get("arrival_s", 0.0))
+            if r["kind"] == "query":
+                q.kind = REQ_QUERY
+                a = r["algo"]
+                q.algo = ALGOS[a] if isinstance(a, str) else int(a)
+                q.source = int(r.get("source", 0))
+                for f in ("value_out", "parent_out"):
+                    b = r.get(f)
+                    if b is not None:
+                        keep.append(b)
+                        setattr(q, f, b.ctypes.data)
+            else:
+                q.kind = REQ_UPDATE
+                for f in ("ins_src", "ins_dst", "ins_w", "del_src", "del_dst"):
+                    b = r.get(f)
+                    if b is not None:
+                        b = _u32(b)
+                        keep.append(b)
+                        setattr(q, f, b.ctypes.data)
+                q.n_ins = len(r.get("ins_src", ()))
+                q.n_del = len(r.get("del_src", ()))
+        out = (Completion * max(n, 1))()
+        _check(lib().sgs_serve(self.h, arr, n, slots, int(realtime), out))
+        res = []
+        for i in range(n):
+            c = out[i]
+            res.append({"status": c.status, "batch": c.batch, "version": c.version,
+                        "start_s": c.start_s, "done_s": c.done_s,
+                        # closed loop (not realtime): every request counts as
+                        # arrived at the start
+                        "latency_s": c.done_s - (arr[i].arrival_s if realtime else 0.0),
+                        "summary": list(c.summary), "edges": c.edges})
+        return res
 
     def remove_query(self, q):
         _check(lib().sgs_query_remove(self.h, q.qid if isinstance(q, Query) else q))

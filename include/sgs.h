@@ -123,6 +123,8 @@ typedef struct sgs_engine_stats {
   double last_batch_ms;       /* device time of the whole last snapshot    */
   uint64_t kernel_launches;   /* the engine's own kernel launches so far
                                  (CUB sorts and scans not counted)         */
+  uint64_t last_batch_edges;  /* edges traversed by all queries in the last
+                                 snapshot (sum of their edges_traversed)   */
 } sgs_engine_stats;
 
 /* Per-kernel-class timing of the relaxation launches (CUDA events on the
@@ -268,6 +270,49 @@ SGS_API int sgs_sssp_csr_noalloc(uint32_t nv, const uint64_t *row,
                                  uint32_t source, uint32_t *dist,
                                  uint32_t *parent, void *stream);
 SGS_API int sgs_get_kernel_stats(sgs_engine *e, int kind, sgs_kernel_stats *out);
+
+/* Served request loop (no counterpart in the reference, whose drivers run
+ * one source through a fixed snapshot list).  A trace of requests, each with
+ * an arrival time in seconds, is served in arrival order on the calling
+ * thread: an update batch is one snapshot applied alone (every query sees
+ * exactly the updates that arrived before it: its `version`); consecutive
+ * queries at the head of the queue are admitted together, up to `slots`
+ * per step (size it from the HBM left after the graph; 0 = no limit), with
+ * sgs_query_add_many, their results read back (summary, and the value /
+ * parent vectors when buffers are given) and the queries retired.  With
+ * `realtime` the loop waits for arrival times on the wall clock (latency =
+ * done_s - arrival_s, queueing included); otherwise every request is taken
+ * at once, in arrival order (a closed loop: latency = done_s).  out[i]
+ * describes req[i]; times are host wall-clock seconds from the start of the
+ * call.  Requests that fail carry their status;
+ * the call itself fails only for malformed arguments. */
+#define SGS_REQ_QUERY 0
+#define SGS_REQ_UPDATE 1
+typedef struct sgs_request {
+  int kind;                 /* SGS_REQ_QUERY or SGS_REQ_UPDATE               */
+  int algo;                 /* query: SGS_BFS / SGS_SSSP / SGS_CC / SGS_PR   */
+  uint32_t source;          /* query source                                  */
+  uint32_t reserved;
+  double arrival_s;         /* >= 0                                          */
+  void *value_out;          /* query, optional host buffer: nv u32, PR: nv
+                               double                                        */
+  uint32_t *parent_out;     /* query, optional host buffer: nv u32           */
+  const uint32_t *ins_src, *ins_dst, *ins_w;  /* update: host arrays        */
+  const uint32_t *del_src, *del_dst;
+  uint64_t n_ins, n_del;
+} sgs_request;
+typedef struct sgs_completion {
+  int status;               /* SGS_OK or this request's error                */
+  uint32_t batch;           /* queries admitted in the same step (1 for an
+                               update)                                       */
+  uint64_t version;         /* updates applied before the query ran; for an
+                               update, its own position in the sequence     */
+  double start_s, done_s;   /* seconds from the start of the call            */
+  uint64_t summary[4];      /* query: as sgs_query_summary                   */
+  uint64_t edges;           /* edges traversed for this request              */
+} sgs_completion;
+SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n,
+                      uint32_t slots, int realtime, sgs_completion *out);
 
 /* Differentiable weighted personalized PageRank (FP64).  Generalises the
  * reference's PageRank fixed point (samples/hybrid_pr/hybrid_pr.cu:26-151,

@@ -1,0 +1,158 @@
+"""Served request loop (sgs_serve): update batches and one-shot queries with
+Poisson arrivals, continuous batching of the queries.
+
+Each query's result must be that of its graph version (the updates that
+arrived before it): values bit-exact against the CPU oracle on that
+snapshot (PageRank within 1e-6), parents valid, and identical to the same
+query run alone on the same snapshot.  Slot admission, ordering and a failed
+update in the middle of the trace are checked too."""
+import numpy as np
+import pytest
+
+import oracle as O
+import sgs
+from test_gpu_parity import Mirror, check_query
+
+pytestmark = pytest.mark.gpu
+
+
+class Res:
+    """A query result as check_query expects it (value/parent vectors)."""
+
+    def __init__(self, algo, source, value, parent):
+        self.algo, self.source, self._v, self._p = algo, source, value, parent
+
+    def value(self):
+        return self._v
+
+    def parent(self):
+        return self._p
+
+    def stats(self):
+        return {"converged": 1}
+
+
+def _trace(nv, row, col, seed, n_upd=10, n_q=26, mean_gap=0.002, bad_update=None):
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(10), np.log(1500), n_upd)).astype(int)
+    tot = int(sizes.sum())
+    i_s, i_d, d_s, d_d = O.gen_updates(nv, row, col, seed + 1, tot, tot)
+    iw = np.array([O.weight_of(3, u, v) for u, v in zip(i_s, i_d)], np.uint32)
+    kinds = ["update"] * n_upd + ["query"] * n_q
+    rng.shuffle(kinds)
+    t = np.cumsum(rng.exponential(mean_gap, len(kinds)))
+    reqs, batches, off, u = [], [], 0, 0
+    algos = [sgs.BFS, sgs.SSSP, sgs.CC, sgs.PR]
+    for k, kind in enumerate(kinds):
+        if kind == "update":
+            n = sizes[u]
+            sl = slice(off, off + n)
+            off += n
+            b = (i_s[sl], i_d[sl], iw[sl], d_s[sl], d_d[sl])
+            if bad_update is not None and u == bad_update:
+                b = (np.array([nv + 5], np.uint32), np.array([0], np.uint32),
+                     np.array([1], np.uint32), d_s[:0], d_d[:0])
+            batches.append(b)
+            reqs.append({"kind": "update", "arrival_s": float(t[k]), "ins_src": b[0], "ins_dst": b[1],
+                         "ins_w": b[2], "del_src": b[3], "del_dst": b[4]})
+            u += 1
+        else:
+            a = algos[rng.integers(0, 4)]
+            vo = np.empty(nv, np.float64 if a == sgs.PR else np.uint32)
+            po = np.empty(nv, np.uint32)
+            reqs.append({"kind": "query", "algo": a, "source": int(rng.integers(0, nv)),
+                         "arrival_s": float(t[k]), "value_out": vo, "parent_out": po})
+    return reqs, batches
+
+
+def _snapshots(nv, row, col, w, batches, ok):
+    m = Mirror(nv, row, col, w)
+    snaps = [(m.row, m.col, m.w)]
+    for b, good in zip(batches, ok):
+        if good:  # versions count the updates that were applied
+            m.apply(*b)
+            snaps.append((m.row, m.col, m.w))
+    return snaps
+
+
+def _check_all(reqs, res, nv, snaps, slots):
+    upd_before = 0
+    order = np.argsort([r["arrival_s"] for r in reqs], kind="stable")
+    n_ok_upd = 0
+    for i in order:
+        r, c = reqs[i], res[i]
+        if r["kind"] == "update":
+            if c["status"] == 0:
+                n_ok_upd += 1
+                assert c["version"] == n_ok_upd
+            continue
+        assert c["status"] == 0
+        assert c["version"] == n_ok_upd  # saw exactly the updates that arrived before it
+        assert 1 <= c["batch"] and (slots == 0 or c["batch"] <= slots)
+        assert c["done_s"] >= c["start_s"] >= 0 and c["latency_s"] >= 0
+        row, col, w = snaps[c["version"]]
+        m = Mirror(nv, row, col, w)
+        check_query(Res(r["algo"], r["source"], r["value_out"], r["parent_out"]), m, sgs.W_EXPLICIT)
+
+
+@pytest.mark.parametrize("gs,slots,realtime", [(4, 0, True), (4, 3, False), (64, 5, True)])
+def test_served_results_match_their_snapshot(gs, slots, realtime):
+    nv, row, col = O.rmat_csr(12, 16, 3)
+    w = O.weights(nv, row, col, 3, 0)
+    reqs, batches = _trace(nv, row, col, 7 + gs + slots)
+    with sgs.Engine(group_size=gs) as e:
+        e.load_csr(nv, row, col, w)
+        res = e.serve(reqs, slots=slots, realtime=realtime)
+    snaps = _snapshots(nv, row, col, w, batches, [True] * len(batches))
+    _check_all(reqs, res, nv, snaps, slots)
+    if slots == 0 and realtime:
+        # some queries were batched together (continuous batching)
+        assert max(c["batch"] for c, r in zip(res, reqs) if r["kind"] == "query") >= 1
+
+
+def test_served_equals_alone():
+    """A query served in the mix gives exactly what it gives alone on the
+    same snapshot (integers bit-exact, PageRank within 1e-6)."""
+    nv, row, col = O.rmat_csr(11, 16, 5)
+    w = O.weights(nv, row, col, 3, 0)
+    reqs, batches = _trace(nv, row, col, 23, n_upd=6, n_q=16, mean_gap=0.0)
+    with sgs.Engine() as e:
+        e.load_csr(nv, row, col, w)
+        res = e.serve(reqs, slots=0, realtime=False)
+    qi = [i for i, r in enumerate(reqs) if r["kind"] == "query"][:8]
+    for i in qi:
+        r, c = reqs[i], res[i]
+        with sgs.Engine(group_size=1) as a:
+            a.load_csr(nv, row, col, w)
+            for b in batches[:c["version"]]:
+                a.apply_batch(*b)
+            q = a.add_query(r["algo"], r["source"])
+            v = q.value()
+        if r["algo"] == sgs.PR:
+            assert np.max(np.abs(v - r["value_out"])) <= 1e-6
+        else:
+            assert np.array_equal(v, r["value_out"])
+
+
+def test_failed_update_does_not_stop_the_loop():
+    nv, row, col = O.rmat_csr(11, 16, 8)
+    w = O.weights(nv, row, col, 3, 0)
+    reqs, batches = _trace(nv, row, col, 31, n_upd=5, n_q=10, mean_gap=0.0, bad_update=2)
+    with sgs.Engine() as e:
+        e.load_csr(nv, row, col, w)
+        res = e.serve(reqs, realtime=False)
+    st = [c["status"] for c, r in zip(res, reqs) if r["kind"] == "update"]
+    assert st[2] < 0
+    assert all(s == 0 for k, s in enumerate(st) if k != 2)
+    ok = [k != 2 for k in range(len(batches))]
+    snaps = _snapshots(nv, row, col, w, batches, ok)
+    _check_all(reqs, res, nv, snaps, 0)
+
+
+def test_serve_rejects_malformed_requests():
+    nv, row, col = O.rmat_csr(8, 8, 1)
+    with sgs.Engine() as e:
+        e.load_csr(nv, row, col, O.weights(nv, row, col, 1, 0))
+        with pytest.raises(sgs.SgsError):
+            e.serve([{"kind": "query", "algo": 0, "arrival_s": -1.0}])
+        assert e.serve([]) == []
