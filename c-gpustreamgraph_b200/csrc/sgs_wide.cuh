@@ -121,8 +121,10 @@ struct WideInvalidateOp {
 // the frontier's edge space (as seg_map / group_map); entries are staged in
 // shared memory, then each warp takes 32 consecutive slots per step.  Per
 // lane counts: the CTA that holds an entry's first slot adds live[v] for
-// every lane of its mask ((query, edge) pairs relaxed); lane_changes counts
-// the lanes changed (resets for the invalidation op).
+// every lane of its mask (the traversed-edge count of the frontier);
+// lane_changes counts the lanes changed (resets for the invalidation op);
+// edge_stat receives the (lane, edge) pairs actually evaluated -- fewer than
+// the traversed count when a restricted round skips destinations.
 template <class Op>
 __global__ void __launch_bounds__(RELAX_THREADS, 3)
     wide_map(GraphView g, FrontierView in, FrontierView out, Op op,
@@ -149,6 +151,9 @@ __global__ void __launch_bounds__(RELAX_THREADS, 3)
   const bool sssp0 = op.algo.sssp >> t & 1ull, sssp1 = op.algo.sssp >> (t + 32) & 1ull;
   const bool cc0 = op.algo.cc >> t & 1ull, cc1 = op.algo.cc >> (t + 32) & 1ull;
   unsigned long long acc0 = 0, acc1 = 0, chg0 = 0, chg1 = 0;
+  uint32_t evald = 0;  // (lane, edge) pairs evaluated by this thread's lanes
+  __shared__ unsigned long long s_eval;
+  if (threadIdx.x == 0) s_eval = 0;
   const uint64_t packed = __ldcg((const unsigned long long *)in.counter);
   const uint32_t n = (uint32_t)(packed >> CNT_SHIFT);
   const uint64_t T = packed & EDGE_MASK;
@@ -262,6 +267,7 @@ __global__ void __launch_bounds__(RELAX_THREADS, 3)
           }
 #pragma unroll
           for (int q = 0; q < D; ++q) {
+            evald += (uint32_t)a0[q] + (uint32_t)a1[q];
             const bool x0 = a0[q] && op.fin(uu[q], vi[q], wi[q], vu0[q], t, sssp0, cc0, c0[q]);
             const bool x1 = a1[q] && op.fin(uu[q], vi[q], wi[q], vu1[q], t + 32, sssp1, cc1, c1[q]);
             chg0 += x0;
@@ -284,15 +290,15 @@ __global__ void __launch_bounds__(RELAX_THREADS, 3)
   atomicAdd(&s_lane[t + 32], acc1);
   atomicAdd(&s_chg[t], chg0);
   atomicAdd(&s_chg[t + 32], chg1);
+  const unsigned long long ev = warp_sum((unsigned long long)evald);
+  if (t == 0 && ev) atomicAdd(&s_eval, ev);
   __syncthreads();
   if (threadIdx.x < WLANES) {
     const unsigned long long x = s_lane[threadIdx.x], c = s_chg[threadIdx.x];
-    if (x) {
-      if (lane_edges) atomicAdd(&lane_edges[threadIdx.x], x);
-      if (edge_stat) atomicAdd(edge_stat, x);
-    }
+    if (x && lane_edges) atomicAdd(&lane_edges[threadIdx.x], x);
     if (c && lane_changes) atomicAdd(&lane_changes[threadIdx.x], c);
   }
+  if (threadIdx.x == 0 && s_eval && edge_stat) atomicAdd(edge_stat, s_eval);
 }
 
 // ---------------------------------------------------------------------------
