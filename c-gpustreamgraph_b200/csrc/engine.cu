@@ -120,6 +120,10 @@ struct Group {
   uint64_t sssp = 0, cc = 0;    // lanes per algorithm (both widths)
   uint64_t inval[WLANES] = {};  // resets per lane in the last deletion phase
   DBuf<uint32_t> ibits;         // bitmap of vertices reset in the last deletion phase
+  // per-lane device counters of the last snapshot: [0,64) resets, [64,128)
+  // edges of the invalidation, [128,192) edges of the repair; read once at
+  // the end of the snapshot
+  DBuf<unsigned long long> dstat;
   bool wide() const { return width == WLANES; }
   LaneAlgo algo() const { return LaneAlgo{algo_packed}; }
   WideAlgo walgo() const { return WideAlgo{sssp, cc}; }
@@ -221,6 +225,8 @@ struct sgs_engine {
   // per-kernel-class timing
   bool ktiming = false;
   std::vector<cudaEvent_t> kev;  // 2 per queued launch
+  std::vector<cudaEvent_t> gev;  // 4 per group per snapshot
+  std::vector<unsigned long long> h_gstat;
   sgs_kernel_stats kst[SGS_K_COUNT]{};
   uint64_t n_launch = 0;  // this engine's own kernel launches (library sorts/scans excluded)
 
@@ -232,6 +238,7 @@ struct sgs_engine {
 
   ~sgs_engine() {
     for (auto ev : kev) cudaEventDestroy(ev);
+    for (auto ev : gev) cudaEventDestroy(ev);
     if (h_cnt) cudaFreeHost(h_cnt);
     if (s) cudaStreamDestroy(s);
   }
@@ -466,6 +473,13 @@ struct sgs_engine {
   // Runs relaxation rounds from the frontier in buffer 0 / cnt[0] until a
   // round produces an empty frontier.  Rounds are queued in batches; the
   // host reads the batch's counters once.
+  void ensure_gev(size_t n) {
+    while (gev.size() < n) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      gev.push_back(e);
+    }
+  }
   void ensure_kev(size_t n) {
     while (kev.size() < n) {
       cudaEvent_t ev;
@@ -547,13 +561,12 @@ struct sgs_engine {
   template <class Launch>
   uint32_t run_rounds(Launch launch, bool wide, bool &converged, int kind, double per_slot,
                       const char *round0, const std::function<void()> *after0 = nullptr) {
+    // no host read before the first batch: an empty start costs a few
+    // launches that exit at once, a host round trip costs more
     const uint32_t maxr = cfg.max_rounds;
-    uint32_t r = 0, rb = 2;
+    uint32_t r = 0, rb = 4;
     converged = false;
     CK(cudaMemsetAsync(rstat.p, 0, sizeof(unsigned long long) * (maxr + 2), s));
-    CK(cudaMemcpyAsync(h_cnt, cnt.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    sync();
-    if (h_cnt[0] == 0) { converged = true; return 0; }
     std::vector<unsigned long long> hr(18);
     while (r < maxr) {
       const uint32_t nb = std::min(rb, maxr - r);
@@ -685,26 +698,6 @@ struct sgs_engine {
     for (auto &q : queries)
       if (q->id == qid) return *q;
     fail(SGS_ERR_INVALID, "unknown query id");
-  }
-
-  // Per-lane stats of every query of a group after a group phase.
-  void lane_stats(Group &G, uint32_t rounds, bool conv, float ms, const uint64_t *extra_edges,
-                  const uint64_t *inval) {
-    unsigned long long le[WLANES];
-    CK(cudaMemcpyAsync(le, b_lane.p, sizeof(unsigned long long) * G.width, cudaMemcpyDeviceToHost, s));
-    sync();
-    for (auto &q : queries) {
-      if (q->grp != &G) continue;
-      const int l = q->lane;
-      const uint64_t e = le[l] + (extra_edges ? extra_edges[l] : 0);
-      q->stats.edges_traversed = e;
-      q->stats.edges_total += e;
-      q->stats.rounds = rounds;
-      q->stats.converged = conv ? 1 : 0;
-      q->stats.ms = ms;
-      q->stats.pr_residual_l1 = 0;
-      q->stats.invalidated = inval ? inval[l] : 0;
-    }
   }
 
   void start_pr(Query &q) {
@@ -980,11 +973,16 @@ struct sgs_engine {
     bool any_pr = false;
     for (auto &q : queries) any_pr |= q->algo == SGS_PR;
     const size_t ng = groups.size();
-    std::vector<float> gms(ng, 0.f);
-    std::vector<std::array<uint64_t, WLANES>> gedges(ng), ginval(ng);
+    // per group: events around its invalidation [4i, 4i+1] and repair
+    // [4i+2, 4i+3]; counters in G.dstat; all read after the last sync
+    ensure_gev(4 * ng);
+    std::vector<uint32_t> grounds(ng, 0);
+    std::vector<char> gdel(ng, 0);
     for (size_t i = 0; i < ng; ++i) {
-      gedges[i].fill(0);
-      ginval[i].fill(0);
+      Group &G = *groups[i];
+      if (!G.used) continue;
+      G.dstat.ensure(3 * WLANES);
+      CK(cudaMemsetAsync(G.dstat.p, 0, sizeof(unsigned long long) * 3 * WLANES, s));
     }
 
     // ---- PR cancel over the old out-lists of touched sources
@@ -1004,7 +1002,8 @@ struct sgs_engine {
       Range rg("sgs:invalidate");
       Group &G = *groups[i];
       if (!G.used) continue;
-      CK(cudaEventRecord(ev_q.a, s));
+      gdel[i] = 1;
+      CK(cudaEventRecord(gev[4 * i], s));
       CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * WLANES, s));
       CK(cudaMemsetAsync(b_inval.p, 0, sizeof(unsigned long long) * WLANES, s));
       reset_counters(0);
@@ -1034,19 +1033,11 @@ struct sgs_engine {
             conv, SGS_K_GROUP_INVAL, 4.0);
       }
       if (!conv) fail(SGS_ERR_NOCONV, "invalidation did not converge");
-      CK(cudaEventRecord(ev_q.b, s));
-      unsigned long long hv[WLANES], he[WLANES];
-      CK(cudaMemcpyAsync(hv, b_inval.p, sizeof(unsigned long long) * G.width, cudaMemcpyDeviceToHost, s));
-      CK(cudaMemcpyAsync(he, b_lane.p, sizeof(unsigned long long) * G.width, cudaMemcpyDeviceToHost, s));
-      sync();
-      float ms = 0;
-      CK(cudaEventElapsedTime(&ms, ev_q.a, ev_q.b));
-      gms[i] += ms;
-      for (int q = 0; q < G.width; ++q) {
-        ginval[i][q] = hv[q];
-        gedges[i][q] = he[q];
-        G.inval[q] = hv[q];
-      }
+      CK(cudaEventRecord(gev[4 * i + 1], s));
+      CK(cudaMemcpyAsync(G.dstat.p, b_inval.p, sizeof(unsigned long long) * WLANES,
+                         cudaMemcpyDeviceToDevice, s));
+      CK(cudaMemcpyAsync(G.dstat.p + WLANES, b_lane.p, sizeof(unsigned long long) * WLANES,
+                         cudaMemcpyDeviceToDevice, s));
     }
 
     // ---- graph update
@@ -1108,53 +1099,72 @@ struct sgs_engine {
       Group &G = *groups[i];
       if (!G.used) continue;
       Range rg("sgs:repair");
-      bool any_inval = false;
-      for (int q = 0; q < G.width; ++q) any_inval |= (G.used >> q & 1ull) && ginval[i][q] > 0;
-      CK(cudaEventRecord(ev_q.a, s));
+      CK(cudaEventRecord(gev[4 * i + 2], s));
       CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * WLANES, s));
       reset_counters(0);
-      if (G.wide()) {
-        if (any_inval)
-          { ++n_launch; k_wide_dense<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(g, G.val.p, G.used, G.cc, wm[0].p,
-                                                                 fview(0, cnt.p)); }
-        else if (ni)
-          { ++n_launch; k_wide_relax_inserted<<<grid_elem(ni), 256, 0, s>>>(
-              g, G.st.p, G.val.p, G.used, G.walgo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr,
-              b_nkept.p, wm[0].p, fview(0, cnt.p), b_lane.p); }
-      } else if (any_inval) {
+      if (G.wide() && !gdel[i]) {  // no deletion phase ran: an empty reset bitmap
+        const size_t nw = (size_t)nv / 32 + 1;
+        G.ibits.ensure(nw);
+        CK(cudaMemsetAsync(G.ibits.p, 0, sizeof(uint32_t) * nw, s));
+      }
+      // the path is chosen on the device from the group's reset counts
+      // (G.dstat[0, 64)): the dense frontier only if a lane was reset
+      const unsigned long long *resets = G.dstat.p;
+      if (G.wide())
+        { ++n_launch; k_wide_dense<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(g, G.val.p, G.used, G.cc, wm[0].p,
+                                                               fview(0, cnt.p), resets); }
+      else
         { ++n_launch; k_group_dense<GMAX><<<grid_elem(nv), 256, 0, s>>>(g, G.val.p, (uint32_t)G.used, G.algo(),
-                                                            gm[0].p, fview(0, cnt.p)); }
-      } else if (ni) {
+                                                            gm[0].p, fview(0, cnt.p), resets); }
+      if (ni && !G.wide())  // narrow, nothing reset: only the inserted edges
         { ++n_launch; k_group_relax_inserted<GMAX><<<grid_elem(ni), 256, 0, s>>>(
             g, G.st.p, G.val.p, (uint32_t)G.used, G.algo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr,
-            b_nkept.p, gm[0].p, fview(0, cnt.p), b_lane.p); }
-      }
+            b_nkept.p, gm[0].p, fview(0, cnt.p), b_lane.p, resets); }
       CK(cudaGetLastError());
-      // inserted edges after the restricted round 0, into its output frontier
+      // wide: the inserted edges after the restricted round 0, into its
+      // output frontier (round 0 is empty when nothing was reset)
       const std::function<void()> ins_after0 = [&] {
-        if (G.wide())
-          { ++n_launch; k_wide_relax_inserted<<<grid_elem(ni), 256, 0, s>>>(
-              g, G.st.p, G.val.p, G.used, G.walgo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr,
-              b_nkept.p, wm[1].p, fview(1, cnt.p + 1), b_lane.p); }
-        else
-          { ++n_launch; k_group_relax_inserted<GMAX><<<grid_elem(ni), 256, 0, s>>>(
-              g, G.st.p, G.val.p, (uint32_t)G.used, G.algo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr,
-              b_nkept.p, gm[1].p, fview(1, cnt.p + 1), b_lane.p); }
+        { ++n_launch; k_wide_relax_inserted<<<grid_elem(ni), 256, 0, s>>>(
+            g, G.st.p, G.val.p, G.used, G.walgo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr,
+            b_nkept.p, wm[1].p, fview(1, cnt.p + 1), b_lane.p); }
       };
       bool conv = false;
-      const uint32_t rounds =
-          any_inval && G.wide() ? group_relax(G, conv, "sgs:sweep", G.ibits.p, ni ? &ins_after0 : nullptr)
-          : any_inval           ? group_relax(G, conv, "sgs:sweep")
-                                : group_relax(G, conv);
-      CK(cudaEventRecord(ev_q.b, s));
-      sync();
-      float ms = 0;
-      CK(cudaEventElapsedTime(&ms, ev_q.a, ev_q.b));
-      lane_stats(G, rounds, conv, gms[i] + ms, gedges[i].data(), ginval[i].data());
+      grounds[i] = G.wide() ? group_relax(G, conv, "sgs:sweep", G.ibits.p, ni ? &ins_after0 : nullptr)
+                            : group_relax(G, conv, "sgs:sweep");
       if (!conv) fail(SGS_ERR_NOCONV, "round limit reached before convergence");
+      CK(cudaEventRecord(gev[4 * i + 3], s));
+      CK(cudaMemcpyAsync(G.dstat.p + 2 * WLANES, b_lane.p, sizeof(unsigned long long) * WLANES,
+                         cudaMemcpyDeviceToDevice, s));
     }
+    // per-lane counters of every group, one read
+    h_gstat.resize(3 * WLANES * std::max<size_t>(ng, 1));
+    for (size_t i = 0; i < ng; ++i)
+      if (groups[i]->used)
+        CK(cudaMemcpyAsync(h_gstat.data() + 3 * WLANES * i, groups[i]->dstat.p,
+                           sizeof(unsigned long long) * 3 * WLANES, cudaMemcpyDeviceToHost, s));
     CK(cudaEventRecord(ev_batch.b, s));
     sync();
+    for (size_t i = 0; i < ng; ++i) {
+      Group &G = *groups[i];
+      if (!G.used) continue;
+      const unsigned long long *h = h_gstat.data() + 3 * WLANES * i;
+      float ms = 0, m2 = 0;
+      if (gdel[i]) CK(cudaEventElapsedTime(&ms, gev[4 * i], gev[4 * i + 1]));
+      CK(cudaEventElapsedTime(&m2, gev[4 * i + 2], gev[4 * i + 3]));
+      for (int q = 0; q < G.width; ++q) G.inval[q] = h[q];
+      for (auto &qp : queries) {
+        if (qp->grp != &G) continue;
+        const int l = qp->lane;
+        const uint64_t e = h[WLANES + l] + h[2 * WLANES + l];
+        qp->stats.edges_traversed = e;
+        qp->stats.edges_total += e;
+        qp->stats.rounds = grounds[i];
+        qp->stats.converged = 1;
+        qp->stats.ms = ms + m2;
+        qp->stats.pr_residual_l1 = 0;
+        qp->stats.invalidated = h[l];
+      }
+    }
     float ams = 0, bms = 0;
     CK(cudaEventElapsedTime(&ams, ev_apply.a, ev_apply.b));
     CK(cudaEventElapsedTime(&bms, ev_batch.a, ev_batch.b));

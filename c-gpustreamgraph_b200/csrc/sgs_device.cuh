@@ -93,6 +93,22 @@ __device__ __forceinline__ uint32_t edge_weight(const GraphView &g, uint64_t o,
   return 1u;
 }
 
+// True when some lane of `lanes` has a non-zero count in cnt[] (per-lane
+// reset counts of a group's last invalidation); one read per block, so a
+// whole launch can be skipped on the device without a host round trip.
+// Block-uniform; must be called by every thread of the block.
+__device__ __forceinline__ bool block_any_lane(const unsigned long long *cnt, uint64_t lanes) {
+  __shared__ int s_any;
+  if (threadIdx.x == 0) {
+    int a = 0;
+    for (int q = 0; q < 64; ++q)
+      if ((lanes >> q & 1ull) && cnt[q]) a = 1;
+    s_any = a;
+  }
+  __syncthreads();
+  return s_any != 0;
+}
+
 // Vertex bitmaps (one bit per vertex): `only` restricts a relaxation round to
 // destinations whose bit is set; `mark` records vertices reset by the
 // parent-tree invalidation.

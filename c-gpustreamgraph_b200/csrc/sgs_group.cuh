@@ -80,11 +80,21 @@ struct GroupRelaxOp {
     load_vals<S>(val, v, p.val);
     return p;
   }
+  // The quad's ids (and weights), loaded one step ahead by group_map.
+  struct Quad {
+    uint4 ids, ws;
+  };
+  __device__ __forceinline__ Quad fetch(const Payload &p, uint32_t j0) const {
+    Quad q;
+    q.ids = ld_quad(adj_ptr(g, p.off) + j0);
+    q.ws = any_w ? ld_quad(wgt_ptr(g, p.off) + j0) : make_uint4(1, 1, 1, 1);
+    return q;
+  }
   // Returns a 4-bit mask of destinations to append; dst[] holds them.
   __device__ __forceinline__ uint32_t visit4(uint32_t u, const Payload &p, uint32_t j0, uint32_t len,
-                                             uint32_t (&dst)[4]) const {
-    const uint4 ids = ld_quad(adj_ptr(g, p.off) + j0);
-    const uint4 ws = any_w ? ld_quad(wgt_ptr(g, p.off) + j0) : make_uint4(1, 1, 1, 1);
+                                             const Quad &qd, uint32_t (&dst)[4]) const {
+    const uint4 ids = qd.ids;
+    const uint4 ws = qd.ws;
     uint32_t okm = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -157,9 +167,15 @@ struct GroupInvalidateOp {
     p.pad = 0;
     return p;
   }
+  struct Quad {
+    uint4 ids;
+  };
+  __device__ __forceinline__ Quad fetch(const Payload &p, uint32_t j0) const {
+    return Quad{ld_quad(adj_ptr(g, p.off) + j0)};
+  }
   __device__ __forceinline__ uint32_t visit4(uint32_t u, const Payload &p, uint32_t j0, uint32_t len,
-                                             uint32_t (&dst)[4]) const {
-    const uint4 ids = ld_quad(adj_ptr(g, p.off) + j0);
+                                             const Quad &qd, uint32_t (&dst)[4]) const {
+    const uint4 ids = qd.ids;
     uint32_t okm = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -197,8 +213,11 @@ struct GroupInvalidateOp {
 // position adds live[v] for every lane of its mask, which counts exactly the
 // (query, edge) pairs relaxed.  The kernel also clears the previous
 // frontier's masks.
+#ifndef SGS_GROUP_MIN_BLOCKS
+#define SGS_GROUP_MIN_BLOCKS 4  // resident CTAs per SM the register budget allows
+#endif
 template <class Op>
-__global__ void __launch_bounds__(RELAX_THREADS, 5)
+__global__ void __launch_bounds__(RELAX_THREADS, SGS_GROUP_MIN_BLOCKS)
     group_map(FrontierView in, FrontierView out, Op op, const uint32_t *prev_vtx,
               const unsigned long long *prev_cnt, uint32_t *prev_mask,
               unsigned long long *lane_edges, unsigned long long *edge_stat) {
@@ -250,20 +269,41 @@ __global__ void __launch_bounds__(RELAX_THREADS, 5)
       __syncthreads();
       const uint64_t lo = max(E0, s_eb[0]);
       const uint64_t hi = min(E1, s_eb[GC]);
+      // Software pipeline: the owner search and id load of a thread's next
+      // quad are issued before the current quad's destination reads, so the
+      // three dependent latencies (search, ids, destination state) of
+      // consecutive quads overlap.
+      auto locate = [&](uint64_t e, int &l, uint32_t &j0) -> bool {
+        if (e >= hi) return false;
+        int a = 0, b = GC - 1;
+        while (a < b) {
+          const int m = (a + b + 1) >> 1;
+          if (s_eb[m] <= e) a = m;
+          else b = m - 1;
+        }
+        l = a;
+        j0 = (uint32_t)(e - s_eb[a]);
+        return j0 < s_len[a];
+      };
+      int lc = 0;
+      uint32_t jc = 0;
+      typename Op::Quad qc{};
+      const bool hc0 = locate(lo + 4 * threadIdx.x, lc, jc);
+      if (hc0) qc = op.fetch(s_pay[lc], jc);
+      bool hc = hc0;
       for (uint64_t base = lo; base < hi; base += 4 * RELAX_THREADS) {
-        const uint64_t e = base + 4 * threadIdx.x;
+        int ln = 0;
+        uint32_t jn = 0;
+        typename Op::Quad qn{};
+        const bool hn = locate(base + 4 * RELAX_THREADS + 4 * threadIdx.x, ln, jn);
+        if (hn) qn = op.fetch(s_pay[ln], jn);
         uint32_t app = 0;
         uint32_t dst[4] = {0, 0, 0, 0};
-        if (e < hi) {
-          int l = 0, r = GC - 1;
-          while (l < r) {
-            const int m = (l + r + 1) >> 1;
-            if (s_eb[m] <= e) l = m;
-            else r = m - 1;
-          }
-          const uint32_t j0 = (uint32_t)(e - s_eb[l]);
-          if (j0 < s_len[l]) app = op.visit4(s_vtx[l], s_pay[l], j0, s_len[l], dst);
-        }
+        if (hc) app = op.visit4(s_vtx[lc], s_pay[lc], jc, s_len[lc], qc, dst);
+        lc = ln;
+        jc = jn;
+        qc = qn;
+        hc = hn;
         if (__ballot_sync(0xFFFFFFFFu, app != 0u)) {
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
@@ -306,9 +346,13 @@ __global__ void k_group_init_lane(unsigned long long *st, uint32_t *val, uint32_
 
 // Every vertex with a non-empty block; mask = selected lanes whose value is
 // finite there (CC lanes always).  One writer per vertex: plain stores.
+// With `only_if_reset`, the launch does nothing unless a selected lane was
+// reset by the last invalidation (its per-lane counts).
 template <int S>
 __global__ void k_group_dense(GraphView g, const uint32_t *val, uint32_t lanes,
-                              LaneAlgo algo, uint32_t *m_out, FrontierView out) {
+                              LaneAlgo algo, uint32_t *m_out, FrontierView out,
+                              const unsigned long long *only_if_reset = nullptr) {
+  if (only_if_reset && !block_any_lane(only_if_reset, lanes)) return;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < g.nv; b += stride) {
     const uint64_t v = b + threadIdx.x;
@@ -386,11 +430,15 @@ __global__ void k_group_seed_deleted(GraphView g, unsigned long long *st, uint32
 // Relaxes just the kept inserted edges in the selected lanes: the whole
 // repair of an insert-only batch, and the inserted-edge half of the repair
 // after an invalidation (the other half is the restricted first round).
+// With `skip_if_reset`, the launch does nothing when a selected lane was
+// reset by the last invalidation (the full sweep covers the inserted edges).
 template <int S>
 __global__ void k_group_relax_inserted(GraphView g, unsigned long long *st, uint32_t *val, uint32_t lanes,
                                        LaneAlgo algo, const uint64_t *keys, const uint32_t *w,
                                        const uint32_t *n_ptr, uint32_t *m_out, FrontierView out,
-                                       unsigned long long *lane_edges) {
+                                       unsigned long long *lane_edges,
+                                       const unsigned long long *skip_if_reset = nullptr) {
+  if (skip_if_reset && block_any_lane(skip_if_reset, lanes)) return;
   const uint32_t n = *n_ptr;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   uint32_t counted = 0;

@@ -348,9 +348,12 @@ __global__ void k_wide_seed_sources(GraphView g, unsigned long long *st, uint32_
 
 // Every vertex with a non-empty block; mask = lanes of `lanes` whose value is
 // finite there (CC lanes always).  A warp reads 32 rows, one per step, and
-// appends the 32 vertices together.
+// appends the 32 vertices together.  With `only_if_reset`, nothing unless a
+// lane of `lanes` was reset by the last invalidation.
 __global__ void k_wide_dense(GraphView g, const uint32_t *val, unsigned long long lanes,
-                             unsigned long long cc, unsigned long long *m_out, FrontierView out) {
+                             unsigned long long cc, unsigned long long *m_out, FrontierView out,
+                             const unsigned long long *only_if_reset = nullptr) {
+  if (only_if_reset && !block_any_lane(only_if_reset, lanes)) return;
   const int t = threadIdx.x & 31;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   const bool l0 = lanes >> t & 1ull, l1 = lanes >> (t + 32) & 1ull;
