@@ -122,6 +122,60 @@ __device__ __forceinline__ void bit_set(uint32_t *bm, uint32_t v) {
 // Warp-aggregated append of (v, d) into a frontier.  Must be called by all 32
 // lanes of a converged warp; `want` selects the lanes that append.  One packed
 // 64-bit atomicAdd per warp reserves the slots and the edge range together.
+// Block-aggregated append of up to N consecutive vertices per thread
+// (v0 + i for want[i]): one atomic per block call for N x blockDim items,
+// entries in thread order, so a block's vertices stay in vertex order.
+template <int N>
+__device__ __forceinline__ void frontier_append_block_n(const FrontierView &f, const bool (&want)[N],
+                                                        uint32_t v0, const uint32_t (&d)[N]) {
+  constexpr int NW = RELAX_THREADS / 32;
+  __shared__ unsigned long long s_warp[NW];
+  __shared__ unsigned long long s_base;
+  const unsigned full = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned long long inc = 0;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+    if (want[i]) inc += (1ull << CNT_SHIFT) | (unsigned long long)((d[i] + 3u) & ~3u);
+  unsigned long long x = inc;
+#pragma unroll
+  for (int s = 1; s < 32; s <<= 1) {
+    const unsigned long long y = __shfl_up_sync(full, x, s);
+    if (lane >= s) x += y;
+  }
+  if (lane == 31) s_warp[wid] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long run = 0;
+    for (int w = 0; w < NW; ++w) {
+      const unsigned long long t = s_warp[w];
+      s_warp[w] = run;
+      run += t;
+    }
+    s_base = run ? atomicAdd((unsigned long long *)f.counter, run) : 0ull;
+  }
+  __syncthreads();
+  if (inc) {
+    unsigned long long pos = s_base + s_warp[wid] + (x - inc);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      if (!want[i]) continue;
+      const uint32_t dp = (d[i] + 3u) & ~3u;
+      const uint32_t slot = (uint32_t)(pos >> CNT_SHIFT);
+      const uint64_t eb = pos & EDGE_MASK;
+      f.vtx[slot] = v0 + i;
+      f.len[slot] = d[i];
+      f.ebase[slot] = eb;
+      if (dp) {
+        const uint64_t u0 = (eb + UNIT - 1) / UNIT, u1 = (eb + dp - 1) / UNIT;
+        for (uint64_t u = u0; u <= u1 && u < f.ucap; ++u) f.ustart[u] = slot;
+      }
+      pos += (1ull << CNT_SHIFT) | (unsigned long long)dp;
+    }
+  }
+  __syncthreads();  // s_warp / s_base are reused by the next call
+}
+
 __device__ __forceinline__ void frontier_append(const FrontierView &f, bool want,
                                                 uint32_t v, uint32_t d,
                                                 uint32_t *aux = nullptr,

@@ -353,27 +353,35 @@ __global__ void k_group_dense(GraphView g, const uint32_t *val, uint32_t lanes,
                               LaneAlgo algo, uint32_t *m_out, FrontierView out,
                               const unsigned long long *only_if_reset = nullptr) {
   if (only_if_reset && !block_any_lane(only_if_reset, lanes)) return;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < g.nv; b += stride) {
-    const uint64_t v = b + threadIdx.x;
-    bool want = false;
-    uint32_t d = 0;
-    if (v < g.nv) {
-      d = g.slots[v];
-      if (d) {
-        uint32_t blk[S];
-        load_vals<S>(val, (uint32_t)v, blk);
-        uint32_t m = 0;
+  // eight consecutive vertices per thread, one block append per 2048
+  constexpr int N = 8;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * N;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x * N; b < g.nv; b += stride) {
+    const uint64_t v0 = b + (uint64_t)threadIdx.x * N;
+    bool want[N];
+    uint32_t d[N];
 #pragma unroll
-        for (int q = 0; q < S; ++q)
-          if ((lanes >> q & 1u) && (algo.at(q) == A_CC || blk[q] != INF32)) m |= 1u << q;
-        if (m) {
-          m_out[v] = m;
-          want = true;
+    for (int i = 0; i < N; ++i) {
+      const uint64_t v = v0 + i;
+      want[i] = false;
+      d[i] = 0;
+      if (v < g.nv) {
+        d[i] = g.slots[v];
+        if (d[i]) {
+          uint32_t blk[S];
+          load_vals<S>(val, (uint32_t)v, blk);
+          uint32_t m = 0;
+#pragma unroll
+          for (int q = 0; q < S; ++q)
+            if ((lanes >> q & 1u) && (algo.at(q) == A_CC || blk[q] != INF32)) m |= 1u << q;
+          if (m) {
+            m_out[v] = m;
+            want[i] = true;
+          }
         }
       }
     }
-    frontier_append_block(out, want, (uint32_t)v, d);
+    frontier_append_block_n<N>(out, want, (uint32_t)v0, d);
   }
 }
 

@@ -116,11 +116,20 @@ struct TombOp {
     GroupPay p;
     p.off = g.off[v];
     p.gs = gstart[slot];
-    // end of the group: first key with a larger source
+    // end of the group: first key with a larger source.  Galloping from
+    // the group start: most sources have one or two deletes, so the first
+    // probe usually ends it; a hub's long group takes log2(size) probes.
     const uint64_t lim = ((uint64_t)v + 1) << 32;
-    uint32_t l = p.gs, r = nkeys;
+    uint32_t lo = p.gs + 1, step = 1, hi = p.gs + 1;  // keys[gs] < lim
+    while (hi < nkeys && keys[hi] < lim) {
+      lo = hi + 1;
+      step <<= 1;
+      hi = p.gs + step;
+    }
+    uint32_t r = hi < nkeys ? hi : nkeys;
+    uint32_t l = lo;
     while (l < r) {
-      uint32_t m = (l + r) >> 1;
+      const uint32_t m = (l + r) >> 1;
       if (keys[m] < lim) l = m + 1;
       else r = m;
     }
@@ -258,16 +267,18 @@ __global__ void k_append_one(FrontierView out, uint32_t v, uint32_t d) {
 
 // Every vertex with a non-empty block (PageRank rounds, loads, repacks).
 __global__ void k_dense_frontier(GraphView g, FrontierView out) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < g.nv; b += stride) {
-    const uint64_t v = b + threadIdx.x;
-    bool want = false;
-    uint32_t d = 0;
-    if (v < g.nv) {
-      d = g.slots[v];
-      want = d > 0;
+  constexpr int N = 8;  // consecutive vertices per thread, one block append per 2048
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * N;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x * N; b < g.nv; b += stride) {
+    const uint64_t v0 = b + (uint64_t)threadIdx.x * N;
+    bool want[N];
+    uint32_t d[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      d[i] = v0 + i < g.nv ? g.slots[v0 + i] : 0u;
+      want[i] = d[i] > 0;
     }
-    frontier_append_block(out, want, (uint32_t)v, d);
+    frontier_append_block_n<N>(out, want, (uint32_t)v0, d);
   }
 }
 
