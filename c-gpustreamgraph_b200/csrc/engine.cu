@@ -204,6 +204,7 @@ struct sgs_engine {
   uint32_t estamp = 1;
   DBuf<double> l1;                         // PR per-round L1
   DBuf<unsigned long long> rstat;          // per-round instance-edge counts
+  DBuf<unsigned long long> hstat;          // per-round host-tier slots
   DBuf<unsigned long long> b_lane;         // [WLANES] per-lane edge counts
   DBuf<unsigned long long> b_inval;        // [WLANES] per-lane resets
   DBuf<uint32_t> b_seed;                   // sources and lanes of new wide lanes
@@ -296,6 +297,7 @@ struct sgs_engine {
     rl_count.ensure(1);
     l1.ensure(cfg.max_rounds + 2);
     rstat.ensure(cfg.max_rounds + 2);
+    hstat.ensure(cfg.max_rounds + 2);
     b_lane.ensure(WLANES);
     b_inval.ensure(WLANES);
     if (cfg.group_size < 1 || cfg.group_size > WLANES) cfg.group_size = GMAX;
@@ -491,7 +493,7 @@ struct sgs_engine {
   // Accounts one timed launch: in = packed input counter of the launch,
   // inst = (instance, edge) pairs it relaxed, per_slot / per_inst = bytes.
   void account(int kind, unsigned long long in, unsigned long long inst, double per_slot,
-               double per_inst, cudaEvent_t a, cudaEvent_t b) {
+               double per_inst, cudaEvent_t a, cudaEvent_t b, unsigned long long host = 0) {
     const uint64_t n = in >> CNT_SHIFT, T = in & EDGE_MASK;
     if (!n) return;
     float ms = 0;
@@ -503,11 +505,13 @@ struct sgs_engine {
     k.entries += n;
     k.bytes_alg += bytes;
     k.ms += ms;
+    k.host_slots += host;
     if (T > k.max_slots) {
       k.max_slots = T;
       k.max_entries = n;
       k.max_bytes_alg = bytes;
       k.max_ms = ms;
+      k.max_host_slots = host;
     }
   }
 
@@ -554,7 +558,7 @@ struct sgs_engine {
     { ++n_launch; group_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
         fview(rr, cnt.p + rr), fview(rr + 1, cnt.p + rr + 1), op,
         hp ? fb[(rr - 1) % 3].vtx.p : nullptr, hp ? cnt.p + rr - 1 : nullptr,
-        hp ? gm[(rr - 1) % 3].p : nullptr, b_lane.p, rstat.p + rr); }
+        hp ? gm[(rr - 1) % 3].p : nullptr, b_lane.p, rstat.p + rr, hstat.p + rr); }
   }
 
   // Round loop shared by both group widths: `launch(rr)` queues round rr.
@@ -567,7 +571,8 @@ struct sgs_engine {
     uint32_t r = 0, rb = 4;
     converged = false;
     CK(cudaMemsetAsync(rstat.p, 0, sizeof(unsigned long long) * (maxr + 2), s));
-    std::vector<unsigned long long> hr(18);
+    CK(cudaMemsetAsync(hstat.p, 0, sizeof(unsigned long long) * (maxr + 2), s));
+    std::vector<unsigned long long> hr(18), hh(18);
     while (r < maxr) {
       const uint32_t nb = std::min(rb, maxr - r);
       if (ktiming) ensure_kev(2 * nb);
@@ -583,13 +588,16 @@ struct sgs_engine {
       CK(cudaGetLastError());
       CK(cudaMemcpyAsync(h_cnt, cnt.p + r, sizeof(unsigned long long) * (nb + 1),
                          cudaMemcpyDeviceToHost, s));
-      if (ktiming)
+      if (ktiming) {
         CK(cudaMemcpyAsync(hr.data(), rstat.p + r, sizeof(unsigned long long) * nb,
                            cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(hh.data(), hstat.p + r, sizeof(unsigned long long) * nb,
+                           cudaMemcpyDeviceToHost, s));
+      }
       sync();
       if (ktiming)
         for (uint32_t k = 0; k < nb; ++k)
-          account(kind, h_cnt[k], hr[k], per_slot, 8.0, kev[2 * k], kev[2 * k + 1]);
+          account(kind, h_cnt[k], hr[k], per_slot, 8.0, kev[2 * k], kev[2 * k + 1], hh[k]);
       for (uint32_t k = 0; k < nb; ++k)
         if (h_cnt[k + 1] == 0) {
           const uint32_t z = r + k + 1;  // first empty frontier

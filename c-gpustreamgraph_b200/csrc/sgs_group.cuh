@@ -220,7 +220,8 @@ template <class Op>
 __global__ void __launch_bounds__(RELAX_THREADS, SGS_GROUP_MIN_BLOCKS)
     group_map(FrontierView in, FrontierView out, Op op, const uint32_t *prev_vtx,
               const unsigned long long *prev_cnt, uint32_t *prev_mask,
-              unsigned long long *lane_edges, unsigned long long *edge_stat) {
+              unsigned long long *lane_edges, unsigned long long *edge_stat,
+              unsigned long long *host_stat) {
   using P = typename Op::Payload;
   constexpr int GC = GCHUNK;
   __shared__ uint64_t s_eb[GC + 1];
@@ -228,8 +229,11 @@ __global__ void __launch_bounds__(RELAX_THREADS, SGS_GROUP_MIN_BLOCKS)
   __shared__ P s_pay[GC];
   __shared__ uint32_t s_vtx[GC];
   __shared__ unsigned long long s_lane[GMAX];
+  __shared__ unsigned long long s_host;  // owned slots in the pinned-host tier
   clear_prev_masks(prev_vtx, prev_cnt, prev_mask);
   if (threadIdx.x < GMAX) s_lane[threadIdx.x] = 0;
+  if (threadIdx.x == 0) s_host = 0;
+  uint32_t host_acc = 0;
   uint32_t lane_acc[GMAX] = {0, 0, 0, 0};  // (query, edge) pairs of owned entries
   const uint64_t packed = __ldcg((const unsigned long long *)in.counter);
   const uint32_t n = (uint32_t)(packed >> CNT_SHIFT);
@@ -259,6 +263,7 @@ __global__ void __launch_bounds__(RELAX_THREADS, SGS_GROUP_MIN_BLOCKS)
           s_len[t] = __ldcg(&in.len[idx]);
           const P pay = op.load(v);
           s_pay[t] = pay;
+          if (eb >= E0 && (pay.off & HOST_BIT)) host_acc += s_len[t];
           if (eb >= E0 && pay.mask) {
             const uint32_t l = op.g.live[v];
 #pragma unroll
@@ -321,11 +326,14 @@ __global__ void __launch_bounds__(RELAX_THREADS, SGS_GROUP_MIN_BLOCKS)
     const unsigned long long x = warp_sum((unsigned long long)lane_acc[q]);
     if ((threadIdx.x & 31) == 0 && x) atomicAdd(&s_lane[q], x);
   }
+  const unsigned long long hs = warp_sum((unsigned long long)host_acc);
+  if ((threadIdx.x & 31) == 0 && hs) atomicAdd(&s_host, hs);
   __syncthreads();
   if (threadIdx.x < GMAX && s_lane[threadIdx.x]) {
     if (lane_edges) atomicAdd(&lane_edges[threadIdx.x], s_lane[threadIdx.x]);
     if (edge_stat) atomicAdd(edge_stat, s_lane[threadIdx.x]);
   }
+  if (threadIdx.x == 0 && s_host && host_stat) atomicAdd(host_stat, s_host);
 }
 
 // ---------------------------------------------------------------------------

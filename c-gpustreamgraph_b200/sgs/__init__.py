@@ -130,6 +130,8 @@ class KernelStats(C.Structure):
         ("max_entries", C.c_uint64),
         ("max_bytes_alg", C.c_double),
         ("max_ms", C.c_double),
+        ("host_slots", C.c_uint64),
+        ("max_host_slots", C.c_uint64),
     ]
 
     def as_dict(self):

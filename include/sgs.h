@@ -149,6 +149,9 @@ typedef struct sgs_kernel_stats {
   uint64_t max_entries;
   double max_bytes_alg;
   double max_ms;
+  uint64_t host_slots;     /* slots of blocks in the pinned-host tier (read
+                              over the host link); narrow groups only       */
+  uint64_t max_host_slots; /* the same for the largest launch               */
 } sgs_kernel_stats;
 
 SGS_API const char *sgs_version(void);
