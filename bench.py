@@ -728,7 +728,8 @@ def served_arm(a, R):
                    "parallelism": "replicas" if R.world > 1 else "single GPU"},
         "latency": {"update": pct("update"), "query": pct("query"), "bfs": pct("query", sgs.BFS),
                     "sssp": pct("query", sgs.SSSP), "pr": pct("query", sgs.PR)},
-        "query_batch": {"mean": round(float(np.mean(qb)), 2) if qb else 0, "max": int(max(qb)) if qb else 0},
+        "lanes_in_flight_at_admission": {"mean": round(float(np.mean(qb)), 2) if qb else 0,
+                                         "max": int(max(qb)) if qb else 0},
         "failed": int(len(res) - sum(ok)),
         "busy_s": round(busy, 3), "wall_s": round(wall, 3), "utilisation": round(busy / wall, 3),
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d / max(len(reqs), 1)),

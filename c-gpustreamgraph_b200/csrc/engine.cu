@@ -233,6 +233,13 @@ struct sgs_engine {
 
   std::vector<std::unique_ptr<Query>> queries;
   std::vector<std::unique_ptr<Group>> groups;
+  // serving: one group kept in flight; queries join free lanes at round
+  // boundaries and leave once no frontier entry carries their lane
+  Group *fg = nullptr;
+  uint32_t fr = 0;                   // next round; its input is buffer fr % 3 / cnt[fr]
+  uint64_t frun = 0;                 // lanes with work in flight
+  uint32_t fadmit[WLANES] = {};      // round at which each lane joined
+  DBuf<unsigned long long> flc;      // per-lane entry counts of the next frontier
   int next_qid = 1;
   sgs_engine_stats est{};
   Events ev_batch, ev_apply, ev_q;
@@ -316,6 +323,8 @@ struct sgs_engine {
     if (n >= (1u << 27)) fail(SGS_ERR_INVALID, "more than 2^27-1 vertices is not supported");
     queries.clear();
     groups.clear();
+    fg = nullptr;
+    frun = 0;
     loaded = false;
     est = sgs_engine_stats{};
     nv = n;
@@ -823,7 +832,7 @@ struct sgs_engine {
       } else {
         Group *G = nullptr;
         for (auto &gp : groups) {
-          if (gp->wide() != wide) continue;
+          if (gp->wide() != wide || gp.get() == fg) continue;
           uint64_t pend = 0;
           for (auto &t : touched)
             if (t.first == gp.get()) pend = t.second;
@@ -844,7 +853,8 @@ struct sgs_engine {
                 for (size_t j = groups.size(); j-- > 0;) {
                   bool pend = false;
                   for (auto &t : touched) pend |= t.first == groups[j].get();
-                  if (groups[j]->used == 0 && !pend) {
+                  if (groups[j]->used == 0 && !pend && !(groups[j].get() == fg && frun)) {
+                    if (groups[j].get() == fg) fg = nullptr;
                     groups.erase(groups.begin() + j);
                     freed = true;
                   }
@@ -882,11 +892,177 @@ struct sgs_engine {
     }
   }
 
+  // ------------------------------------------------------------ serving
+  Group &flight_group() {
+    if (!fg) {
+      auto ng = std::make_unique<Group>();
+      ng->width = cfg.group_size > (uint32_t)GMAX ? WLANES : GMAX;
+      ng->st.ensure((size_t)nv * ng->width);
+      ng->val.ensure((size_t)nv * ng->width);
+      if (ng->wide()) ensure_wide_masks();
+      fg = ng.get();
+      groups.push_back(std::move(ng));
+    }
+    flc.ensure(WLANES);
+    return *fg;
+  }
+  uint32_t flight_lanes() const {
+    const uint32_t w = cfg.group_size > (uint32_t)GMAX ? WLANES : GMAX;
+    return std::min<uint32_t>(w, std::max<uint32_t>(cfg.group_size, 1));
+  }
+  uint32_t flight_free() {
+    Group &G = flight_group();
+    uint32_t f = 0;
+    for (uint32_t l = 0; l < flight_lanes(); ++l) f += !(G.used >> l & 1ull);
+    return f;
+  }
+
+  // Joins BFS/SSSP/CC queries to the flight: lanes initialised, sources (CC:
+  // every vertex) seeded into the next round's frontier.
+  void flight_admit(uint32_t n, const int *algos, const uint32_t *sources, int *ids) {
+    if (!loaded) fail(SGS_ERR_STATE, "no graph loaded");
+    Group &G = flight_group();
+    for (uint32_t i = 0; i < n; ++i)
+      if (algos[i] < 0 || algos[i] > 2) fail(SGS_ERR_INVALID, "flight lanes take BFS, SSSP or CC");
+    if (n > flight_free()) fail(SGS_ERR_STATE, "no free lane in the flight");
+    if (!frun) {  // a new flight: counters from round 0, masks are clean
+      reset_counters(0);
+      fr = 0;
+    }
+    GraphView g = view();
+    uint64_t fresh = 0, cc = 0;
+    std::vector<Query *> qs;
+    for (uint32_t i = 0; i < n; ++i) {
+      int l = 0;
+      while (G.used >> l & 1ull) ++l;
+      auto q = std::make_unique<Query>();
+      q->id = next_qid++;
+      q->algo = algos[i];
+      q->source = std::min(sources[i], nv - 1);
+      q->grp = &G;
+      q->lane = l;
+      G.set_lane(l, q->algo);
+      G.used |= 1ull << l;
+      fresh |= 1ull << l;
+      if (q->algo == SGS_CC) cc |= 1ull << l;
+      fadmit[l] = fr;
+      ids[i] = q->id;
+      qs.push_back(q.get());
+      queries.push_back(std::move(q));
+      CK(cudaMemsetAsync(b_lane.p + l, 0, sizeof(unsigned long long), s));
+    }
+    const uint32_t b = fr % 3;
+    if (G.wide()) {
+      { ++n_launch; k_wide_init_lanes<<<grid_elem((uint64_t)nv * 32), 256, 0, s>>>(G.st.p, G.val.p, nv, fresh, G.cc); }
+      if (cc)
+        { ++n_launch; k_seed_all_or<unsigned long long><<<grid_elem(nv), RELAX_THREADS, 0, s>>>(
+            g, (unsigned long long)cc, wm[b].p, fview(fr, cnt.p + fr)); }
+      std::vector<uint32_t> src, lane;
+      for (Query *q : qs)
+        if (q->algo != SGS_CC) {
+          src.push_back(q->source);
+          lane.push_back((uint32_t)q->lane);
+        }
+      if (!src.empty()) {
+        b_seed.ensure(2 * src.size());
+        CK(cudaMemcpyAsync(b_seed.p, src.data(), sizeof(uint32_t) * src.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(b_seed.p + src.size(), lane.data(), sizeof(uint32_t) * lane.size(),
+                           cudaMemcpyHostToDevice, s));
+        { ++n_launch; k_wide_seed_sources<<<grid_elem(src.size()), 256, 0, s>>>(
+            g, G.st.p, G.val.p, b_seed.p, b_seed.p + src.size(), (uint32_t)src.size(), wm[b].p,
+            fview(fr, cnt.p + fr)); }
+      }
+    } else {
+      for (Query *q : qs)
+        { ++n_launch; k_group_init_lane<GMAX><<<grid_elem(nv), 256, 0, s>>>(G.st.p, G.val.p, nv, q->lane, q->algo,
+                                                                q->source); }
+      if (cc)
+        { ++n_launch; k_seed_all_or<uint32_t><<<grid_elem(nv), RELAX_THREADS, 0, s>>>(
+            g, (uint32_t)cc, gm[b].p, fview(fr, cnt.p + fr)); }
+      for (Query *q : qs)
+        if (q->algo != SGS_CC)
+          { ++n_launch; k_group_seed_one<<<1, 32, 0, s>>>(g, q->source, 1u << q->lane, gm[b].p, fview(fr, cnt.p + fr)); }
+    }
+    CK(cudaGetLastError());
+    frun |= fresh;
+  }
+
+  // Runs up to `rounds` relaxation rounds of the flight and returns the
+  // queries whose lanes no longer appear in the frontier (their results are
+  // final; they stay registered until removed).
+  void flight_advance(uint32_t rounds, std::vector<int> &done) {
+    done.clear();
+    if (!frun || !fg) return;
+    Group &G = *fg;
+    const uint32_t maxr = cfg.max_rounds;
+    rounds = std::max<uint32_t>(1, std::min<uint32_t>(rounds, 16));
+    if (fr + rounds + 3 >= maxr) {
+      // rebase the round index (same buffers: keep fr mod 3)
+      const uint32_t nb = 3 + fr % 3;
+      CK(cudaMemcpyAsync(cnt.p + nb - 1, cnt.p + fr - 1, 2 * sizeof(unsigned long long),
+                         cudaMemcpyDeviceToDevice, s));
+      CK(cudaMemsetAsync(cnt.p + nb + 1, 0, sizeof(unsigned long long) * (maxr + 1 - nb), s));
+      fr = nb;
+    }
+    GraphView g = view();
+    const bool anyw = G.sssp && cfg.weight_mode == SGS_W_EXPLICIT;
+    for (uint32_t k = 0; k < rounds; ++k) {
+      const uint32_t rr = fr + k;
+      if (G.wide())
+        launch_wide(rr, WideRelaxOp<>{G.st.p, G.val.p, G.walgo()}, nullptr);
+      else
+        launch_group(rr, GroupRelaxOp<GMAX>{g, G.st.p, G.val.p, gm[rr % 3].p, gm[(rr + 1) % 3].p,
+                                            G.algo(), anyw});
+    }
+    const uint32_t nf = fr + rounds;  // the next input frontier
+    CK(cudaMemsetAsync(flc.p, 0, sizeof(unsigned long long) * WLANES, s));
+    if (G.wide())
+      { ++n_launch; k_lane_counts<unsigned long long><<<grid_elem(nv), 256, 0, s>>>(
+          fb[nf % 3].vtx.p, cnt.p + nf, wm[nf % 3].p, flc.p); }
+    else
+      { ++n_launch; k_lane_counts<uint32_t><<<grid_elem(nv), 256, 0, s>>>(fb[nf % 3].vtx.p, cnt.p + nf,
+                                                                      gm[nf % 3].p, flc.p); }
+    CK(cudaGetLastError());
+    unsigned long long lc[WLANES], le[WLANES];
+    CK(cudaMemcpyAsync(h_cnt, cnt.p + fr, sizeof(unsigned long long) * (rounds + 1),
+                       cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(lc, flc.p, sizeof(lc), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(le, b_lane.p, sizeof(le), cudaMemcpyDeviceToHost, s));
+    sync();
+    uint32_t z = 0;  // first empty frontier of the batch, if any
+    for (uint32_t k = 1; k <= rounds && !z; ++k)
+      if ((h_cnt[k] >> CNT_SHIFT) == 0) z = fr + k;
+    uint64_t fin = 0;
+    if (z) {
+      clear_masks(G.wide(), z - 1);
+      fin = frun;
+    } else {
+      for (int l = 0; l < G.width; ++l)
+        if ((frun >> l & 1ull) && lc[l] == 0) fin |= 1ull << l;
+    }
+    const uint32_t end = z ? z : nf;
+    for (auto &q : queries) {
+      if (q->grp != &G || !(fin >> q->lane & 1ull)) continue;
+      q->stats.edges_traversed = le[q->lane];
+      q->stats.edges_total += le[q->lane];
+      q->stats.rounds = end - fadmit[q->lane];
+      q->stats.converged = 1;
+      q->stats.invalidated = 0;
+      done.push_back(q->id);
+    }
+    frun &= ~fin;
+    fr = end;
+  }
+
   // Frees the state of groups without lanes in use; true if any was freed.
   bool release_empty_groups() {
     bool any = false;
     for (size_t j = groups.size(); j-- > 0;)
       if (groups[j]->used == 0) {
+        if (groups[j].get() == fg) {
+          if (frun) continue;
+          fg = nullptr;
+        }
         groups.erase(groups.begin() + j);
         any = true;
       }
@@ -1587,6 +1763,30 @@ SGS_API int sgs_query_add_many(sgs_engine *e, uint32_t n, const int *algos, cons
       if (!e->find(qids[i]).stats.converged) fail(SGS_ERR_NOCONV, "round limit reached before convergence");
   });
 }
+
+}  // extern "C"
+
+// Flight interface used by the served loop (serve.cpp); not exported.
+namespace sgs {
+int flight_free(sgs_engine *e, uint32_t *lanes) {
+  return guarded([&] { *lanes = e->flight_free(); });
+}
+int flight_admit(sgs_engine *e, uint32_t n, const int *algos, const uint32_t *sources, int *ids) {
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    e->flight_admit(n, algos, sources, ids);
+  });
+}
+int flight_advance(sgs_engine *e, uint32_t rounds, std::vector<int> &done, uint64_t *running) {
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    e->flight_advance(rounds, done);
+    *running = e->frun;
+  });
+}
+}  // namespace sgs
+
+extern "C" {
 
 SGS_API int sgs_query_remove(sgs_engine *e, int qid) {
   if (!e) { g_last_error = "null engine"; return SGS_ERR_INVALID; }

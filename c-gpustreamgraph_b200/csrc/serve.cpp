@@ -3,22 +3,23 @@
 // No counterpart in the reference, whose drivers run one source through a
 // fixed list of snapshots (samples/hybrid_sssp/hybrid_sssp.cu:204-296).
 // Here a trace of requests -- update batches and one-shot queries, each with
-// an arrival time -- is served in arrival order on one host thread:
+// an arrival time -- is served in arrival order (FIFO) on one host thread,
+// with continuous batching at the granularity of relaxation rounds:
 //
-//   * an update batch is one snapshot (sgs_apply_batch), applied alone and
-//     in order, so every query sees exactly the updates that arrived before
-//     it and none after it (its "version");
-//   * consecutive queries at the head of the queue are admitted together
-//     (continuous batching): up to `slots` of them go through one
-//     sgs_query_add_many, so the BFS/SSSP/CC ones share group lanes and one
-//     convergence, and the PageRank ones (which have no source) share one
-//     computation; queries that arrive meanwhile wait for the next step;
-//   * a query's result (summary, and optionally its value/parent vectors)
-//     is read back and the query retired before the next step.
+//   * BFS/SSSP/CC queries join free lanes of one group kept in flight (up to
+//     `slots` lanes in use), between two rounds: a query that arrives while
+//     others are on the GPU starts at the next round boundary and its rounds
+//     overlap theirs in the same edge passes;
+//   * a query leaves as soon as no entry of the frontier carries its lane:
+//     its result is read back (summary, and optionally its value/parent
+//     vectors) and its lane freed for the next arrival;
+//   * an update batch is one snapshot, applied when the flight is empty, so
+//     every query sees exactly the updates that arrived before it (its
+//     "version"); queries behind an update wait for it;
+//   * PageRank has no lanes (and no source): consecutive PR queries share one
+//     computation, run when the flight is empty.
 //
-// `slots` bounds the queries in flight: the caller sizes it from the HBM
-// left after the graph (a lane's state is resident while it runs).  With
-// `realtime` the loop waits for arrival times on the wall clock, and
+// With `realtime` the loop waits for arrival times on the wall clock, and
 // latency = done_s - arrival_s includes queueing; without it every request
 // is taken as soon as the loop reaches it (a closed loop, latency = done_s).
 // Times are host wall-clock seconds from the start of the call.
@@ -26,6 +27,7 @@
 #include <chrono>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <numeric>
 #include <string>
 #include <thread>
@@ -35,7 +37,11 @@
 
 namespace sgs {
 void set_last_error(const std::string &msg);
-}
+// flight interface (engine.cu)
+int flight_free(sgs_engine *e, uint32_t *lanes);
+int flight_admit(sgs_engine *e, uint32_t n, const int *algos, const uint32_t *sources, int *ids);
+int flight_advance(sgs_engine *e, uint32_t rounds, std::vector<int> &done, uint64_t *running);
+}  // namespace sgs
 
 namespace {
 
@@ -44,6 +50,21 @@ using clk = std::chrono::steady_clock;
 double since(clk::time_point t0) {
   return std::chrono::duration<double>(clk::now() - t0).count();
 }
+
+constexpr uint32_t kRoundsPerStep = 4;  // rounds between two admission points
+
+// Result of a finished query into its completion record.
+void finish(sgs_engine *e, int qid, const sgs_request &r, sgs_completion &c) {
+  sgs_query_stats qs;
+  if (sgs_get_query_stats(e, qid, &qs) == SGS_OK) c.edges = qs.edges_traversed;
+  if (c.status == SGS_OK) c.status = sgs_query_summary(e, qid, c.summary);
+  if (c.status == SGS_OK && r.value_out)
+    c.status = sgs_gather(e, qid, SGS_FIELD_VALUE, r.value_out, SGS_MEM_HOST);
+  if (c.status == SGS_OK && r.parent_out && r.algo != SGS_PR)
+    c.status = sgs_gather(e, qid, SGS_FIELD_PARENT, r.parent_out, SGS_MEM_HOST);
+}
+
+bool lane_query(const sgs_request &r) { return r.kind == SGS_REQ_QUERY && r.algo != SGS_PR; }
 
 }  // namespace
 
@@ -65,6 +86,10 @@ SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n, uint32_
       sgs::set_last_error("request " + std::to_string(i) + ": arrival time must be >= 0");
       return SGS_ERR_INVALID;
     }
+    if (r.kind == SGS_REQ_QUERY && (r.algo < 0 || r.algo > 3)) {
+      sgs::set_last_error("request " + std::to_string(i) + ": unknown algorithm");
+      return SGS_ERR_INVALID;
+    }
   }
   std::vector<uint32_t> order(n);
   std::iota(order.begin(), order.end(), 0u);
@@ -74,92 +99,146 @@ SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n, uint32_
 
   const clk::time_point t0 = clk::now();
   std::deque<uint32_t> pending;
+  std::map<int, uint32_t> inflight;  // query id -> request
   uint32_t next = 0, done = 0;
-  uint64_t version = 0;
-  std::vector<int> algos, qids;
-  std::vector<uint32_t> sources, batch, slot;
+  uint64_t version = 0, running = 0;
+  std::vector<int> algos, qids, fin;
+  std::vector<uint32_t> sources, batch;
   while (done < n) {
-    double now = since(t0);
+    const double now = since(t0);
     while (next < n && (!realtime || req[order[next]].arrival_s <= now)) pending.push_back(order[next++]);
-    if (pending.empty()) {
-      // idle until the next arrival
-      const double wait = req[order[next]].arrival_s - now;
-      if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait));
-      continue;
-    }
-    const uint32_t head = pending.front();
-    if (req[head].kind == SGS_REQ_UPDATE) {
-      pending.pop_front();
-      const sgs_request &r = req[head];
-      sgs_completion &c = out[head];
-      c.start_s = since(t0);
-      c.status = sgs_apply_batch(e, r.ins_src, r.ins_dst, r.ins_w, r.n_ins, r.del_src, r.del_dst,
-                                 r.n_del, SGS_MEM_HOST);
-      if (c.status == SGS_OK) {
-        ++version;
-        sgs_engine_stats st;
-        if (sgs_get_engine_stats(e, &st) == SGS_OK) c.edges = st.last_batch_edges;
+
+    // 1. admission: lane queries at the head of the queue into free lanes
+    if (!pending.empty() && lane_query(req[pending.front()])) {
+      uint32_t free = 0;
+      if (sgs::flight_free(e, &free) != SGS_OK) free = 0;
+      if (slots) free = std::min<uint32_t>(free, slots > inflight.size() ? slots - (uint32_t)inflight.size() : 0u);
+      batch.clear();
+      while (batch.size() < free && !pending.empty() && lane_query(req[pending.front()])) {
+        batch.push_back(pending.front());
+        pending.pop_front();
       }
-      c.version = version;
-      c.batch = 1;
-      c.done_s = since(t0);
+      const uint32_t nb = (uint32_t)batch.size();
+      if (nb) {
+        algos.resize(nb);
+        sources.resize(nb);
+        qids.assign(nb, 0);
+        for (uint32_t k = 0; k < nb; ++k) {
+          algos[k] = req[batch[k]].algo;
+          sources[k] = req[batch[k]].source;
+        }
+        const double start = since(t0);
+        const int rc = sgs::flight_admit(e, nb, algos.data(), sources.data(), qids.data());
+        const uint32_t lanes_now = (uint32_t)inflight.size() + nb;  // lanes in flight with it
+        for (uint32_t k = 0; k < nb; ++k) {
+          sgs_completion &c = out[batch[k]];
+          c.start_s = start;
+          c.version = version;
+          c.batch = lanes_now;
+          c.status = rc;
+          if (rc == SGS_OK) {
+            inflight[qids[k]] = batch[k];
+          } else {
+            if (qids[k] > 0) sgs_query_remove(e, qids[k]);
+            c.done_s = since(t0);
+            ++done;
+          }
+        }
+      }
+    }
+
+    if (inflight.empty() && !pending.empty() && lane_query(req[pending.front()])) {
+      // nothing in flight and still no lane for the head: the flight cannot
+      // start (e.g. its state could not be allocated); fail the request
+      const uint32_t head = pending.front();
+      pending.pop_front();
+      out[head].status = SGS_ERR_STATE;
+      out[head].version = version;
+      out[head].start_s = out[head].done_s = since(t0);
       ++done;
       continue;
     }
-    // the run of queries at the head of the queue, up to `slots`
-    batch.clear();
-    while (!pending.empty() && req[pending.front()].kind == SGS_REQ_QUERY &&
-           (slots == 0 || batch.size() < slots)) {
-      batch.push_back(pending.front());
-      pending.pop_front();
-    }
-    const uint32_t nb = (uint32_t)batch.size();
-    // PageRank does not depend on the source: the batch's PR queries share
-    // one computation (slot[k] = which registered query answers request k)
-    algos.clear();
-    sources.clear();
-    slot.assign(nb, 0);
-    int pr_slot = -1;
-    for (uint32_t k = 0; k < nb; ++k) {
-      const sgs_request &r = req[batch[k]];
-      if (r.algo == SGS_PR && pr_slot >= 0) {
-        slot[k] = (uint32_t)pr_slot;
+
+    // 2. the flight: a few rounds, then retire the lanes that finished
+    if (!inflight.empty()) {
+      const int rc = sgs::flight_advance(e, kRoundsPerStep, fin, &running);
+      if (rc != SGS_OK) {  // fail every query in flight, keep serving
+        for (auto &kv : inflight) {
+          out[kv.second].status = rc;
+          out[kv.second].done_s = since(t0);
+          sgs_query_remove(e, kv.first);
+          ++done;
+        }
+        inflight.clear();
         continue;
       }
-      slot[k] = (uint32_t)algos.size();
-      if (r.algo == SGS_PR) pr_slot = (int)algos.size();
-      algos.push_back(r.algo);
-      sources.push_back(r.source);
+      for (int qid : fin) {
+        auto it = inflight.find(qid);
+        if (it == inflight.end()) continue;
+        finish(e, qid, req[it->second], out[it->second]);
+        sgs_query_remove(e, qid);
+        out[it->second].done_s = since(t0);
+        inflight.erase(it);
+        ++done;
+      }
+      continue;
     }
-    const uint32_t nq = (uint32_t)algos.size();
-    qids.assign(nq, 0);
-    const double start = since(t0);
-    const int rc = sgs_query_add_many(e, nq, algos.data(), sources.data(), qids.data());
-    for (uint32_t k = 0; k < nb; ++k) {
-      const sgs_request &r = req[batch[k]];
-      sgs_completion &c = out[batch[k]];
-      const int qid = qids[slot[k]];
-      c.start_s = start;
-      c.version = version;
-      c.batch = nb;
-      c.status = rc;
-      if (rc == SGS_OK) {
-        sgs_query_stats qs;
-        if (sgs_get_query_stats(e, qid, &qs) == SGS_OK) c.edges = qs.edges_traversed;
-        c.status = sgs_query_summary(e, qid, c.summary);
-        if (c.status == SGS_OK && r.value_out)
-          c.status = sgs_gather(e, qid, SGS_FIELD_VALUE, r.value_out, SGS_MEM_HOST);
-        if (c.status == SGS_OK && r.parent_out && r.algo != SGS_PR)
-          c.status = sgs_gather(e, qid, SGS_FIELD_PARENT, r.parent_out, SGS_MEM_HOST);
+
+    // 3. the flight is empty: an update, or PageRank, at the head
+    if (!pending.empty()) {
+      const uint32_t head = pending.front();
+      const sgs_request &r = req[head];
+      if (r.kind == SGS_REQ_UPDATE) {
+        pending.pop_front();
+        sgs_completion &c = out[head];
+        c.start_s = since(t0);
+        c.status = sgs_apply_batch(e, r.ins_src, r.ins_dst, r.ins_w, r.n_ins, r.del_src, r.del_dst,
+                                   r.n_del, SGS_MEM_HOST);
+        if (c.status == SGS_OK) {
+          ++version;
+          sgs_engine_stats st;
+          if (sgs_get_engine_stats(e, &st) == SGS_OK) c.edges = st.last_batch_edges;
+        }
+        c.version = version;
+        c.batch = 1;
+        c.done_s = since(t0);
+        ++done;
+        continue;
+      }
+      if (r.kind == SGS_REQ_QUERY && r.algo == SGS_PR) {
+        // consecutive PageRank queries share one computation
+        batch.clear();
+        while (!pending.empty() && req[pending.front()].kind == SGS_REQ_QUERY &&
+               req[pending.front()].algo == SGS_PR) {
+          batch.push_back(pending.front());
+          pending.pop_front();
+        }
+        const double start = since(t0);
+        int qid = 0;
+        const int rc = sgs_query_add(e, SGS_PR, 0, &qid);
+        for (uint32_t k : batch) {
+          sgs_completion &c = out[k];
+          c.start_s = start;
+          c.version = version;
+          c.batch = (uint32_t)batch.size();
+          c.status = rc;
+          if (rc == SGS_OK) finish(e, qid, req[k], c);
+        }
+        if (qid > 0) sgs_query_remove(e, qid);
+        const double end = since(t0);
+        for (uint32_t k : batch) out[k].done_s = end;
+        done += (uint32_t)batch.size();
+        continue;
       }
     }
-    // retire the batch (a failed add may have registered some of them)
-    for (uint32_t k = 0; k < nq; ++k)
-      if (qids[k] > 0) sgs_query_remove(e, qids[k]);
-    const double fin = since(t0);
-    for (uint32_t k = 0; k < nb; ++k) out[batch[k]].done_s = fin;
-    done += nb;
+
+    // 4. idle until the next arrival
+    if (next < n) {
+      const double wait = req[order[next]].arrival_s - since(t0);
+      if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait));
+    }
   }
+  (void)running;
   return SGS_OK;
 }
 

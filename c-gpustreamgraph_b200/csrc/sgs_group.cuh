@@ -550,6 +550,45 @@ __global__ void k_group_summary(const unsigned long long *st, uint32_t nv, int l
   }
 }
 
+// Lanes present in a frontier: per-lane counts of its entries' mask bits
+// (narrow u32 or wide u64 masks), for a serving loop that retires a lane as
+// soon as no entry carries it.
+template <class M>
+__global__ void k_lane_counts(const uint32_t *vtx, const unsigned long long *cnt, const M *mask,
+                              unsigned long long *out) {
+  __shared__ unsigned long long s[64];
+  if (threadIdx.x < 64) s[threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t n = (uint32_t)(__ldcg(cnt) >> CNT_SHIFT);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    unsigned long long m = (unsigned long long)__ldcg(&mask[__ldcg(&vtx[i])]);
+    while (m) {
+      const int q = __ffsll((long long)m) - 1;
+      atomicAdd(&s[q], 1ull);
+      m &= m - 1;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 64 && s[threadIdx.x]) atomicAdd(&out[threadIdx.x], s[threadIdx.x]);
+}
+
+// Dense seeding of CC lanes into a frontier that may already hold entries:
+// OR the lanes in, append only vertices whose mask was empty.
+template <class M>
+__global__ void k_seed_all_or(GraphView g, M bits, M *m_out, FrontierView out) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < g.nv; b += stride) {
+    const uint64_t v = b + threadIdx.x;
+    bool want = false;
+    uint32_t d = 0;
+    if (v < g.nv) {
+      d = g.slots[v];
+      if (d) want = atomicOr(&m_out[v], bits) == (M)0;
+    }
+    frontier_append_block(out, want, (uint32_t)v, d);
+  }
+}
+
 // Masks of the last non-empty frontier (after convergence).
 __global__ void k_clear_masks(const uint32_t *vtx, const unsigned long long *cnt, uint32_t *mask) {
   clear_prev_masks(vtx, cnt, mask);

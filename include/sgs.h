@@ -277,18 +277,22 @@ SGS_API int sgs_get_kernel_stats(sgs_engine *e, int kind, sgs_kernel_stats *out)
 /* Served request loop (no counterpart in the reference, whose drivers run
  * one source through a fixed snapshot list).  A trace of requests, each with
  * an arrival time in seconds, is served in arrival order on the calling
- * thread: an update batch is one snapshot applied alone (every query sees
- * exactly the updates that arrived before it: its `version`); consecutive
- * queries at the head of the queue are admitted together, up to `slots`
- * per step (size it from the HBM left after the graph; 0 = no limit), with
- * sgs_query_add_many, their results read back (summary, and the value /
- * parent vectors when buffers are given) and the queries retired.  With
- * `realtime` the loop waits for arrival times on the wall clock (latency =
- * done_s - arrival_s, queueing included); otherwise every request is taken
- * at once, in arrival order (a closed loop: latency = done_s).  out[i]
- * describes req[i]; times are host wall-clock seconds from the start of the
- * call.  Requests that fail carry their status;
- * the call itself fails only for malformed arguments. */
+ * thread, with continuous batching at the granularity of relaxation rounds:
+ * BFS/SSSP/CC queries join free lanes of one group kept in flight (at most
+ * `slots` lanes in use; 0 = the group's width) between two rounds, so a query
+ * arriving while others run starts at the next round boundary and shares
+ * their edge passes; a query leaves as soon as no frontier entry carries its
+ * lane (summary, and the value / parent vectors when buffers are given, read
+ * back) and frees the lane.  An update batch is one snapshot, applied when
+ * the flight is empty, so every query sees exactly the updates that arrived
+ * before it (its `version`).  PageRank queries (no lanes, no source) share
+ * one computation per run of consecutive PR requests.  With `realtime` the
+ * loop waits for arrival times on the wall clock (latency = done_s -
+ * arrival_s, queueing included); otherwise every request is taken at once, in
+ * arrival order (a closed loop: latency = done_s).  out[i] describes req[i];
+ * times are host wall-clock seconds from the start of the call.  Requests
+ * that fail carry their status; the call itself fails only for malformed
+ * arguments. */
 #define SGS_REQ_QUERY 0
 #define SGS_REQ_UPDATE 1
 typedef struct sgs_request {
@@ -306,8 +310,9 @@ typedef struct sgs_request {
 } sgs_request;
 typedef struct sgs_completion {
   int status;               /* SGS_OK or this request's error                */
-  uint32_t batch;           /* queries admitted in the same step (1 for an
-                               update)                                       */
+  uint32_t batch;           /* queries: lanes in flight when it joined (PR:
+                               requests sharing the computation); 1 for an
+                               update                                        */
   uint64_t version;         /* updates applied before the query ran; for an
                                update, its own position in the sequence     */
   double start_s, done_s;   /* seconds from the start of the call            */

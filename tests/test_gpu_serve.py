@@ -156,3 +156,33 @@ def test_serve_rejects_malformed_requests():
         with pytest.raises(sgs.SgsError):
             e.serve([{"kind": "query", "algo": 0, "arrival_s": -1.0}])
         assert e.serve([]) == []
+
+
+def test_queries_join_a_running_flight():
+    """Continuous batching: queries that arrive while others are on the GPU
+    start at the next round boundary and finish on their own -- some query
+    starts while another is still running -- and results stay exact."""
+    nv, row, col = O.rmat_csr(14, 16, 6)
+    w = O.weights(nv, row, col, 3, 0)
+    rng = np.random.default_rng(4)
+    reqs = []
+    t = 0.0
+    for k in range(40):
+        t += rng.exponential(0.0005)
+        a = [sgs.BFS, sgs.SSSP][k % 2]
+        reqs.append({"kind": "query", "algo": a, "source": int(rng.integers(0, nv)), "arrival_s": t,
+                     "value_out": np.empty(nv, np.uint32), "parent_out": np.empty(nv, np.uint32)})
+    with sgs.Engine(group_size=64) as e:
+        e.load_csr(nv, row, col, w)
+        res = e.serve(reqs, slots=16, realtime=True)
+    overlap = False
+    for i, a in enumerate(res):
+        for b in res[i + 1:]:
+            if a["start_s"] < b["start_s"] < a["done_s"] or b["start_s"] < a["start_s"] < b["done_s"]:
+                overlap = True
+    assert overlap
+    assert max(c["batch"] for c in res) <= 16
+    m = Mirror(nv, row, col, w)
+    for r, c in zip(reqs, res):
+        assert c["status"] == 0 and c["version"] == 0
+        check_query(Res(r["algo"], r["source"], r["value_out"], r["parent_out"]), m, sgs.W_EXPLICIT)
