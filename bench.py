@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--persistent", type=int, default=None,
+                    help="1: each relaxation phase as one cooperative launch over rounds")
     ap.add_argument("--workload", default="snapshot", choices=["snapshot", "ppr", "batched", "served"],
                     help="snapshot: incremental SSSP/BFS/CC (the headline); ppr: weighted "
                          "personalized PageRank forward + adjoint; batched: 256 BFS + 256 SSSP "
@@ -182,6 +184,11 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def pers(a):
+    """Engine option for --persistent (the library default otherwise)."""
+    return {} if a.persistent is None else {"persistent": int(a.persistent)}
+
+
 def measure_h2d_gbs(dev, nbytes=1 << 30, reps=3):
     """Pinned host -> device copy bandwidth (GB/s), best of `reps`, CUDA
     events: the host-link peak for blocks kept in the pinned-host tier."""
@@ -220,7 +227,7 @@ def engine_arm(a, R):
 
     dev = torch.device("cuda", R.local)
     torch.cuda.set_device(dev)
-    e = sgs.Engine(device=R.local, hbm_budget_gb=a.budget_gb, weight_mode=sgs.W_EXPLICIT)
+    e = sgs.Engine(device=R.local, hbm_budget_gb=a.budget_gb, weight_mode=sgs.W_EXPLICIT, **pers(a))
     t0 = time.time()
     e.load_rmat(a.scale, a.edge_factor, a.seed, 0.57, 0.19, 0.19, wseed=a.seed)
     t_gen = time.time() - t0
@@ -482,7 +489,7 @@ def batched_arm(a, R):
     dev = torch.device("cuda", R.local)
     torch.cuda.set_device(dev)
     t0 = time.time()
-    e = sgs.Engine(device=R.local, weight_mode=sgs.W_EXPLICIT, group_size=a.group_size)
+    e = sgs.Engine(device=R.local, weight_mode=sgs.W_EXPLICIT, group_size=a.group_size, **pers(a))
     e.load_rmat(a.batched_scale, a.edge_factor, a.seed, 0.57, 0.19, 0.19, wseed=a.seed)
     nv = int(e.engine_stats()["nv"])
     row, col, _ = e.export()
@@ -567,7 +574,7 @@ def batched_arm(a, R):
     if a.plain_sample > 0:
         k = min(a.plain_sample, nq)
         sample = specs[:k // 2] + specs[a.batched_bfs:a.batched_bfs + (k - k // 2)]
-        p = sgs.Engine(device=R.local, weight_mode=sgs.W_EXPLICIT, group_size=1)
+        p = sgs.Engine(device=R.local, weight_mode=sgs.W_EXPLICIT, group_size=1, **pers(a))
         p.load_rmat(a.batched_scale, a.edge_factor, a.seed, 0.57, 0.19, 0.19, wseed=a.seed)
         pq = p.add_queries(sample)
         pe, pms = run_snapshots(p, pq, batches, dev_of, a.warmup, a.steps)

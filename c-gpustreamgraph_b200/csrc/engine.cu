@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <array>
+#include <map>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -624,6 +625,107 @@ struct sgs_engine {
     return r;
   }
 
+  // ------------------------------------------------- persistent round loops
+  std::map<const void *, int> coop_cache;
+  DBuf<uint32_t> d_rounds;
+  // One wave of co-resident CTAs for a cooperative launch.
+  int coop_grid(const void *f) {
+    auto it = coop_cache.find(f);
+    if (it != coop_cache.end()) return it->second;
+    int b = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, RELAX_THREADS, 0));
+    if (b < 1) fail(SGS_ERR_CUDA, "persistent round kernel cannot be resident");
+    const int g = nsm * b;
+    coop_cache[f] = g;
+    return g;
+  }
+  template <class M>
+  RoundBufs<M> round_bufs(DBuf<M> (&masks)[3]) {
+    RoundBufs<M> rb;
+    for (int i = 0; i < 3; ++i) {
+      rb.vtx[i] = fb[i].vtx.p;
+      rb.len[i] = fb[i].len.p;
+      rb.ebase[i] = fb[i].ebase.p;
+      rb.ustart[i] = fb[i].ustart.p;
+      rb.mask[i] = masks[i].p;
+    }
+    rb.cnt = cnt.p;
+    rb.ucap = ucap;
+    return rb;
+  }
+  // After a persistent launch: its round count (one host read) and, with
+  // kernel timing, the whole launch accounted as one.
+  uint32_t finish_persistent(uint32_t r0, bool &converged, int kind, double per_slot,
+                             cudaEvent_t a, cudaEvent_t b) {
+    uint32_t rounds = 0;
+    CK(cudaMemcpyAsync(&rounds, d_rounds.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    std::vector<unsigned long long> hc, hr, hh;
+    if (ktiming) {
+      const size_t m = cfg.max_rounds + 2;
+      hc.resize(m);
+      hr.resize(m);
+      hh.resize(m);
+      CK(cudaMemcpyAsync(hc.data(), cnt.p, sizeof(unsigned long long) * m, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(hr.data(), rstat.p, sizeof(unsigned long long) * m, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(hh.data(), hstat.p, sizeof(unsigned long long) * m, cudaMemcpyDeviceToHost, s));
+    }
+    sync();
+    converged = rounds < cfg.max_rounds;
+    if (ktiming) {
+      unsigned long long n = 0, T = 0, inst = 0, host = 0;
+      for (uint32_t r = r0; r < rounds && r < cfg.max_rounds; ++r) {
+        n += hc[r] >> CNT_SHIFT;
+        T += hc[r] & EDGE_MASK;
+        inst += hr[r];
+        host += hh[r];
+      }
+      if (n) account(kind, (n << CNT_SHIFT) | T, inst, per_slot, 8.0, a, b, host);
+    }
+    return rounds;
+  }
+  template <class Op>
+  uint32_t run_group_persistent(const Op &op, uint32_t r0, bool &converged, int kind, double per_slot) {
+    d_rounds.ensure(1);
+    if (r0 == 0) {
+      CK(cudaMemsetAsync(rstat.p, 0, sizeof(unsigned long long) * (cfg.max_rounds + 2), s));
+      CK(cudaMemsetAsync(hstat.p, 0, sizeof(unsigned long long) * (cfg.max_rounds + 2), s));
+    }
+    RoundBufs<uint32_t> rb = round_bufs(gm);
+    uint32_t maxr = cfg.max_rounds;
+    unsigned long long *le = b_lane.p, *rs = rstat.p, *hs = hstat.p;
+    uint32_t *ro = d_rounds.p;
+    Op o = op;
+    void *args[] = {&rb, &o, &r0, &maxr, &le, &rs, &hs, &ro};
+    const void *f = (const void *)group_rounds<Op>;
+    if (ktiming) { ensure_kev(2); CK(cudaEventRecord(kev[0], s)); }
+    ++n_launch;
+    CK(cudaLaunchCooperativeKernel(f, coop_grid(f), RELAX_THREADS, args, 0, s));
+    if (ktiming) CK(cudaEventRecord(kev[1], s));
+    return finish_persistent(r0, converged, kind, per_slot, ktiming ? kev[0] : nullptr,
+                             ktiming ? kev[1] : nullptr);
+  }
+  template <class Op>
+  uint32_t run_wide_persistent(const Op &op, uint32_t r0, bool &converged, int kind, double per_slot,
+                               unsigned long long *lane_changes) {
+    d_rounds.ensure(1);
+    if (r0 == 0) CK(cudaMemsetAsync(rstat.p, 0, sizeof(unsigned long long) * (cfg.max_rounds + 2), s));
+    CK(cudaMemsetAsync(hstat.p, 0, sizeof(unsigned long long) * (cfg.max_rounds + 2), s));
+    GraphView g = view();
+    RoundBufs<unsigned long long> rb = round_bufs(wm);
+    uint32_t maxr = cfg.max_rounds;
+    unsigned long long *le = b_lane.p, *lc = lane_changes, *rs = rstat.p;
+    uint32_t *ro = d_rounds.p;
+    Op o = op;
+    void *args[] = {&g, &rb, &o, &r0, &maxr, &le, &lc, &rs, &ro};
+    const void *f = (const void *)wide_rounds<Op>;
+    if (ktiming) { ensure_kev(2); CK(cudaEventRecord(kev[0], s)); }
+    ++n_launch;
+    CK(cudaLaunchCooperativeKernel(f, coop_grid(f), RELAX_THREADS, args, 0, s));
+    if (ktiming) CK(cudaEventRecord(kev[1], s));
+    return finish_persistent(r0, converged, kind, per_slot, ktiming ? kev[0] : nullptr,
+                             ktiming ? kev[1] : nullptr);
+  }
+
   // Masks of the frontier of round f (buffer f % 3, counter cnt[f]).
   void clear_masks(bool wide, uint32_t f) {
     if (wide)
@@ -652,11 +754,30 @@ struct sgs_engine {
       WideRelaxOp<> op{G.st.p, G.val.p, G.walgo()};
       WideRelaxOp<true> op0{G.st.p, G.val.p, G.walgo()};
       op0.only = only0;
+      if (cfg.persistent) {
+        if (!only0 && !after0) return run_wide_persistent(op, 0, conv, SGS_K_WIDE, anyw ? 8.0 : 4.0, nullptr);
+        // round 0 (restricted) and its hook as plain launches, then one launch
+        CK(cudaMemsetAsync(rstat.p, 0, sizeof(unsigned long long) * (cfg.max_rounds + 2), s));
+        if (round0) nvtxRangePushA(round0);
+        if (only0) launch_wide(0, op0, nullptr);
+        else launch_wide(0, op, nullptr);
+        if (round0) nvtxRangePop();
+        if (after0) (*after0)();
+        return run_wide_persistent(op, 1, conv, SGS_K_WIDE, anyw ? 8.0 : 4.0, nullptr);
+      }
       if (only0)
         return run_wide_rounds(op0, op, conv, SGS_K_WIDE, anyw ? 8.0 : 4.0, nullptr, round0, after0);
       return run_wide_rounds(op, op, conv, SGS_K_WIDE, anyw ? 8.0 : 4.0, nullptr, round0, after0);
     }
     const uint32_t anyw = G.any_sssp(G.used | 0xF) && cfg.weight_mode == SGS_W_EXPLICIT;
+    if (cfg.persistent && !after0) {
+      if (round0) nvtxRangePushA(round0);
+      const uint32_t r = run_group_persistent(
+          GroupRelaxOp<GMAX>{g, G.st.p, G.val.p, nullptr, nullptr, G.algo(), anyw}, 0, conv, SGS_K_GROUP,
+          anyw ? 8.0 : 4.0);
+      if (round0) nvtxRangePop();
+      return r;
+    }
     return run_rounds(
         [&](uint32_t rr) {
           uint32_t *mi = gm[rr % 3].p, *mo = gm[(rr + 1) % 3].p;
@@ -1204,17 +1325,23 @@ struct sgs_engine {
         CK(cudaGetLastError());
         WideInvalidateOp op{G.st.p, G.val.p, WideAlgo{0ull, G.cc}};  // no weights needed
         op.mark = G.ibits.p;
-        run_wide_rounds(op, op, conv, SGS_K_WIDE_INVAL, 4.0, b_inval.p);
+        if (cfg.persistent) run_wide_persistent(op, 0, conv, SGS_K_WIDE_INVAL, 4.0, b_inval.p);
+        else run_wide_rounds(op, op, conv, SGS_K_WIDE_INVAL, 4.0, b_inval.p);
       } else {
         { ++n_launch; k_group_seed_deleted<GMAX><<<grid_elem(nd), 256, 0, s>>>(
             g, G.st.p, G.val.p, (uint32_t)G.used, G.algo(), b_dkeys_s.p, (uint32_t)nd, b_inval.p,
             nullptr, gm[0].p, fview(0, cnt.p)); }
         CK(cudaGetLastError());
-        run_group_rounds(
-            [&](uint32_t, uint32_t *mi, uint32_t *mo) {
-              return GroupInvalidateOp<GMAX>{g, G.st.p, G.val.p, mi, mo, G.algo(), b_inval.p, nullptr};
-            },
-            conv, SGS_K_GROUP_INVAL, 4.0);
+        if (cfg.persistent)
+          run_group_persistent(GroupInvalidateOp<GMAX>{g, G.st.p, G.val.p, nullptr, nullptr, G.algo(),
+                                                       b_inval.p, nullptr},
+                               0, conv, SGS_K_GROUP_INVAL, 4.0);
+        else
+          run_group_rounds(
+              [&](uint32_t, uint32_t *mi, uint32_t *mo) {
+                return GroupInvalidateOp<GMAX>{g, G.st.p, G.val.p, mi, mo, G.algo(), b_inval.p, nullptr};
+              },
+              conv, SGS_K_GROUP_INVAL, 4.0);
       }
       if (!conv) fail(SGS_ERR_NOCONV, "invalidation did not converge");
       CK(cudaEventRecord(gev[4 * i + 1], s));
@@ -1627,6 +1754,7 @@ SGS_API void sgs_config_default(sgs_config *c) {
   c->slack_div = 8;
   c->arena_headroom = 0.30;
   c->group_size = 4;
+  c->persistent = 0;
 }
 
 SGS_API int sgs_create(const sgs_config *cfg, sgs_engine **out) {

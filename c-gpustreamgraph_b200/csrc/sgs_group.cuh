@@ -15,6 +15,8 @@
 // propagation, reset_del_edges / SyncPushDDB_del parent-tree invalidation,
 // driver.cuh:398-430 and :1985-2031).
 #pragma once
+#include <cooperative_groups.h>
+
 #include "sgs_device.cuh"
 #include "sgs_segmap.cuh"
 
@@ -217,11 +219,12 @@ struct GroupInvalidateOp {
 #define SGS_GROUP_MIN_BLOCKS 4  // resident CTAs per SM the register budget allows
 #endif
 template <class Op>
-__global__ void __launch_bounds__(RELAX_THREADS, SGS_GROUP_MIN_BLOCKS)
-    group_map(FrontierView in, FrontierView out, Op op, const uint32_t *prev_vtx,
-              const unsigned long long *prev_cnt, uint32_t *prev_mask,
-              unsigned long long *lane_edges, unsigned long long *edge_stat,
-              unsigned long long *host_stat) {
+__device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out, const Op &op,
+                                               const uint32_t *prev_vtx,
+                                               const unsigned long long *prev_cnt, uint32_t *prev_mask,
+                                               unsigned long long *lane_edges,
+                                               unsigned long long *edge_stat,
+                                               unsigned long long *host_stat) {
   using P = typename Op::Payload;
   constexpr int GC = GCHUNK;
   __shared__ uint64_t s_eb[GC + 1];
@@ -334,6 +337,76 @@ __global__ void __launch_bounds__(RELAX_THREADS, SGS_GROUP_MIN_BLOCKS)
     if (edge_stat) atomicAdd(edge_stat, s_lane[threadIdx.x]);
   }
   if (threadIdx.x == 0 && s_host && host_stat) atomicAdd(host_stat, s_host);
+  __syncthreads();  // shared state is reused when the body runs again
+}
+
+template <class Op>
+__global__ void __launch_bounds__(RELAX_THREADS, SGS_GROUP_MIN_BLOCKS)
+    group_map(FrontierView in, FrontierView out, Op op, const uint32_t *prev_vtx,
+              const unsigned long long *prev_cnt, uint32_t *prev_mask,
+              unsigned long long *lane_edges, unsigned long long *edge_stat,
+              unsigned long long *host_stat) {
+  group_map_body(in, out, op, prev_vtx, prev_cnt, prev_mask, lane_edges, edge_stat, host_stat);
+}
+
+// The three rotating frontier buffers, their counters and lane masks, as one
+// persistent launch sees them: round r reads buffer r % 3 / cnt[r] and masks
+// r % 3, and writes buffer (r+1) % 3 / cnt[r+1].
+template <class M>
+struct RoundBufs {
+  uint32_t *vtx[3];
+  uint32_t *len[3];
+  uint64_t *ebase[3];
+  uint32_t *ustart[3];
+  unsigned long long *cnt;
+  M *mask[3];
+  uint32_t ucap;
+  __device__ __forceinline__ FrontierView view(uint32_t r) const {
+    FrontierView f;
+    f.vtx = vtx[r % 3];
+    f.len = len[r % 3];
+    f.ebase = ebase[r % 3];
+    f.ustart = ustart[r % 3];
+    f.counter = (uint64_t *)(cnt + r);
+    f.ucap = ucap;
+    return f;
+  }
+};
+
+// Rounds r0, r0+1, ... of a phase in one cooperative launch: round r, a
+// grid-wide barrier (cooperative_groups grid sync; the cooperative launch
+// makes every block resident), then the next round unless round r appended
+// nothing.  The masks of the last non-empty frontier are cleared before the
+// kernel returns; *rounds_out = the first empty frontier's index (or
+// max_rounds when the limit is hit).
+template <class Op>
+__global__ void __launch_bounds__(RELAX_THREADS, SGS_GROUP_MIN_BLOCKS)
+    group_rounds(RoundBufs<uint32_t> rb, Op op, uint32_t r0, uint32_t max_rounds,
+                 unsigned long long *lane_edges, unsigned long long *rstat, unsigned long long *hstat,
+                 uint32_t *rounds_out) {
+  cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+  uint32_t r = r0;
+  bool conv = false;
+  for (; r < max_rounds; ++r) {
+    Op o = op;
+    o.m_in = rb.mask[r % 3];
+    o.m_out = rb.mask[(r + 1) % 3];
+    const bool hp = r >= 1;
+    group_map_body(rb.view(r), rb.view(r + 1), o, hp ? rb.vtx[(r - 1) % 3] : nullptr,
+                   hp ? rb.cnt + r - 1 : nullptr, hp ? rb.mask[(r - 1) % 3] : nullptr, lane_edges,
+                   rstat + r, hstat + r);
+    __threadfence();
+    grid.sync();
+    if ((__ldcg(rb.cnt + r + 1) >> CNT_SHIFT) == 0) {
+      conv = true;
+      ++r;
+      break;
+    }
+  }
+  // r: the first empty frontier (converged) or max_rounds
+  if (r >= 1) clear_prev_masks(rb.vtx[(r - 1) % 3], rb.cnt + r - 1, rb.mask[(r - 1) % 3]);
+  if (!conv) clear_prev_masks(rb.vtx[r % 3], rb.cnt + r, rb.mask[r % 3]);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *rounds_out = r;
 }
 
 // ---------------------------------------------------------------------------

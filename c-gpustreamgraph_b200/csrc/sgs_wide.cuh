@@ -18,6 +18,7 @@
 // (reset_del_edges / SyncPushDDB_del, driver.cuh:398-430, :1985-2031).
 #pragma once
 #include "sgs_device.cuh"
+#include "sgs_group.cuh"
 #include "sgs_segmap.cuh"
 
 namespace sgs {
@@ -126,12 +127,14 @@ struct WideInvalidateOp {
 // edge_stat receives the (lane, edge) pairs actually evaluated -- fewer than
 // the traversed count when a restricted round skips destinations.
 template <class Op>
-__global__ void __launch_bounds__(RELAX_THREADS, 3)
-    wide_map(GraphView g, FrontierView in, FrontierView out, Op op,
-             const unsigned long long *m_in, unsigned long long *m_out, const uint32_t *prev_vtx,
-             const unsigned long long *prev_cnt, unsigned long long *prev_mask,
-             unsigned long long *lane_edges, unsigned long long *lane_changes,
-             unsigned long long *edge_stat) {
+__device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView in, FrontierView out,
+                                              const Op &op, const unsigned long long *m_in,
+                                              unsigned long long *m_out, const uint32_t *prev_vtx,
+                                              const unsigned long long *prev_cnt,
+                                              unsigned long long *prev_mask,
+                                              unsigned long long *lane_edges,
+                                              unsigned long long *lane_changes,
+                                              unsigned long long *edge_stat) {
   constexpr int GC = WCHUNK;
   __shared__ uint64_t s_eb[GC + 1];
   __shared__ uint64_t s_off[GC];
@@ -299,6 +302,46 @@ __global__ void __launch_bounds__(RELAX_THREADS, 3)
     if (c && lane_changes) atomicAdd(&lane_changes[threadIdx.x], c);
   }
   if (threadIdx.x == 0 && s_eval && edge_stat) atomicAdd(edge_stat, s_eval);
+  __syncthreads();  // shared state is reused when the body runs again
+}
+
+template <class Op>
+__global__ void __launch_bounds__(RELAX_THREADS, 3)
+    wide_map(GraphView g, FrontierView in, FrontierView out, Op op,
+             const unsigned long long *m_in, unsigned long long *m_out, const uint32_t *prev_vtx,
+             const unsigned long long *prev_cnt, unsigned long long *prev_mask,
+             unsigned long long *lane_edges, unsigned long long *lane_changes,
+             unsigned long long *edge_stat) {
+  wide_map_body(g, in, out, op, m_in, m_out, prev_vtx, prev_cnt, prev_mask, lane_edges,
+                lane_changes, edge_stat);
+}
+
+// Rounds r0, r0+1, ... of a wide phase in one cooperative launch (see
+// group_rounds).
+template <class Op>
+__global__ void __launch_bounds__(RELAX_THREADS, 3)
+    wide_rounds(GraphView g, RoundBufs<unsigned long long> rb, Op op, uint32_t r0, uint32_t max_rounds,
+                unsigned long long *lane_edges, unsigned long long *lane_changes,
+                unsigned long long *rstat, uint32_t *rounds_out) {
+  cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+  uint32_t r = r0;
+  bool conv = false;
+  for (; r < max_rounds; ++r) {
+    const bool hp = r >= 1;
+    wide_map_body(g, rb.view(r), rb.view(r + 1), op, rb.mask[r % 3], rb.mask[(r + 1) % 3],
+                  hp ? rb.vtx[(r - 1) % 3] : nullptr, hp ? rb.cnt + r - 1 : nullptr,
+                  hp ? rb.mask[(r - 1) % 3] : nullptr, lane_edges, lane_changes, rstat + r);
+    __threadfence();
+    grid.sync();
+    if ((__ldcg(rb.cnt + r + 1) >> CNT_SHIFT) == 0) {
+      conv = true;
+      ++r;
+      break;
+    }
+  }
+  if (r >= 1) clear_prev_masks64(rb.vtx[(r - 1) % 3], rb.cnt + r - 1, rb.mask[(r - 1) % 3]);
+  if (!conv) clear_prev_masks64(rb.vtx[r % 3], rb.cnt + r, rb.mask[r % 3]);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *rounds_out = r;
 }
 
 // ---------------------------------------------------------------------------

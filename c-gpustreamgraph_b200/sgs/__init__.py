@@ -79,6 +79,7 @@ class Config(C.Structure):
         ("slack_div", C.c_uint32),
         ("arena_headroom", C.c_double),
         ("group_size", C.c_uint32),
+        ("persistent", C.c_uint32),
     ]
 
 

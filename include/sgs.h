@@ -96,6 +96,11 @@ typedef struct sgs_config {
                              pass: 1..4 (narrow groups: lanes in one 32-B
                              sector) or 5..64 (wide groups: one 512-B row
                              per vertex, a warp's threads over the lanes) */
+  uint32_t persistent;    /* 1: every relaxation / invalidation phase runs
+                             as one cooperative launch looping over rounds
+                             with a grid barrier between them (no host read
+                             per batch of rounds); 0: rounds launched in
+                             batches with one counter read per batch       */
 } sgs_config;
 
 typedef struct sgs_query_stats {

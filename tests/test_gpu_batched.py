@@ -138,3 +138,32 @@ def test_add_many_narrow_groups_and_pagerank():
             check_query(q, m, sgs.W_EXPLICIT)
         with pytest.raises(sgs.SgsError):
             e.add_queries([(7, 0)])
+
+
+@pytest.mark.parametrize("gs", [4, 64])
+def test_persistent_launch_matches_batched_launches(gs):
+    """persistent=1 (each phase one cooperative launch looping over rounds)
+    gives the same values as rounds launched in batches, and the oracle."""
+    nv, row, col = O.rmat_csr(12, 16, 13)
+    w = O.weights(nv, row, col, 5, 0)
+    specs = _specs(nv, 6, 6, 2, 21)
+    i_s, i_d, iw, d_s, d_d = _stream(nv, row, col, 4, 3, 900, 5)
+    res = {}
+    for pers in (0, 1):
+        with sgs.Engine(group_size=gs, persistent=pers) as e:
+            e.load_csr(nv, row, col, w)
+            qs = e.add_queries(specs)
+            m = Mirror(nv, row, col, w)
+            out = [[q.value() for q in qs]]
+            for k in range(3):
+                sl = slice(k * 900, (k + 1) * 900)
+                e.apply_batch(i_s[sl], i_d[sl], iw[sl], d_s[sl], d_d[sl])
+                m.apply(i_s[sl], i_d[sl], iw[sl], d_s[sl], d_d[sl])
+                if pers:
+                    for q in qs:
+                        check_query(q, m, sgs.W_EXPLICIT)
+                out.append([q.value() for q in qs])
+            res[pers] = out
+    for a, b in zip(res[0], res[1]):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
