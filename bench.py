@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="skip sgs_autotune (by default it picks the relaxation map's CTAs per SM "
+                         "and the launch mode by timing a probe, before the timed region)")
     ap.add_argument("--persistent", type=int, default=None,
                     help="1: each relaxation phase as one cooperative launch over rounds")
     ap.add_argument("--workload", default="snapshot", choices=["snapshot", "ppr", "batched", "served"],
@@ -240,6 +243,7 @@ def engine_arm(a, R):
                                                nbatch * half)
     i_w = sgs.hash_weights(a.seed, i_s, i_d)
     del row, col
+    tune = e.autotune() if a.autotune else None
     queries = [e.add_query(sgs.SSSP, 0), e.add_query(sgs.BFS, 0), e.add_query(sgs.CC, 0)]
 
     def batch(k):
@@ -383,7 +387,8 @@ def engine_arm(a, R):
                    "l2": "inputs larger than L2 (edge arena %.1f GB vs %d MB L2)" % (
                        st["arena_bytes_hbm"] / 1e9, L2_BYTES // 2**20),
                    "parallelism": "replicas" if R.world > 1 else "single GPU",
-                   "queries": ["sssp:0", "bfs:0", "cc"]},
+                   "queries": ["sssp:0", "bfs:0", "cc"],
+                   "autotune": tune, "persistent": a.persistent},
         "e2e": e2e,
         "gpu_launches": gpu_launches,
         "roofline": roof,
@@ -512,6 +517,7 @@ def batched_arm(a, R):
         return dev_b[key]
 
     t_gen = time.time() - t0
+    tune = e.autotune() if a.autotune else None
     # static start of all queries together
     e.synchronize()
     ts = time.perf_counter()
@@ -603,7 +609,7 @@ def batched_arm(a, R):
         "config": {"workload": f"{a.batched_bfs} BFS + {a.batched_sssp} SSSP queries, R-MAT scale "
                                f"{a.batched_scale} ef {a.edge_factor} seed {a.seed}, {a.batched_updates} "
                                f"updates/snapshot (50/50), group_size {a.group_size}",
-                   "nv": nv, "largest_wcc": int(wcc),
+                   "nv": nv, "largest_wcc": int(wcc), "autotune": tune, "persistent": a.persistent,
                    "l2": "inputs larger than L2 (per-group state %.1f GB)" % (nv * 64 * 12 / 1e9),
                    "parallelism": "replicas" if R.world > 1 else "single GPU"},
         "e2e": e2e, "gpu_launches": launches, "roofline": roof, "clocks": clk,

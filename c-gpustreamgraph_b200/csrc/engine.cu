@@ -277,7 +277,8 @@ struct sgs_engine {
     return f;
   }
   unsigned long long *special(uint32_t k) { return cnt.p + cfg.max_rounds + 2 + k; }
-  uint32_t grid_map() const { return (uint32_t)nsm * 8; }
+  uint32_t map_cps = 16;  // CTAs per SM of the load-balanced maps (sgs_autotune)
+  uint32_t grid_map() const { return (uint32_t)nsm * map_cps; }
   uint32_t grid_elem(uint64_t n) const { return blocks_for(n, (uint32_t)nsm * 8); }
   size_t wbytes() const { return cfg.weight_mode == SGS_W_EXPLICIT ? 8 : 4; }
 
@@ -1175,6 +1176,47 @@ struct sgs_engine {
     fr = end;
   }
 
+  // ------------------------------------------------------------- autotune
+  // Times a probe -- the static convergence of SSSP, BFS and CC from vertex
+  // 0 in one group, device time from the engine's events -- for every pair
+  // of (CTAs per SM of the relaxation map, launch mode) and keeps the
+  // fastest.  Results do not depend on either choice.
+  void autotune(sgs_tune *out) {
+    if (!loaded) fail(SGS_ERR_STATE, "no graph loaded");
+    static const uint32_t cps[] = {4, 8, 16, 32};
+    const uint32_t keep_cps = map_cps, keep_pers = cfg.persistent;
+    double best = 1e300;
+    uint32_t bc = keep_cps, bp = keep_pers, tried = 0;
+    const int algos[3] = {SGS_SSSP, SGS_BFS, SGS_CC};
+    const uint32_t srcs[3] = {0, 0, 0};
+    for (uint32_t pers = 0; pers < 2; ++pers)
+      for (uint32_t c : cps) {
+        map_cps = c;
+        cfg.persistent = pers;
+        double t = 1e300;
+        for (int rep = 0; rep < 2; ++rep) {  // the first run also warms up
+          int ids[3];
+          add_queries(3, algos, srcs, ids);
+          t = std::min(t, find(ids[0]).stats.ms);
+          for (int id : ids) remove_query(id);
+        }
+        ++tried;
+        if (t < best) {
+          best = t;
+          bc = c;
+          bp = pers;
+        }
+      }
+    map_cps = bc;
+    cfg.persistent = bp;
+    (void)keep_cps;
+    (void)keep_pers;
+    out->ctas_per_sm = bc;
+    out->persistent = bp;
+    out->best_ms = best;
+    out->tried = tried;
+  }
+
   // Frees the state of groups without lanes in use; true if any was freed.
   bool release_empty_groups() {
     bool any = false;
@@ -2054,6 +2096,14 @@ SGS_API void sgs_hash_weights(uint64_t wseed, uint64_t n, const uint32_t *src, c
   const uint64_t key = h_mix64(wseed ^ 0x57454947ull);
   for (uint64_t i = 0; i < n; ++i)
     w[i] = 1u + (uint32_t)(h_fin64(key ^ (((uint64_t)src[i] << 32) | dst[i])) >> 58);
+}
+
+SGS_API int sgs_autotune(sgs_engine *e, sgs_tune *out) {
+  if (!e || !out) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    e->autotune(out);
+  });
 }
 
 SGS_API int sgs_kernel_timing(sgs_engine *e, int enable) {

@@ -50,7 +50,7 @@ EXPORTS = [
     "sgs_read_edge_list", "sgs_read_stream_sizes", "sgs_read_update_file", "sgs_free",
     "sgs_ppr_create_csr", "sgs_ppr_create", "sgs_ppr_destroy", "sgs_ppr_info",
     "sgs_ppr_export", "sgs_ppr_forward", "sgs_ppr_backward", "sgs_ppr_timing",
-    "sgs_ppr_get_stats", "sgs_serve",
+    "sgs_ppr_get_stats", "sgs_serve", "sgs_autotune",
 ]
 
 K_GROUP, K_GROUP_INVAL, K_PR_PUSH, K_WIDE, K_WIDE_INVAL = range(5)
@@ -160,6 +160,11 @@ class Completion(C.Structure):
     ]
 
 
+class Tune(C.Structure):
+    _fields_ = [("ctas_per_sm", C.c_uint32), ("persistent", C.c_uint32), ("best_ms", C.c_double),
+                ("tried", C.c_uint32)]
+
+
 class PprStats(C.Structure):
     _fields_ = [
         ("iters", C.c_int32),
@@ -228,6 +233,7 @@ def lib():
     L.sgs_ppr_backward.argtypes = [vp, vp, vp, vp, u32, dbl, dbl, u32, vp, vp, C.POINTER(i32), i32]
     L.sgs_ppr_timing.argtypes = [vp, i32]
     L.sgs_serve.argtypes = [vp, C.POINTER(Request), u32, u32, i32, C.POINTER(Completion)]
+    L.sgs_autotune.argtypes = [vp, C.POINTER(Tune)]
     L.sgs_ppr_get_stats.argtypes = [vp, C.POINTER(PprStats)]
     for name in EXPORTS:
         if name not in ("sgs_version", "sgs_last_error", "sgs_config_default",
@@ -459,6 +465,14 @@ class Engine:
                         "latency_s": c.done_s - (arr[i].arrival_s if realtime else 0.0),
                         "summary": list(c.summary), "edges": c.edges})
         return res
+
+    def autotune(self):
+        """sgs_autotune: picks the relaxation map's CTAs per SM and the launch
+        mode by timing a probe on the loaded graph; returns the choice."""
+        t = Tune()
+        _check(lib().sgs_autotune(self.h, C.byref(t)))
+        return {"ctas_per_sm": t.ctas_per_sm, "persistent": t.persistent, "best_ms": t.best_ms,
+                "tried": t.tried}
 
     def remove_query(self, q):
         _check(lib().sgs_query_remove(self.h, q.qid if isinstance(q, Query) else q))

@@ -257,6 +257,20 @@ SGS_API void sgs_free(void *p);
 
 SGS_API int sgs_kernel_timing(sgs_engine *e, int enable);
 
+/* Autotuner (no counterpart in the reference): on the loaded graph, times a
+ * probe -- the static convergence of SSSP, BFS and CC from vertex 0 sharing
+ * one group -- for each CTAs-per-SM count of the load-balanced relaxation
+ * map (4, 8, 16, 32; default 16) and each launch mode (batched rounds or one persistent
+ * launch), and keeps the fastest pair for the engine's later work.  The
+ * choices change speed only, never results.  Costs 16 static convergences. */
+typedef struct sgs_tune {
+  uint32_t ctas_per_sm;   /* chosen CTAs per SM of the relaxation map       */
+  uint32_t persistent;    /* chosen launch mode (sgs_config.persistent)     */
+  double best_ms;         /* device time of the probe with that choice      */
+  uint32_t tried;         /* combinations timed                             */
+} sgs_tune;
+SGS_API int sgs_autotune(sgs_engine *e, sgs_tune *out);
+
 /* From-scratch SSSP (w != NULL) or BFS (w == NULL) over a CSR that the caller
  * already holds in device memory (row: nv+1 u64 offsets, col/w: row[nv] u32),
  * writing dist[nv] and, if parent != NULL, parent[nv] (device pointers) on

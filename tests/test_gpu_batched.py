@@ -167,3 +167,21 @@ def test_persistent_launch_matches_batched_launches(gs):
     for a, b in zip(res[0], res[1]):
         for x, y in zip(a, b):
             assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("gs", [4, 64])
+def test_autotune_picks_a_setting_and_keeps_results(gs):
+    nv, row, col = O.rmat_csr(12, 16, 17)
+    w = O.weights(nv, row, col, 2, 0)
+    i_s, i_d, iw, d_s, d_d = _stream(nv, row, col, 6, 1, 800, 2)
+    with sgs.Engine(group_size=gs) as e:
+        e.load_csr(nv, row, col, w)
+        t = e.autotune()
+        assert t["tried"] == 8 and t["ctas_per_sm"] in (4, 8, 16, 32) and t["persistent"] in (0, 1)
+        assert t["best_ms"] > 0
+        qs = e.add_queries(_specs(nv, 3, 3, 1, 8))
+        e.apply_batch(i_s, i_d, iw, d_s, d_d)
+        m = Mirror(nv, row, col, w)
+        m.apply(i_s, i_d, iw, d_s, d_d)
+        for q in qs:
+            check_query(q, m, sgs.W_EXPLICIT)
