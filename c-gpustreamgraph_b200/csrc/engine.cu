@@ -277,7 +277,7 @@ struct sgs_engine {
     return f;
   }
   unsigned long long *special(uint32_t k) { return cnt.p + cfg.max_rounds + 2 + k; }
-  uint32_t map_cps = 16;  // CTAs per SM of the load-balanced maps (sgs_autotune)
+  uint32_t map_cps = 32;  // CTAs per SM of the load-balanced maps (sgs_autotune)
   uint32_t grid_map() const { return (uint32_t)nsm * map_cps; }
   uint32_t grid_elem(uint64_t n) const { return blocks_for(n, (uint32_t)nsm * 8); }
   size_t wbytes() const { return cfg.weight_mode == SGS_W_EXPLICIT ? 8 : 4; }

@@ -260,7 +260,7 @@ SGS_API int sgs_kernel_timing(sgs_engine *e, int enable);
 /* Autotuner (no counterpart in the reference): on the loaded graph, times a
  * probe -- the static convergence of SSSP, BFS and CC from vertex 0 sharing
  * one group -- for each CTAs-per-SM count of the load-balanced relaxation
- * map (4, 8, 16, 32; default 16) and each launch mode (batched rounds or one persistent
+ * map (4, 8, 16, 32; default 32) and each launch mode (batched rounds or one persistent
  * launch), and keeps the fastest pair for the engine's later work.  The
  * choices change speed only, never results.  Costs 16 static convergences. */
 typedef struct sgs_tune {
