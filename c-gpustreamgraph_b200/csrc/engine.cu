@@ -755,7 +755,7 @@ struct sgs_engine {
       WideRelaxOp<> op{G.st.p, G.val.p, G.walgo()};
       WideRelaxOp<true> op0{G.st.p, G.val.p, G.walgo()};
       op0.only = only0;
-      if (cfg.persistent) {
+      if (cfg.persistent & 1u) {
         if (!only0 && !after0) return run_wide_persistent(op, 0, conv, SGS_K_WIDE, anyw ? 8.0 : 4.0, nullptr);
         // round 0 (restricted) and its hook as plain launches, then one launch
         CK(cudaMemsetAsync(rstat.p, 0, sizeof(unsigned long long) * (cfg.max_rounds + 2), s));
@@ -771,7 +771,7 @@ struct sgs_engine {
       return run_wide_rounds(op, op, conv, SGS_K_WIDE, anyw ? 8.0 : 4.0, nullptr, round0, after0);
     }
     const uint32_t anyw = G.any_sssp(G.used | 0xF) && cfg.weight_mode == SGS_W_EXPLICIT;
-    if (cfg.persistent && !after0) {
+    if ((cfg.persistent & 1u) && !after0) {
       if (round0) nvtxRangePushA(round0);
       const uint32_t r = run_group_persistent(
           GroupRelaxOp<GMAX>{g, G.st.p, G.val.p, nullptr, nullptr, G.algo(), anyw}, 0, conv, SGS_K_GROUP,
@@ -1192,7 +1192,7 @@ struct sgs_engine {
     for (uint32_t pers = 0; pers < 2; ++pers)
       for (uint32_t c : cps) {
         map_cps = c;
-        cfg.persistent = pers;
+        cfg.persistent = (keep_pers & 2u) | pers;
         double t = 1e300;
         for (int rep = 0; rep < 2; ++rep) {  // the first run also warms up
           int ids[3];
@@ -1208,11 +1208,11 @@ struct sgs_engine {
         }
       }
     map_cps = bc;
-    cfg.persistent = bp;
+    cfg.persistent = (keep_pers & 2u) | bp;
     (void)keep_cps;
     (void)keep_pers;
     out->ctas_per_sm = bc;
-    out->persistent = bp;
+    out->persistent = cfg.persistent;
     out->best_ms = best;
     out->tried = tried;
   }
@@ -1367,14 +1367,14 @@ struct sgs_engine {
         CK(cudaGetLastError());
         WideInvalidateOp op{G.st.p, G.val.p, WideAlgo{0ull, G.cc}};  // no weights needed
         op.mark = G.ibits.p;
-        if (cfg.persistent) run_wide_persistent(op, 0, conv, SGS_K_WIDE_INVAL, 4.0, b_inval.p);
+        if (cfg.persistent & 2u) run_wide_persistent(op, 0, conv, SGS_K_WIDE_INVAL, 4.0, b_inval.p);
         else run_wide_rounds(op, op, conv, SGS_K_WIDE_INVAL, 4.0, b_inval.p);
       } else {
         { ++n_launch; k_group_seed_deleted<GMAX><<<grid_elem(nd), 256, 0, s>>>(
             g, G.st.p, G.val.p, (uint32_t)G.used, G.algo(), b_dkeys_s.p, (uint32_t)nd, b_inval.p,
             nullptr, gm[0].p, fview(0, cnt.p)); }
         CK(cudaGetLastError());
-        if (cfg.persistent)
+        if (cfg.persistent & 2u)
           run_group_persistent(GroupInvalidateOp<GMAX>{g, G.st.p, G.val.p, nullptr, nullptr, G.algo(),
                                                        b_inval.p, nullptr},
                                0, conv, SGS_K_GROUP_INVAL, 4.0);
@@ -1796,7 +1796,7 @@ SGS_API void sgs_config_default(sgs_config *c) {
   c->slack_div = 8;
   c->arena_headroom = 0.30;
   c->group_size = 4;
-  c->persistent = 0;
+  c->persistent = 2;  // invalidation phases persistent: many small rounds
 }
 
 SGS_API int sgs_create(const sgs_config *cfg, sgs_engine **out) {

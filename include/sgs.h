@@ -96,11 +96,13 @@ typedef struct sgs_config {
                              pass: 1..4 (narrow groups: lanes in one 32-B
                              sector) or 5..64 (wide groups: one 512-B row
                              per vertex, a warp's threads over the lanes) */
-  uint32_t persistent;    /* 1: every relaxation / invalidation phase runs
-                             as one cooperative launch looping over rounds
-                             with a grid barrier between them (no host read
-                             per batch of rounds); 0: rounds launched in
-                             batches with one counter read per batch       */
+  uint32_t persistent;    /* bit 0: relaxation phases, bit 1: invalidation
+                             phases run as one cooperative launch looping
+                             over rounds with a grid barrier between them
+                             (no host read per batch of rounds); a clear bit:
+                             rounds launched in batches with one counter
+                             read per batch.  Default 2: the invalidation's
+                             many small rounds gain most                  */
 } sgs_config;
 
 typedef struct sgs_query_stats {
@@ -265,7 +267,7 @@ SGS_API int sgs_kernel_timing(sgs_engine *e, int enable);
  * choices change speed only, never results.  Costs 16 static convergences. */
 typedef struct sgs_tune {
   uint32_t ctas_per_sm;   /* chosen CTAs per SM of the relaxation map       */
-  uint32_t persistent;    /* chosen launch mode (sgs_config.persistent)     */
+  uint32_t persistent;    /* resulting sgs_config.persistent (bit 0 tuned)  */
   double best_ms;         /* device time of the probe with that choice      */
   uint32_t tried;         /* combinations timed                             */
 } sgs_tune;

@@ -149,7 +149,7 @@ def test_persistent_launch_matches_batched_launches(gs):
     specs = _specs(nv, 6, 6, 2, 21)
     i_s, i_d, iw, d_s, d_d = _stream(nv, row, col, 4, 3, 900, 5)
     res = {}
-    for pers in (0, 1):
+    for pers in (0, 1, 2, 3):
         with sgs.Engine(group_size=gs, persistent=pers) as e:
             e.load_csr(nv, row, col, w)
             qs = e.add_queries(specs)
@@ -164,9 +164,10 @@ def test_persistent_launch_matches_batched_launches(gs):
                         check_query(q, m, sgs.W_EXPLICIT)
                 out.append([q.value() for q in qs])
             res[pers] = out
-    for a, b in zip(res[0], res[1]):
-        for x, y in zip(a, b):
-            assert np.array_equal(x, y)
+    for p in (1, 2, 3):
+        for a, b in zip(res[0], res[p]):
+            for x, y in zip(a, b):
+                assert np.array_equal(x, y)
 
 
 @pytest.mark.parametrize("gs", [4, 64])
@@ -177,7 +178,7 @@ def test_autotune_picks_a_setting_and_keeps_results(gs):
     with sgs.Engine(group_size=gs) as e:
         e.load_csr(nv, row, col, w)
         t = e.autotune()
-        assert t["tried"] == 8 and t["ctas_per_sm"] in (4, 8, 16, 32) and t["persistent"] in (0, 1)
+        assert t["tried"] == 8 and t["ctas_per_sm"] in (4, 8, 16, 32) and t["persistent"] in (0, 1, 2, 3)
         assert t["best_ms"] > 0
         qs = e.add_queries(_specs(nv, 3, 3, 1, 8))
         e.apply_batch(i_s, i_d, iw, d_s, d_d)
