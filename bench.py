@@ -53,6 +53,11 @@ def parse():
     ap.add_argument("--edge-factor", type=int, default=16)
     ap.add_argument("--updates", type=int, default=1_000_000)
     ap.add_argument("--budget-gb", type=float, default=4.0)
+    ap.add_argument("--permute", action="store_true",
+                    help="relabel the R-MAT vertices by a seeded random permutation (hubs spread over "
+                         "all segments); the source is vertex 0's new label")
+    ap.add_argument("--cache-gb", type=float, default=0.0,
+                    help="device edge cache of the host tier, carved out of --budget-gb (0: none)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-e2e", action="store_true")
@@ -222,6 +227,20 @@ def profile_traffic():
         return None
 
 
+def permute_graph(e, seed):
+    """Reloads the engine's graph with vertex v relabelled p[v] (p a seeded
+    random permutation, as the reference's unused GAP generator permutes,
+    include/framework/generator.h:53-63); returns p[0]."""
+    row, col, w = e.export(weights=True)
+    nv = len(row) - 1
+    p = np.random.default_rng(seed * 7919 + 17).permutation(nv).astype(np.uint32)
+    src = p[np.repeat(np.arange(nv, dtype=np.uint32), np.diff(row).astype(np.int64))]
+    dst = p[col]
+    del row, col
+    e.load_edge_list(src, dst, w, nv=nv)
+    return int(p[0])
+
+
 # ----------------------------------------------------------------- engine arm
 def engine_arm(a, R):
     import torch
@@ -230,9 +249,13 @@ def engine_arm(a, R):
 
     dev = torch.device("cuda", R.local)
     torch.cuda.set_device(dev)
-    e = sgs.Engine(device=R.local, hbm_budget_gb=a.budget_gb, weight_mode=sgs.W_EXPLICIT, **pers(a))
+    e = sgs.Engine(device=R.local, hbm_budget_gb=a.budget_gb, cache_gb=a.cache_gb,
+                   weight_mode=sgs.W_EXPLICIT, **pers(a))
     t0 = time.time()
     e.load_rmat(a.scale, a.edge_factor, a.seed, 0.57, 0.19, 0.19, wseed=a.seed)
+    source = 0
+    if a.permute:
+        source = permute_graph(e, a.seed)
     t_gen = time.time() - t0
     st0 = e.engine_stats()
     nv = int(st0["nv"])
@@ -244,7 +267,8 @@ def engine_arm(a, R):
     i_w = sgs.hash_weights(a.seed, i_s, i_d)
     del row, col
     tune = e.autotune() if a.autotune else None
-    queries = [e.add_query(sgs.SSSP, 0), e.add_query(sgs.BFS, 0), e.add_query(sgs.CC, 0)]
+    queries = [e.add_query(sgs.SSSP, source), e.add_query(sgs.BFS, source), e.add_query(sgs.CC, 0)]
+    e.cache_refresh()  # warm the edge cache after the static run (no-op without one)
 
     def batch(k):
         s = slice(k * half, (k + 1) * half)
@@ -269,7 +293,8 @@ def engine_arm(a, R):
     R.barrier()
     torch.cuda.synchronize()
     e.synchronize()
-    launches0 = e.engine_stats()["kernel_launches"]
+    cs0 = e.engine_stats()
+    launches0 = cs0["kernel_launches"]
     clocks.start()
     w0 = time.perf_counter()
     edges = 0
@@ -286,10 +311,20 @@ def engine_arm(a, R):
     R.barrier()
     wall_ms = (time.perf_counter() - w0) * 1e3
     clk = clocks.stop()
-    gpu_launches = int(e.engine_stats()["kernel_launches"] - launches0)
+    cs1 = e.engine_stats()
+    gpu_launches = int(cs1["kernel_launches"] - launches0)
     kst = e.kernel_stats()
     e.kernel_timing(False)
     del dev_batches
+    cache = None
+    if cs1["cache_lines"]:
+        hit = cs1["cache_hit_slots"] - cs0["cache_hit_slots"]
+        miss = cs1["cache_miss_slots"] - cs0["cache_miss_slots"]
+        cache = {"gb": a.cache_gb, "lines": int(cs1["cache_lines"]), "resident": int(cs1["cache_resident"]),
+                 "admissions": int(cs1["cache_admissions"] - cs0["cache_admissions"]),
+                 "last_admitted": int(cs1["last_admitted"]), "last_evicted": int(cs1["last_evicted"]),
+                 "host_tier_slots_timed": int(hit + miss),
+                 "hit_fraction": round(hit / max(hit + miss, 1), 4)}
     # ---------------- e2e (host pinned inputs, summaries read back)
     e2e = None
     if not a.no_e2e:
@@ -324,7 +359,7 @@ def engine_arm(a, R):
     # ---------------- full-size self check: incremental == from-scratch
     # (parents are not unique, so the check compares reached count, value sum
     # and max value)
-    fresh = [e.add_query(sgs.SSSP, 0), e.add_query(sgs.BFS, 0), e.add_query(sgs.CC, 0)]
+    fresh = [e.add_query(sgs.SSSP, source), e.add_query(sgs.BFS, source), e.add_query(sgs.CC, 0)]
     selfcheck = {}
     for name, q, f in zip(("sssp", "bfs", "cc"), queries, fresh):
         selfcheck[name] = bool(np.array_equal(q.summary()[:3], f.summary()[:3]))
@@ -379,7 +414,9 @@ def engine_arm(a, R):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (device R-MAT, seeded weights and update stream)",
         "config": {"workload": f"incremental SSSP/BFS/CC, R-MAT scale {a.scale} ef {a.edge_factor} seed {a.seed}, "
-                               f"{a.updates} updates/snapshot (50/50), source 0, HBM budget {a.budget_gb} GB",
+                               f"{a.updates} updates/snapshot (50/50), source 0, HBM budget {a.budget_gb} GB"
+                               + (f" ({a.cache_gb} GB of it as edge cache)" if a.cache_gb > 0 else "")
+                               + (", vertex ids randomly permuted" if getattr(a, "permute", False) else ""),
                    "nv": nv, "ne_initial": int(st0["ne"]), "ne_final": int(st["ne"]),
                    "hbm_resident_fraction": st["hbm_resident_vertices"] / max(nv, 1),
                    "arena_bytes_hbm": int(st["arena_bytes_hbm"]),
@@ -388,7 +425,7 @@ def engine_arm(a, R):
                        st["arena_bytes_hbm"] / 1e9, L2_BYTES // 2**20),
                    "parallelism": "replicas" if R.world > 1 else "single GPU",
                    "queries": ["sssp:0", "bfs:0", "cc"],
-                   "autotune": tune, "persistent": a.persistent},
+                   "autotune": tune, "persistent": a.persistent, "edge_cache": cache},
         "e2e": e2e,
         "gpu_launches": gpu_launches,
         "roofline": roof,
@@ -975,7 +1012,8 @@ def reference_arm(a, R):
         "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (CPU R-MAT and update stream, same graph and stream as the engine arm)",
         "config": {"workload": f"incremental SSSP/BFS/CC, R-MAT scale {a.scale} ef {a.edge_factor} seed {a.seed}, "
-                               f"{a.updates} updates/snapshot (50/50), source 0, HBM budget {a.budget_gb} GB",
+                               f"{a.updates} updates/snapshot (50/50), source 0, HBM budget {a.budget_gb} GB"
+                               + (f" ({a.cache_gb} GB of it as edge cache)" if a.cache_gb > 0 else ""),
                    "nv": nv, "setup_s": round(setup_s, 1)},
         "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": "per snapshot: the reference's BFSHost (compiled from its sources) from "

@@ -141,6 +141,11 @@ int main(int argc, char **argv) {
     sgs_query_stats st = engine.Stats();
     std::printf("static: %u rounds, %llu edges, %.3f ms\n", st.rounds,
                 (unsigned long long)st.edges_traversed, st.ms);
+    // the reference warms its edge cache here (compute_hot_vertices_*,
+    // confirm_candidate_batch, LoadCache; hybrid_sssp.cu:252-254)
+    engine.compute_hot_vertices_sssp();
+    engine.confirm_candidate_batch();
+    engine.LoadCache();
     const std::string us = f.get("update_size"), uf = f.get("updatefile");
     if (!us.empty() && !uf.empty()) {
       engine.get_update_file(us, uf);

@@ -28,6 +28,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include "../../include/sgs.h"
+#include "sgs_cache.cuh"
 #include "sgs_group.cuh"
 #include "sgs_kernels.cuh"
 #include "sgs_wide.cuh"
@@ -245,7 +246,30 @@ struct sgs_engine {
   sgs_engine_stats est{};
   Events ev_batch, ev_apply, ev_q;
 
+  // device edge cache of the host tier (sgs_cache.cuh): lines of CLINE
+  // slots admitted per snapshot by hotness, copied on a side stream
+  bool cache_on = false;
+  uint64_t c_lines = 0;                // capacity (lines)
+  uint64_t h_lines = 0;                // lines of the host arena (cmap entries)
+  uint64_t cbase = 0;                  // cached lines: adj_d/wgt_d slots [cbase, cbase + c_lines*CLINE)
+  DBuf<uint32_t> cmap, cown;           // host line -> cache line, cache line -> host line
+  DBuf<uint32_t> cscore, chist, c_new, c_free;
+  DBuf<uint2> c_pend;                  // (host line, cache line) of the last admission
+  DBuf<unsigned long long> c_cc;       // counters (CC_*)
+  DBuf<uint32_t> hot;                  // per vertex: four u8 activation counters
+  uint32_t hot_k = 0;                  // the byte the current snapshot fills
+  cudaStream_t s2 = nullptr;           // side stream of the line copies
+  cudaEvent_t ev_cadmit = nullptr, ev_ccopy = nullptr;
+  bool c_pending = false;              // copies issued, lines not yet published
+  uint64_t c_admissions = 0;
+
   ~sgs_engine() {
+    if (s2) {
+      cudaStreamSynchronize(s2);
+      cudaStreamDestroy(s2);
+    }
+    if (ev_cadmit) cudaEventDestroy(ev_cadmit);
+    if (ev_ccopy) cudaEventDestroy(ev_ccopy);
     for (auto ev : kev) cudaEventDestroy(ev);
     for (auto ev : gev) cudaEventDestroy(ev);
     if (h_cnt) cudaFreeHost(h_cnt);
@@ -253,7 +277,7 @@ struct sgs_engine {
   }
 
   GraphView view() {
-    GraphView g;
+    GraphView g{};
     g.nv = nv;
     g.off = off.p;
     g.slots = slots.p;
@@ -264,6 +288,15 @@ struct sgs_engine {
     g.adj_h = adj_h.p;
     g.wgt_h = wgt_h.p;
     g.wmode = cfg.weight_mode;
+    if (cache_on && h_lines) {
+      g.cmap = cmap.p;
+      g.adj_c = adj_d.p + cbase;
+      g.wgt_c = wgt_d.p ? wgt_d.p + cbase : nullptr;
+      g.cbase = cbase;
+      g.hot = hot.p;
+      g.hot_sh = 8 * hot_k;
+      g.cstat = c_cc.p;
+    }
     return g;
   }
   FrontierView fview(uint32_t buf, unsigned long long *counter) {
@@ -313,6 +346,96 @@ struct sgs_engine {
     ev_batch.init();
     ev_apply.init();
     ev_q.init();
+    cache_init();
+  }
+
+  // ------------------------------------------------------------ edge cache
+  // On when both an HBM budget and a cache size are given: the cache is
+  // carved out of the budget (the static HBM tier gets the rest).
+  void cache_init() {
+    if (!(cfg.cache_gb > 0 && cfg.hbm_budget_gb > 0)) return;
+    c_lines = (uint64_t)(cfg.cache_gb * 1e9 / (double)(CLINE * wbytes()));
+    if (c_lines == 0) return;
+    if (c_lines >= NO_LINE) fail(SGS_ERR_INVALID, "cache_gb too large");
+    cache_on = true;
+    cown.ensure(c_lines);
+    c_new.ensure(c_lines);
+    c_free.ensure(c_lines);
+    c_pend.ensure(c_lines);
+    chist.ensure(HOT_BINS);
+    c_cc.ensure(CC_N);
+    CK(cudaMemsetAsync(cown.p, 0xFF, sizeof(uint32_t) * c_lines, s));
+    CK(cudaMemsetAsync(c_cc.p, 0, sizeof(unsigned long long) * CC_N, s));
+    CK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ev_cadmit, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_ccopy, cudaEventDisableTiming));
+  }
+  double static_budget_gb() const {
+    return cache_on ? std::max(0.0, cfg.hbm_budget_gb - cfg.cache_gb) : cfg.hbm_budget_gb;
+  }
+  // Waits for copies in flight (before arenas are reallocated).
+  void cache_quiesce() {
+    if (!cache_on) return;
+    CK(cudaStreamSynchronize(s2));
+    c_pending = false;
+  }
+  // A new host arena of cap_h slots: every line dropped; a new graph also
+  // starts a new hotness window.
+  void cache_layout(uint64_t cap_h) {
+    if (!cache_on) return;
+    cache_quiesce();
+    h_lines = (cap_h + CLINE - 1) / CLINE;
+    cmap.ensure(std::max<uint64_t>(h_lines, 1));
+    cscore.ensure(std::max<uint64_t>(h_lines, 1));
+    if (h_lines) CK(cudaMemsetAsync(cmap.p, 0xFF, sizeof(uint32_t) * h_lines, s));
+    CK(cudaMemsetAsync(cown.p, 0xFF, sizeof(uint32_t) * c_lines, s));
+    if (!loaded) {
+      hot.ensure(nv);
+      CK(cudaMemsetAsync(hot.p, 0, sizeof(uint32_t) * nv, s));
+      hot_k = 0;
+      CK(cudaMemsetAsync(c_cc.p, 0, sizeof(unsigned long long) * CC_N, s));
+    }
+  }
+  // Makes the lines of the last admission visible once their copy is done
+  // (the main stream waits for the side stream).
+  void cache_publish() {
+    if (!c_pending) return;
+    CK(cudaStreamWaitEvent(s, ev_ccopy, 0));
+    { ++n_launch; k_cache_publish<<<grid_elem(c_lines), 256, 0, s>>>(c_pend.p, c_cc.p, cmap.p); }
+    CK(cudaGetLastError());
+    c_pending = false;
+  }
+  // Admission from the hotness window (advanced by one snapshot when
+  // `rotate`): evictions, new lines paired with free cache lines, and their
+  // copies on the side stream, which overlap whatever the main stream runs
+  // next.  The lines become visible at the next cache_publish.
+  void cache_admit(bool rotate) {
+    if (!cache_on || !h_lines) return;
+    cache_publish();  // every owned cache line mapped before the keep pass
+    const uint32_t next = (hot_k + 1) & 3u;
+    CK(cudaMemsetAsync(cscore.p, 0, sizeof(uint32_t) * h_lines, s));
+    CK(cudaMemsetAsync(chist.p, 0, sizeof(uint32_t) * HOT_BINS, s));
+    CK(cudaMemsetAsync(c_cc.p + CC_TICK, 0, sizeof(unsigned long long) * (CC_N - CC_TICK), s));
+    const GraphView g = view();
+    { ++n_launch; k_cache_score<<<grid_elem(nv), 256, 0, s>>>(g, rotate ? 8 * next : 32u, cscore.p, h_lines); }
+    if (rotate) hot_k = next;
+    { ++n_launch; k_cache_hist<<<grid_elem(h_lines), 256, 0, s>>>(cscore.p, h_lines, chist.p); }
+    { ++n_launch; k_cache_threshold<<<1, 1024, 0, s>>>(chist.p, c_lines, c_cc.p); }
+    { ++n_launch; k_cache_keep<<<grid_elem(c_lines), 256, 0, s>>>(cmap.p, cown.p, cscore.p, c_lines, c_cc.p); }
+    { ++n_launch; k_cache_pick<<<grid_elem(h_lines), 256, 0, s>>>(cmap.p, cscore.p, h_lines, c_lines, c_new.p,
+                                                      c_cc.p); }
+    { ++n_launch; k_cache_free<<<grid_elem(c_lines), 256, 0, s>>>(cown.p, c_lines, c_free.p, c_cc.p); }
+    { ++n_launch; k_cache_pair<<<grid_elem(c_lines), 256, 0, s>>>(c_new.p, c_free.p, c_lines, cown.p, c_pend.p,
+                                                      c_cc.p); }
+    CK(cudaEventRecord(ev_cadmit, s));
+    CK(cudaStreamWaitEvent(s2, ev_cadmit, 0));
+    { ++n_launch; k_cache_copy<<<(uint32_t)nsm * 4, 256, 0, s2>>>(
+        c_pend.p, c_cc.p, adj_h.p, cfg.weight_mode == SGS_W_EXPLICIT ? wgt_h.p : nullptr,
+        adj_d.p + cbase, cfg.weight_mode == SGS_W_EXPLICIT ? wgt_d.p + cbase : nullptr); }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ev_ccopy, s2));
+    c_pending = true;
+    ++c_admissions;
   }
 
   // ------------------------------------------------------------- graph load
@@ -373,6 +496,7 @@ struct sgs_engine {
   // with slack, offsets, tier split, arena allocation.  Leaves off/cap set and
   // the arenas allocated but empty; returns nothing (fills members).
   void layout_from(const uint32_t *sz, uint64_t extra) {
+    cache_quiesce();
     DBuf<uint64_t> scan;
     scan.ensure((size_t)nv + 1);
     { ++n_launch; k_layout_caps<<<grid_elem(nv), 256, 0, s>>>(sz, nv, cfg.slack_div, cap.p); }
@@ -389,7 +513,7 @@ struct sgs_engine {
     // tier split on segment boundaries
     uint32_t sp = nv;
     if (cfg.hbm_budget_gb > 0) {
-      const double budget_slots = cfg.hbm_budget_gb * 1e9 / (double)wbytes();
+      const double budget_slots = static_budget_gb() * 1e9 / (double)wbytes();
       const double usable = budget_slots / (1.0 + std::max(0.0, cfg.arena_headroom));
       const uint32_t nseg = std::max<uint32_t>(1, cfg.segments);
       // segment s = vertices [b_s, b_{s+1}) with ~total/nseg slots each
@@ -401,28 +525,37 @@ struct sgs_engine {
         uint32_t b = sg == nseg ? nv
                                 : (uint32_t)(std::lower_bound(hs.begin(), hs.end(), target) - hs.begin());
         b = std::min(b, nv);
-        if ((double)hs[b] <= usable) sp = b;
+        // the resident blocks plus the room asked for relocations must fit
+        if ((double)hs[b] + (double)extra <= usable) sp = b;
         else break;
       }
     }
     split = sp;
     const double hr = std::max(0.0, cfg.arena_headroom);
     uint64_t need_d = hs[sp], need_h = total - hs[sp];
-    uint64_t cap_d = need_d + (uint64_t)(need_d * hr) + 4096 + (sp == nv ? extra : 0);
+    uint64_t cap_d = need_d + (uint64_t)(need_d * hr) + 4096 + (sp > 0 ? extra : 0);
     uint64_t cap_h = need_h ? need_h + (uint64_t)(need_h * hr) + 4096 + extra : 0;
     if (cfg.hbm_budget_gb > 0) {
-      const uint64_t budget_slots = (uint64_t)(cfg.hbm_budget_gb * 1e9 / (double)wbytes());
+      const uint64_t budget_slots = (uint64_t)(static_budget_gb() * 1e9 / (double)wbytes());
       cap_d = std::min(cap_d, std::max(budget_slots, need_d));
       if (sp < nv && cap_h < need_h + extra) cap_h = need_h + extra + 4096;
     }
-    adj_d.ensure(cap_d);
-    if (cfg.weight_mode == SGS_W_EXPLICIT) wgt_d.ensure(cap_d);
+    cap_h = (cap_h + CLINE - 1) / CLINE * CLINE;  // whole cache lines
+    // the HBM arena, then (with the edge cache) the cache lines after it, so
+    // a block held in one cached line reads like an HBM block; the lines
+    // start on a line boundary (cap_d itself need not be a multiple of 4,
+    // and the quads read from a line are 16-B loads)
+    cbase = (cap_d + CLINE - 1) / CLINE * CLINE;
+    const uint64_t cache_slots = cache_on ? c_lines * CLINE : 0;
+    adj_d.ensure(cbase + cache_slots);
+    if (cfg.weight_mode == SGS_W_EXPLICIT) wgt_d.ensure(cbase + cache_slots);
     if (cap_h) {
       adj_h.ensure(cap_h);
       if (cfg.weight_mode == SGS_W_EXPLICIT) wgt_h.ensure(cap_h);
     }
     arena_cap[0] = cap_d;
     arena_cap[1] = cap_h;
+    cache_layout(cap_h);
     { ++n_launch; k_assign_off<<<grid_elem(nv), 256, 0, s>>>(scan.p, nv, sp, hs[sp], off.p); }
     unsigned long long tops[2] = {need_d, need_h};
     CK(cudaMemcpyAsync(arena_top.p, tops, sizeof(tops), cudaMemcpyHostToDevice, s));
@@ -458,6 +591,7 @@ struct sgs_engine {
   // Repack: fresh arenas sized from the current slot counts (+extra room),
   // every block copied (tombstones included).
   void repack(uint64_t extra) {
+    cache_quiesce();  // no line copy may read the old host arena
     DBuf<uint64_t> old_off;
     old_off.ensure(nv);
     CK(cudaMemcpyAsync(old_off.p, off.p, sizeof(uint64_t) * nv, cudaMemcpyDeviceToDevice, s));
@@ -1400,6 +1534,9 @@ struct sgs_engine {
       apply_graph(ni, nd);
     }
     CK(cudaEventRecord(ev_apply.b, s));
+    // ---- edge cache: admission from the hotness window; the copies run on
+    // the side stream under the repair below
+    cache_admit(/*rotate=*/true);
     g = view();
 
     // ---- PR compensate over the new out-lists, then convergence
@@ -1489,6 +1626,7 @@ struct sgs_engine {
       CK(cudaMemcpyAsync(G.dstat.p + 2 * WLANES, b_lane.p, sizeof(unsigned long long) * WLANES,
                          cudaMemcpyDeviceToDevice, s));
     }
+    cache_publish();  // the snapshot ends when its line copies are visible
     // per-lane counters of every group, one read
     h_gstat.resize(3 * WLANES * std::max<size_t>(ng, 1));
     for (size_t i = 0; i < ng; ++i)
@@ -1550,6 +1688,7 @@ struct sgs_engine {
   // block is relocated (capacity x1.5) within its tier; the arena is repacked
   // first when the relocations would not fit.
   void apply_graph(uint64_t ni, uint64_t nd) {
+    cache_publish();  // no line copy may run while blocks are written (through)
     GraphView g = view();
     unsigned long long *tombs = b_stat.p + 2;
     CK(cudaMemsetAsync(tombs, 0, sizeof(unsigned long long), s));
@@ -1999,7 +2138,30 @@ SGS_API int sgs_get_engine_stats(sgs_engine *e, sgs_engine_stats *out) {
       CK(cudaStreamSynchronize(e->s));
     }
     e->est.slots = e->slots_total;
+    if (e->cache_on) {
+      unsigned long long cc[CC_N];
+      CK(cudaMemcpyAsync(cc, e->c_cc.p, sizeof(cc), cudaMemcpyDeviceToHost, e->s));
+      CK(cudaStreamSynchronize(e->s));
+      e->est.cache_lines = e->c_lines;
+      e->est.cache_admissions = e->c_admissions;
+      e->est.last_admitted = e->c_admissions ? cc[CC_ADMIT] : 0;
+      e->est.last_evicted = e->c_admissions ? cc[CC_EVICT] : 0;
+      e->est.cache_resident = e->c_admissions ? e->c_lines - (cc[CC_FREE] - cc[CC_ADMIT]) : 0;
+      e->est.cache_hit_slots = cc[CC_WALK] - std::min(cc[CC_WALK], cc[CC_MISS]);
+      e->est.cache_miss_slots = cc[CC_MISS];
+    }
     *out = e->est;
+  });
+}
+
+SGS_API int sgs_cache_refresh(sgs_engine *e) {
+  if (!e) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    if (!e->loaded) fail(SGS_ERR_STATE, "no graph loaded");
+    CK(cudaSetDevice(e->dev));
+    e->cache_admit(/*rotate=*/false);
+    e->cache_publish();
+    e->sync();
   });
 }
 

@@ -53,6 +53,21 @@ struct GraphView {
   uint32_t *adj_h;   // pinned, mapped host arena (may be null)
   uint32_t *wgt_h;
   int wmode;
+  // device edge cache of the host tier (all null when the cache is off):
+  // cmap[c] = cache line holding host-arena line c (slots [c*CLINE,
+  // (c+1)*CLINE)) or NO_LINE; adj_c/wgt_c hold the cached lines
+  const uint32_t *cmap;
+  uint32_t *adj_c;  // = adj_d + cbase: the cache lines follow the HBM arena
+  uint32_t *wgt_c;
+  uint64_t cbase;
+  // hotness: per vertex four u8 counters of activations (one per snapshot of
+  // a four-snapshot window); relaxation kernels add 1 to byte hot_sh / 8 of
+  // every host-tier vertex they expand
+  uint32_t *hot;
+  uint32_t hot_sh;
+  // [0] host-tier slots the relaxation maps walked, [1] of those, slots read
+  // over the host link (the rest came from the cache)
+  unsigned long long *cstat;
 };
 
 struct FrontierView {
@@ -81,6 +96,80 @@ __device__ __forceinline__ uint32_t *adj_wptr(const GraphView &g, uint64_t o) {
 }
 __device__ __forceinline__ uint32_t *wgt_wptr(const GraphView &g, uint64_t o) {
   return ((o & HOST_BIT) ? g.wgt_h : g.wgt_d) + (o & OFF_MASK);
+}
+
+// Device edge cache.  The host arena is cut into lines of CLINE slots (512 B
+// of ids, and as much of weights); a line the cache holds is read from HBM
+// instead of over the host link.  The host copy stays authoritative and the
+// cache is written through (every write of a snapshot into a cached line is
+// made to both copies), so the two never differ and any reader may use
+// either.
+// Blocks and the quads read from them are 16-B aligned, so a quad never
+// straddles two lines.
+constexpr uint32_t CLINE_SHIFT = 7;
+constexpr uint32_t CLINE = 1u << CLINE_SHIFT;
+constexpr uint32_t NO_LINE = 0xFFFFFFFFu;
+
+// Cache line holding host-arena slot h, or NO_LINE.
+__device__ __forceinline__ uint32_t cache_line(const GraphView &g, uint64_t h) {
+  return g.cmap ? __ldg(g.cmap + (h >> CLINE_SHIFT)) : NO_LINE;
+}
+// Slots j.. of the block at offset o, for reading: HBM arena, cached line or
+// host arena.
+__device__ __forceinline__ const uint32_t *adj_at(const GraphView &g, uint64_t o, uint32_t j) {
+  if (!(o & HOST_BIT)) return g.adj_d + o + j;
+  const uint64_t h = (o & OFF_MASK) + j;
+  const uint32_t m = cache_line(g, h);
+  if (m != NO_LINE) return g.adj_c + ((uint64_t)m << CLINE_SHIFT) + (h & (CLINE - 1));
+  return g.adj_h + h;
+}
+__device__ __forceinline__ const uint32_t *wgt_at(const GraphView &g, uint64_t o, uint32_t j) {
+  if (!(o & HOST_BIT)) return g.wgt_d + o + j;
+  const uint64_t h = (o & OFF_MASK) + j;
+  const uint32_t m = cache_line(g, h);
+  if (m != NO_LINE) return g.wgt_c + ((uint64_t)m << CLINE_SHIFT) + (h & (CLINE - 1));
+  return g.wgt_h + h;
+}
+// Offset to read the block at o (len slots) from: when the whole block lies
+// in one cached line, its place in the cache region of the HBM arena (an HBM
+// offset, so no per-read lookup follows); otherwise o.
+__device__ __forceinline__ uint64_t resolve_block(const GraphView &g, uint64_t o, uint32_t len) {
+  if (!(o & HOST_BIT) || !g.cmap || !len) return o;
+  const uint64_t h0 = o & OFF_MASK;
+  if ((h0 >> CLINE_SHIFT) != ((h0 + len - 1) >> CLINE_SHIFT)) return o;
+  const uint32_t m = __ldg(g.cmap + (h0 >> CLINE_SHIFT));
+  return m == NO_LINE ? o : g.cbase + ((uint64_t)m << CLINE_SHIFT) + (h0 & (CLINE - 1));
+}
+
+// Write-through of slot j of the block at offset o: the cached copy of its
+// line, or null (HBM block, or line not cached).
+__device__ __forceinline__ uint32_t *cache_slot_w(const GraphView &g, uint32_t *base, uint64_t o,
+                                                  uint32_t j) {
+  if (!(o & HOST_BIT) || !g.cmap) return nullptr;
+  const uint64_t h = (o & OFF_MASK) + j;
+  const uint32_t m = g.cmap[h >> CLINE_SHIFT];
+  return m == NO_LINE ? nullptr : base + ((uint64_t)m << CLINE_SHIFT) + (h & (CLINE - 1));
+}
+// Stores id (and weight) into slot j of the block at o, and into its cached
+// line if there is one.
+__device__ __forceinline__ void store_slot(const GraphView &g, uint64_t o, uint32_t j, uint32_t id,
+                                           bool has_w, uint32_t w) {
+  uint32_t *a = ((o & HOST_BIT) ? g.adj_h : g.adj_d) + (o & OFF_MASK) + j;
+  *a = id;
+  if (has_w) ((o & HOST_BIT) ? g.wgt_h : g.wgt_d)[(o & OFF_MASK) + j] = w;
+  if (uint32_t *c = cache_slot_w(g, g.adj_c, o, j)) {
+    *c = id;
+    if (has_w) g.wgt_c[c - g.adj_c] = w;
+  }
+}
+
+// One activation of host-tier vertex v in the current snapshot's counter
+// (saturating at 255; the counters of the window are summed at admission).
+// Called by the one thread that owns v's frontier entry.
+__device__ __forceinline__ void hot_bump(const GraphView &g, uint32_t v, uint64_t o) {
+  if (!g.hot || !(o & HOST_BIT)) return;
+  const uint32_t h = g.hot[v];
+  if ((h >> g.hot_sh & 0xFFu) != 0xFFu) g.hot[v] = h + (1u << g.hot_sh);
 }
 
 // Weight of slot j of u's block.  Synthesized mode reproduces the

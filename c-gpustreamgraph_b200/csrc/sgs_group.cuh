@@ -88,8 +88,8 @@ struct GroupRelaxOp {
   };
   __device__ __forceinline__ Quad fetch(const Payload &p, uint32_t j0) const {
     Quad q;
-    q.ids = ld_quad(adj_ptr(g, p.off) + j0);
-    q.ws = any_w ? ld_quad(wgt_ptr(g, p.off) + j0) : make_uint4(1, 1, 1, 1);
+    q.ids = ld_quad(adj_at(g, p.off, j0));
+    q.ws = any_w ? ld_quad(wgt_at(g, p.off, j0)) : make_uint4(1, 1, 1, 1);
     return q;
   }
   // Returns a 4-bit mask of destinations to append; dst[] holds them.
@@ -173,7 +173,7 @@ struct GroupInvalidateOp {
     uint4 ids;
   };
   __device__ __forceinline__ Quad fetch(const Payload &p, uint32_t j0) const {
-    return Quad{ld_quad(adj_ptr(g, p.off) + j0)};
+    return Quad{ld_quad(adj_at(g, p.off, j0))};
   }
   __device__ __forceinline__ uint32_t visit4(uint32_t u, const Payload &p, uint32_t j0, uint32_t len,
                                              const Quad &qd, uint32_t (&dst)[4]) const {
@@ -232,10 +232,10 @@ __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out
   __shared__ P s_pay[GC];
   __shared__ uint32_t s_vtx[GC];
   __shared__ unsigned long long s_lane[GMAX];
-  __shared__ unsigned long long s_host;  // owned slots in the pinned-host tier
+  __shared__ unsigned long long s_host, s_all;  // host-tier slots read over the link / owned
   clear_prev_masks(prev_vtx, prev_cnt, prev_mask);
   if (threadIdx.x < GMAX) s_lane[threadIdx.x] = 0;
-  if (threadIdx.x == 0) s_host = 0;
+  if (threadIdx.x == 0) s_host = s_all = 0;
   uint32_t host_acc = 0;
   uint32_t lane_acc[GMAX] = {0, 0, 0, 0};  // (query, edge) pairs of owned entries
   const uint64_t packed = __ldcg((const unsigned long long *)in.counter);
@@ -264,9 +264,15 @@ __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out
           const uint32_t v = __ldcg(&in.vtx[idx]);
           s_vtx[t] = v;
           s_len[t] = __ldcg(&in.len[idx]);
-          const P pay = op.load(v);
+          P pay = op.load(v);
+          if (pay.off & HOST_BIT) {
+            if (eb >= E0) {
+              hot_bump(op.g, v, pay.off);
+              if (op.g.cstat) atomicAdd(&s_all, (unsigned long long)s_len[t]);
+            }
+            pay.off = resolve_block(op.g, pay.off, s_len[t]);
+          }
           s_pay[t] = pay;
-          if (eb >= E0 && (pay.off & HOST_BIT)) host_acc += s_len[t];
           if (eb >= E0 && pay.mask) {
             const uint32_t l = op.g.live[v];
 #pragma unroll
@@ -307,7 +313,12 @@ __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out
         if (hn) qn = op.fetch(s_pay[ln], jn);
         uint32_t app = 0;
         uint32_t dst[4] = {0, 0, 0, 0};
-        if (hc) app = op.visit4(s_vtx[lc], s_pay[lc], jc, s_len[lc], qc, dst);
+        if (hc) {
+          app = op.visit4(s_vtx[lc], s_pay[lc], jc, s_len[lc], qc, dst);
+          const uint64_t o = s_pay[lc].off;
+          if ((o & HOST_BIT) && cache_line(op.g, (o & OFF_MASK) + jc) == NO_LINE)
+            host_acc += min(4u, s_len[lc] - jc);
+        }
         lc = ln;
         jc = jn;
         qc = qn;
@@ -337,6 +348,10 @@ __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out
     if (edge_stat) atomicAdd(edge_stat, s_lane[threadIdx.x]);
   }
   if (threadIdx.x == 0 && s_host && host_stat) atomicAdd(host_stat, s_host);
+  if (threadIdx.x == 0 && op.g.cstat) {
+    if (s_all) atomicAdd(&op.g.cstat[0], s_all);
+    if (s_host) atomicAdd(&op.g.cstat[1], s_host);
+  }
   __syncthreads();  // shared state is reused when the body runs again
 }
 

@@ -49,16 +49,17 @@ struct PrPushOp {
     p.c = pv[v];
     return p;
   }
+  __device__ __forceinline__ void touch(uint32_t v, const Payload &p) const { hot_bump(g, v, p.off); }
   __device__ __forceinline__ uint32_t visit(uint32_t, const Payload &p, uint32_t j,
                                             bool &, uint32_t &, uint32_t &) const {
-    const uint32_t dst = adj_ptr(g, p.off)[j];
+    const uint32_t dst = *adj_at(g, p.off, j);
     if (dst == SGS_TOMB) return 0;
     if (p.c != 0.0) atomicAdd(&r[dst], p.c);
     return 1;
   }
   __device__ __forceinline__ uint32_t visit4(uint32_t, const Payload &p, uint32_t j0, uint32_t len,
                                              bool (&)[4], uint32_t (&)[4], uint32_t (&)[4]) const {
-    const uint4 ids = ld_quad(adj_ptr(g, p.off) + j0);
+    const uint4 ids = ld_quad(adj_at(g, p.off, j0));
     uint32_t c = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -89,7 +90,7 @@ struct PrAmendOp {
   }
   __device__ __forceinline__ uint32_t visit(uint32_t, const Payload &p, uint32_t j,
                                             bool &, uint32_t &, uint32_t &) const {
-    const uint32_t dst = adj_ptr(g, p.off)[j];
+    const uint32_t dst = *adj_at(g, p.off, j);
     if (dst == SGS_TOMB) return 0;
     if (p.c != 0.0) atomicAdd(&r[dst], p.c);
     return 1;
@@ -143,7 +144,8 @@ struct TombOp {
   __device__ __forceinline__ uint32_t visit4(uint32_t u, const Payload &p, uint32_t j0, uint32_t len,
                                              bool (&)[4], uint32_t (&)[4], uint32_t (&)[4]) const {
     uint32_t *a = adj_wptr(g, p.off) + j0;
-    const uint4 q = *reinterpret_cast<const uint4 *>(a);
+    uint32_t *ca = cache_slot_w(g, g.adj_c, p.off, j0);  // cached copy: read from it, write both
+    const uint4 q = *reinterpret_cast<const uint4 *>(ca ? ca : a);
     uint32_t c = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -158,6 +160,7 @@ struct TombOp {
       }
       if (l < p.ge && keys[l] == key) {
         a[k] = SGS_TOMB;
+        if (ca) ca[k] = SGS_TOMB;
         ++c;
       }
     }
@@ -502,8 +505,8 @@ __global__ void k_insert_write(GraphView g, const uint64_t *keys, const uint32_t
       else hi = m;
     }
     const uint64_t pos = wbase[u] + (i - lo);
-    adj_wptr(g, pos)[0] = v;
-    if (g.wmode == W_EXPLICIT) wgt_wptr(g, pos)[0] = w[i];
+    const bool ew = g.wmode == W_EXPLICIT;
+    store_slot(g, pos, 0, v, ew, ew ? w[i] : 0u);
   }
 }
 
@@ -536,8 +539,8 @@ struct RelocCopyOp {
   }
   __device__ __forceinline__ uint32_t visit(uint32_t, const Payload &p, uint32_t j,
                                             bool &, uint32_t &, uint32_t &) const {
-    adj_wptr(g, p.to)[j] = adj_ptr(g, p.from)[j];
-    if (g.wmode == W_EXPLICIT) wgt_wptr(g, p.to)[j] = wgt_ptr(g, p.from)[j];
+    const bool ew = g.wmode == W_EXPLICIT;
+    store_slot(g, p.to, j, *adj_at(g, p.from, j), ew, ew ? *wgt_at(g, p.from, j) : 0u);
     return 0;
   }
 };

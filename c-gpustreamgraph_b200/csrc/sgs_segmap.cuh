@@ -2,6 +2,8 @@
 // (template only, so several translation units can instantiate it).
 #pragma once
 #include <cub/block/block_reduce.cuh>
+#include <type_traits>
+#include <utility>
 
 #include "sgs_device.cuh"
 
@@ -20,6 +22,14 @@ namespace sgs {
 // full warps.
 // ---------------------------------------------------------------------------
 constexpr int CHUNK = 256;
+
+// Ops that define touch(v, payload) are told once per frontier entry (by the
+// CTA that owns the entry's first slot); PageRank's push counts hotness there.
+template <class Op, class = void>
+struct op_touches : std::false_type {};
+template <class Op>
+struct op_touches<Op, std::void_t<decltype(std::declval<const Op &>().touch(
+                          0u, std::declval<const typename Op::Payload &>()))>> : std::true_type {};
 
 // Ops either implement visit (one slot) or, with kQuad, visit4 (four
 // consecutive slots j0..j0+3 of one block, j0 a multiple of 4; slots >= len
@@ -78,6 +88,8 @@ __global__ void __launch_bounds__(RELAX_THREADS)
           s_vtx[t] = v;
           s_len[t] = __ldcg(&in.len[idx]);
           s_pay[t] = op.load(idx, v);
+          if constexpr (op_touches<Op>::value)
+            if (eb >= E0) op.touch(v, s_pay[t]);
         }
       }
       __syncthreads();

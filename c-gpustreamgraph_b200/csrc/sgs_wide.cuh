@@ -155,6 +155,9 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
   const bool cc0 = op.algo.cc >> t & 1ull, cc1 = op.algo.cc >> (t + 32) & 1ull;
   unsigned long long acc0 = 0, acc1 = 0, chg0 = 0, chg1 = 0;
   uint32_t evald = 0;  // (lane, edge) pairs evaluated by this thread's lanes
+  uint32_t miss_acc = 0;  // host-tier slots this thread read over the link
+  __shared__ unsigned long long s_host;  // host-tier slots of the entries this CTA owns
+  if (threadIdx.x == 0) s_host = 0;
   __shared__ unsigned long long s_eval;
   if (threadIdx.x == 0) s_eval = 0;
   const uint64_t packed = __ldcg((const unsigned long long *)in.counter);
@@ -183,8 +186,17 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
           const uint32_t v = __ldcg(&in.vtx[idx]);
           s_vtx[h] = v;
           s_len[h] = __ldcg(&in.len[idx]);
-          s_off[h] = g.off[v];
+          const uint64_t o = g.off[v];
           s_mask[h] = __ldcg(&m_in[v]);
+          if (o & HOST_BIT) {
+            if (eb >= E0) {
+              hot_bump(g, v, o);
+              if (g.cstat) atomicAdd(&s_host, (unsigned long long)s_len[h]);
+            }
+            s_off[h] = resolve_block(g, o, s_len[h]);
+          } else {
+            s_off[h] = o;
+          }
         }
       }
       __syncthreads();
@@ -220,11 +232,21 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
           const uint32_t j = (uint32_t)(e - s_eb[l]);
           if (j < s_len[l]) {
             le = l;
-            v = __ldcg(adj_ptr(g, s_off[l]) + j);
+            // slot position in its arena: HBM, cache line or host
+            uint64_t x = s_off[l] + j;
+            int tier = 0;
+            if (x & HOST_BIT) {
+              x &= OFF_MASK;
+              const uint32_t m = cache_line(g, x);
+              tier = m != NO_LINE ? 1 : 2;
+              if (m != NO_LINE) x = ((uint64_t)m << CLINE_SHIFT) + (x & (CLINE - 1));
+              miss_acc += tier == 2;
+            }
+            v = __ldcg((tier == 0 ? g.adj_d : tier == 1 ? g.adj_c : g.adj_h) + x);
             ok = v != SGS_TOMB;
             if constexpr (Op::kRestrict) ok = ok && bit_at(op.only, v);
             if (ok && op.algo.sssp && s_mask[l] & op.algo.sssp)
-              w = g.wmode == W_EXPLICIT ? __ldcg(wgt_ptr(g, s_off[l]) + j)
+              w = g.wmode == W_EXPLICIT ? __ldcg((tier == 0 ? g.wgt_d : tier == 1 ? g.wgt_c : g.wgt_h) + x)
                   : g.wmode == W_SYNTH  ? (s_vtx[l] + v) % 128u + 1u
                                         : 1u;
           }
@@ -295,6 +317,8 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
   atomicAdd(&s_chg[t + 32], chg1);
   const unsigned long long ev = warp_sum((unsigned long long)evald);
   if (t == 0 && ev) atomicAdd(&s_eval, ev);
+  const unsigned long long miss = warp_sum((unsigned long long)miss_acc);
+  if (g.cstat && t == 0 && miss) atomicAdd(&g.cstat[1], miss);
   __syncthreads();
   if (threadIdx.x < WLANES) {
     const unsigned long long x = s_lane[threadIdx.x], c = s_chg[threadIdx.x];
@@ -302,6 +326,7 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
     if (c && lane_changes) atomicAdd(&lane_changes[threadIdx.x], c);
   }
   if (threadIdx.x == 0 && s_eval && edge_stat) atomicAdd(edge_stat, s_eval);
+  if (threadIdx.x == 0 && g.cstat && s_host) atomicAdd(&g.cstat[0], s_host);
   __syncthreads();  // shared state is reused when the body runs again
 }
 

@@ -50,7 +50,7 @@ EXPORTS = [
     "sgs_read_edge_list", "sgs_read_stream_sizes", "sgs_read_update_file", "sgs_free",
     "sgs_ppr_create_csr", "sgs_ppr_create", "sgs_ppr_destroy", "sgs_ppr_info",
     "sgs_ppr_export", "sgs_ppr_forward", "sgs_ppr_backward", "sgs_ppr_timing",
-    "sgs_ppr_get_stats", "sgs_serve", "sgs_autotune",
+    "sgs_ppr_get_stats", "sgs_serve", "sgs_autotune", "sgs_cache_refresh",
 ]
 
 K_GROUP, K_GROUP_INVAL, K_PR_PUSH, K_WIDE, K_WIDE_INVAL = range(5)
@@ -114,6 +114,13 @@ class EngineStats(C.Structure):
         ("last_batch_ms", C.c_double),
         ("kernel_launches", C.c_uint64),
         ("last_batch_edges", C.c_uint64),
+        ("cache_lines", C.c_uint64),
+        ("cache_resident", C.c_uint64),
+        ("cache_admissions", C.c_uint64),
+        ("last_admitted", C.c_uint64),
+        ("last_evicted", C.c_uint64),
+        ("cache_hit_slots", C.c_uint64),
+        ("cache_miss_slots", C.c_uint64),
     ]
 
     def as_dict(self):
@@ -234,6 +241,7 @@ def lib():
     L.sgs_ppr_timing.argtypes = [vp, i32]
     L.sgs_serve.argtypes = [vp, C.POINTER(Request), u32, u32, i32, C.POINTER(Completion)]
     L.sgs_autotune.argtypes = [vp, C.POINTER(Tune)]
+    L.sgs_cache_refresh.argtypes = [vp]
     L.sgs_ppr_get_stats.argtypes = [vp, C.POINTER(PprStats)]
     for name in EXPORTS:
         if name not in ("sgs_version", "sgs_last_error", "sgs_config_default",
@@ -528,6 +536,11 @@ class Engine:
 
     def synchronize(self):
         _check(lib().sgs_synchronize(self.h))
+
+    def cache_refresh(self):
+        """Edge-cache admission now, from the current hotness window; returns
+        when the admitted lines are visible (no-op without a cache)."""
+        _check(lib().sgs_cache_refresh(self.h))
 
     def kernel_timing(self, enable=True):
         _check(lib().sgs_kernel_timing(self.h, int(enable)))

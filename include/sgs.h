@@ -30,6 +30,12 @@
  *                                    GatherBuffer (framework.cuh:1657-1679)
  *   sgs_get_query_stats           <- RunningInfo counters
  *                                    (framework/hybrid_policy.h:38-136)
+ *   sgs_cache_refresh             <- compute_hot_vertices_* +
+ *                                    confirm_candidate_batch + LoadCache
+ *                                    (framework.cuh:149-308, :1304-1385;
+ *                                    variants/driver.cuh:437-516); the same
+ *                                    admission also runs inside every
+ *                                    sgs_apply_batch
  */
 #ifndef SGS_H
 #define SGS_H
@@ -82,7 +88,14 @@ typedef struct sgs_config {
   uint32_t segments;      /* -SEGMENT: vertex segments (residency unit)    */
   uint32_t n_stream;      /* -n_stream: accepted for drop-in; unused       */
   uint32_t block_size;    /* -block_size: accepted for drop-in; unused     */
-  double cache_gb;        /* -cache: accepted; see hbm_budget_gb           */
+  double cache_gb;        /* -cache: HBM bytes (1e9) of the device edge
+                             cache of the host tier, carved out of
+                             hbm_budget_gb (needs a budget; 0: no cache).
+                             Lines of 128 slots of host-resident blocks are
+                             admitted per snapshot by hotness (activations
+                             over a four-snapshot window) and copied on a
+                             side stream; the static HBM segments get
+                             hbm_budget_gb - cache_gb                      */
   double hbm_budget_gb;   /* HBM budget for edge blocks; <= 0: unlimited.
                              Segments beyond it live in pinned host memory
                              and are read over the host link              */
@@ -132,6 +145,17 @@ typedef struct sgs_engine_stats {
                                  (CUB sorts and scans not counted)         */
   uint64_t last_batch_edges;  /* edges traversed by all queries in the last
                                  snapshot (sum of their edges_traversed)   */
+  /* device edge cache (zero when off) */
+  uint64_t cache_lines;       /* capacity in lines of 128 slots            */
+  uint64_t cache_resident;    /* lines held after the last admission       */
+  uint64_t cache_admissions;  /* admissions so far (one per snapshot, plus
+                                 sgs_cache_refresh calls)                  */
+  uint64_t last_admitted;     /* lines copied in by the last admission     */
+  uint64_t last_evicted;      /* lines evicted by the last admission       */
+  uint64_t cache_hit_slots;   /* host-tier slots that BFS/SSSP/CC passes read
+                                 from the cache (since load)               */
+  uint64_t cache_miss_slots;  /* host-tier slots they read over the host link
+                                 (since load)                              */
 } sgs_engine_stats;
 
 /* Per-kernel-class timing of the relaxation launches (CUDA events on the
@@ -204,6 +228,12 @@ SGS_API int sgs_apply_batch(sgs_engine *e, const uint32_t *ins_src,
                             const uint32_t *ins_dst, const uint32_t *ins_w,
                             uint64_t n_ins, const uint32_t *del_src,
                             const uint32_t *del_dst, uint64_t n_del, int mem);
+
+/* Re-runs the edge-cache admission now from the current hotness window
+ * (without advancing it) and waits until the admitted lines are visible; a
+ * no-op when the cache is off.  For drivers that warm the cache after the
+ * static run, as the reference's do with LoadCache. */
+SGS_API int sgs_cache_refresh(sgs_engine *e);
 
 /* Copies nv elements of a field (u32, or f64 for PR value/buffer). */
 SGS_API int sgs_gather(sgs_engine *e, int qid, int field, void *out, int mem);

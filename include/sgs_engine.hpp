@@ -17,8 +17,10 @@
 // Here a snapshot is applied by the second call of the pair (add_edge or
 // Compensate), which hands inserts and deletes to sgs_apply_batch together:
 // the reference's own order within a snapshot (inserts, then deletes,
-// framework.cuh:1011-1012) is kept by the engine.  The cache-lifecycle calls
-// are accepted and do nothing: residency follows the HBM budget.  Errors throw
+// framework.cuh:1011-1012) is kept by the engine.  Of the cache-lifecycle
+// calls, LoadCache runs the edge-cache admission (sgs_cache_refresh); the
+// hotness and candidate calls are folded into it.  Every snapshot also admits
+// by itself inside sgs_apply_batch.  Errors throw
 // sgs::Error (the reference exits through GROUTE_CUDA_CHECK instead).
 #pragma once
 #include <cstdint>
@@ -129,13 +131,15 @@ class Engine {
   void Compensate(std::pair<uint32_t, uint32_t> &lb, uint32_t k) { add_edge(lb, k); }
 
   // Cache lifecycle of the reference (framework.cuh:149-308, 1304-1385):
-  // residency is managed by the HBM budget, so these are no-ops.
+  // hotness scoring, candidate choice, eviction and compaction are one
+  // admission pass of the engine's line cache, run by LoadCache (and by every
+  // snapshot); the other calls have nothing left to do.
   void compute_hot_vertices_pr() {}
   void compute_hot_vertices_sssp() {}
   void confirm_candidate_batch() {}
   void evication_cache() {}
   void compact_cache() {}
-  void LoadCache() {}
+  void LoadCache() { check(sgs_cache_refresh(h_)); }
 
   void GatherValue() { gather(SGS_FIELD_VALUE); }
   void GatherParent() { gather(SGS_FIELD_PARENT); }
