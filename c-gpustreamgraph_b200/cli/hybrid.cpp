@@ -66,6 +66,7 @@ const std::map<std::string, bool> &known() {
       {"residence", true}, {"sparse", false}, {"non_atomic", false}, {"cut_threshold", true},
       {"top_ranks", true}, {"print_ranks", false}, {"norm", false},
       {"hbm_budget", true}, {"weights", true}, {"snapshots", true}, {"device", true},
+      {"pull", true},
   };
   return k;
 }
@@ -128,6 +129,8 @@ int main(int argc, char **argv) {
   const std::string wmode = f.get("weights", "synth");
   c.weight_mode = wmode == "file" ? SGS_W_EXPLICIT : wmode == "unit" ? SGS_W_UNIT : SGS_W_SYNTH;
   if (SGS_APP == SGS_PR) c.pr_tol = f.num("error", 1e-6) * (1.0 - c.pr_alpha);
+  // -pull: bit 0 PageRank pull sweeps, bit 1 direction-optimizing BFS starts
+  c.pull = (uint32_t)f.num("pull", SGS_APP == SGS_BFS ? 3 : 1);
   try {
     using clk = std::chrono::steady_clock;
     sgs::Engine engine(SGS_APP, &c);

@@ -30,6 +30,7 @@
 #include "../../include/sgs.h"
 #include "sgs_cache.cuh"
 #include "sgs_group.cuh"
+#include "sgs_pull.cuh"
 #include "sgs_kernels.cuh"
 #include "sgs_wide.cuh"
 
@@ -263,6 +264,16 @@ struct sgs_engine {
   bool c_pending = false;              // copies issued, lines not yet published
   uint64_t c_admissions = 0;
 
+  // in-edge store (sgs_pull.cuh), HBM only, source ids only: built by the
+  // first pull sweep, then updated by every snapshot
+  bool in_built = false, in_failed = false;
+  DBuf<uint64_t> in_off;
+  DBuf<uint32_t> in_slots, in_live, in_cap, in_adj;
+  DBuf<unsigned long long> in_top;     // [2]; tier 1 unused
+  uint64_t in_capslots = 0;
+  uint64_t in_builds = 0;
+  DBuf<uint64_t> t_dkeys, t_ikeys, t_tmp;  // the batch's keys transposed
+
   ~sgs_engine() {
     if (s2) {
       cudaStreamSynchronize(s2);
@@ -297,6 +308,17 @@ struct sgs_engine {
       g.hot_sh = 8 * hot_k;
       g.cstat = c_cc.p;
     }
+    return g;
+  }
+  GraphView in_view() {
+    GraphView g{};
+    g.nv = nv;
+    g.off = in_off.p;
+    g.slots = in_slots.p;
+    g.live = in_live.p;
+    g.cap = in_cap.p;
+    g.adj_d = in_adj.p;
+    g.wmode = SGS_W_UNIT;
     return g;
   }
   FrontierView fview(uint32_t buf, unsigned long long *counter) {
@@ -438,6 +460,143 @@ struct sgs_engine {
     ++c_admissions;
   }
 
+  // -------------------------------------------------------- in-edge store
+  // Transposes the out-store: in-degrees, capacities with the same slack,
+  // offsets by a scan, then every live out-slot (u -> d) places u in d's
+  // in-block through a per-destination cursor.  Uses frontier buffers 0 and
+  // 1 and counters special(0..1): callers build it before they seed a
+  // frontier (or after the last one they use).
+  void in_build() {
+    const GraphView g = view();
+    in_slots.ensure(nv);
+    in_live.ensure(nv);
+    in_cap.ensure(nv);
+    in_off.ensure((size_t)nv + 1);
+    in_top.ensure(2);
+    CK(cudaMemsetAsync(in_slots.p, 0, sizeof(uint32_t) * nv, s));
+    CK(cudaMemsetAsync(special(0), 0, sizeof(unsigned long long) * 2, s));
+    FrontierView f0 = fview(0, special(0));
+    { ++n_launch; k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(g, f0); }
+    { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(f0, fview(1, special(1)),
+                                                 InCountOp{g, in_slots.p}, nullptr); }
+    { ++n_launch; k_layout_caps<<<grid_elem(nv), 256, 0, s>>>(in_slots.p, nv, cfg.slack_div, in_cap.p); }
+    { ++n_launch; k_u32_to_u64<<<grid_elem(nv), 256, 0, s>>>(in_cap.p, nv, in_off.p); }
+    CK(cudaMemsetAsync(in_off.p + nv, 0, sizeof(uint64_t), s));
+    size_t tb = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, in_off.p, in_off.p, (int)(nv + 1), s));
+    cub_ensure(tb);
+    CK(cub::DeviceScan::ExclusiveSum(cub_tmp.p, tb, in_off.p, in_off.p, (int)(nv + 1), s));
+    uint64_t total = 0;
+    CK(cudaMemcpyAsync(&total, in_off.p + nv, sizeof(total), cudaMemcpyDeviceToHost, s));
+    sync();
+    in_capslots = total + (uint64_t)(total * std::max(0.0, cfg.arena_headroom)) + 4096;
+    in_adj.ensure(in_capslots);
+    unsigned long long tops[2] = {total, 0};
+    CK(cudaMemcpyAsync(in_top.p, tops, sizeof(tops), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(in_live.p, 0, sizeof(uint32_t) * nv, s));  // the fill cursors
+    { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
+        f0, fview(1, special(1)), InFillOp{g, in_off.p, in_live.p, in_adj.p}, nullptr); }
+    CK(cudaMemcpyAsync(in_live.p, in_slots.p, sizeof(uint32_t) * nv, cudaMemcpyDeviceToDevice, s));
+    CK(cudaGetLastError());
+    sync();
+    in_built = true;
+    ++in_builds;
+  }
+  void in_release() {
+    in_off.release();
+    in_slots.release();
+    in_live.release();
+    in_cap.release();
+    in_adj.release();
+    in_built = false;
+  }
+  // True when the in-store is there (built now if needed).  If it cannot be
+  // allocated the engine keeps to push sweeps (both run on the GPU).
+  bool ensure_in() {
+    if (!cfg.pull || in_failed) return false;
+    if (in_built) return true;
+    try {
+      in_build();
+    } catch (const SgsError &f) {
+      if (f.code != SGS_ERR_OOM) throw;
+      in_release();
+      in_failed = true;
+      return false;
+    }
+    return true;
+  }
+  // The snapshot's deletes and kept inserts applied to the in-store, keys
+  // transposed and sorted; when relocations would not fit, the store is
+  // rebuilt from the (already updated) out-store instead.
+  void in_apply(uint64_t ni, uint64_t nd, uint32_t nkept) {
+    if (!in_built) return;
+    const GraphView gi = in_view();
+    const int eb = sort_bits();
+    size_t tb = 0;
+    if (nd) {
+      t_dkeys.ensure(nd);
+      t_tmp.ensure(std::max<uint64_t>(nd, nkept));
+      { ++n_launch; k_transpose_keys<<<grid_elem(nd), 256, 0, s>>>(b_dkeys_s.p, (uint32_t)nd, nullptr, t_tmp.p); }
+      CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, t_tmp.p, t_dkeys.p, (int)nd, 0, eb, s));
+      cub_ensure(tb);
+      CK(cub::DeviceRadixSort::SortKeys(cub_tmp.p, tb, t_tmp.p, t_dkeys.p, (int)nd, 0, eb, s));
+      CK(cudaMemsetAsync(special(4), 0, sizeof(unsigned long long) * 2, s));
+      b_gstart.ensure((size_t)nv + 1);
+      { ++n_launch; k_group_heads<<<grid_elem(nd), 256, 0, s>>>(gi, t_dkeys.p, nullptr, (uint32_t)nd, b_gstart.p,
+                                                  nullptr, 0, fview(0, special(4))); }
+      TombOp op{gi, t_dkeys.p, b_gstart.p, (uint32_t)nd};
+      { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(4)), fview(1, special(5)), op,
+                                                   nullptr); }
+      CK(cudaGetLastError());
+    }
+    if (!ni || !nkept) return;
+    t_ikeys.ensure(nkept);
+    t_tmp.ensure(nkept);
+    { ++n_launch; k_transpose_keys<<<grid_elem(nkept), 256, 0, s>>>(b_ikept.p, nkept, nullptr, t_tmp.p); }
+    tb = 0;
+    CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, t_tmp.p, t_ikeys.p, (int)nkept, 0, eb, s));
+    cub_ensure(tb);
+    CK(cub::DeviceRadixSort::SortKeys(cub_tmp.p, tb, t_tmp.p, t_ikeys.p, (int)nkept, 0, eb, s));
+    InsertCtx c{};
+    c.arena_top = in_top.p;
+    c.arena_cap[0] = in_capslots;
+    c.arena_cap[1] = 0;
+    c.err = b_err.p;
+    c.wbase = wbase.p;
+    CK(cudaMemsetAsync(b_stat.p, 0, sizeof(unsigned long long) * 2, s));
+    { ++n_launch; k_insert_plan<<<grid_elem(nkept), 256, 0, s>>>(gi, t_ikeys.p, b_nkept.p, c, 1, b_stat.p); }
+    unsigned long long h[2], tops[2];
+    CK(cudaMemcpyAsync(h, b_stat.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(tops, in_top.p, sizeof(tops), cudaMemcpyDeviceToHost, s));
+    sync();
+    if (tops[0] + h[0] > in_capslots) {  // no room for the relocations: transpose again
+      in_build();
+      return;
+    }
+    rl_vtx.ensure(nkept + 1);
+    rl_len.ensure(nkept + 1);
+    rl_from.ensure(nkept + 1);
+    rl_to.ensure(nkept + 1);
+    c.rl_vtx = rl_vtx.p;
+    c.rl_from = rl_from.p;
+    c.rl_to = rl_to.p;
+    c.rl_len = rl_len.p;
+    c.rl_count64 = rl_count.p;
+    CK(cudaMemsetAsync(rl_count.p, 0, sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(b_err.p, 0, sizeof(unsigned int), s));
+    { ++n_launch; k_insert_plan<<<grid_elem(nkept), 256, 0, s>>>(gi, t_ikeys.p, b_nkept.p, c, 0, nullptr); }
+    { ++n_launch; k_insert_write<<<grid_elem(nkept), 256, 0, s>>>(gi, t_ikeys.p, nullptr, b_nkept.p, wbase.p); }
+    CK(cudaMemsetAsync(special(6), 0, sizeof(unsigned long long) * 2, s));
+    { ++n_launch; k_reloc_frontier<<<grid_elem(nkept), 256, 0, s>>>(rl_count.p, rl_len.p, fview(0, special(6))); }
+    { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(6)), fview(1, special(7)),
+                                                 RelocCopyOp{gi, rl_from.p, rl_to.p}, nullptr); }
+    CK(cudaGetLastError());
+    unsigned int herr = 0;
+    CK(cudaMemcpyAsync(&herr, b_err.p, sizeof(herr), cudaMemcpyDeviceToHost, s));
+    sync();
+    if (herr) fail(SGS_ERR_OOM, "in-edge arena exhausted while inserting");
+  }
+
   // ------------------------------------------------------------- graph load
   // Lays the graph out in arenas from a device CSR: per-vertex capacity with
   // slack, offsets by an exclusive scan, the first `split` vertices in HBM
@@ -451,6 +610,8 @@ struct sgs_engine {
     fg = nullptr;
     frun = 0;
     loaded = false;
+    in_release();
+    in_failed = false;
     est = sgs_engine_stats{};
     nv = n;
     uint64_t ne_in = 0;
@@ -706,6 +867,52 @@ struct sgs_engine {
         hp ? gm[(rr - 1) % 3].p : nullptr, b_lane.p, rstat.p + rr, hstat.p + rr); }
   }
 
+  // BFS rounds of the lanes `lanes` (all BFS) of a narrow group, each round
+  // top-down (group_map) or bottom-up over the in-edge store
+  // (k_bfs_pull_round), chosen on the host from the frontier's size with
+  // Beamer's rule: bottom-up once the frontier's out-edges exceed 1/14 of the
+  // edges not yet explored, back to top-down when the frontier holds fewer
+  // than 1/24 of the vertices.  One counter read per round.
+  uint64_t bfs_bottom_up_total = 0;
+  uint32_t run_bfs_diropt(Group &G, uint32_t lanes, bool &converged) {
+    const GraphView g = view(), gi = in_view();
+    const uint32_t maxr = cfg.max_rounds;
+    converged = false;
+    CK(cudaMemsetAsync(rstat.p, 0, sizeof(unsigned long long) * (maxr + 2), s));
+    CK(cudaMemsetAsync(hstat.p, 0, sizeof(unsigned long long) * (maxr + 2), s));
+    bool bu = false;
+    uint64_t explored = 0;
+    for (uint32_t r = 0; r < maxr; ++r) {
+      unsigned long long c = 0;
+      CK(cudaMemcpyAsync(&c, cnt.p + r, sizeof(c), cudaMemcpyDeviceToHost, s));
+      sync();
+      const uint64_t nf = c >> CNT_SHIFT, mf = c & EDGE_MASK;
+      if (nf == 0) {
+        if (r >= 1) clear_masks(false, r - 1);
+        CK(cudaGetLastError());
+        converged = true;
+        return r;
+      }
+      const uint64_t mu = ne > explored ? ne - explored : 0;
+      if (!bu && mf * 14 > mu) bu = true;
+      else if (bu && nf * 24 < nv) bu = false;
+      explored += mf;
+      if (!bu) {
+        launch_group(r, GroupRelaxOp<GMAX>{g, G.st.p, G.val.p, gm[r % 3].p, gm[(r + 1) % 3].p, G.algo(), 0});
+      } else {
+        const bool hp = r >= 1;
+        { ++n_launch; k_bfs_pull_round<GMAX><<<grid_elem(nv), RELAX_THREADS, 0, s>>>(
+            g, gi, G.st.p, G.val.p, lanes, gm[r % 3].p, gm[(r + 1) % 3].p, fview(r, cnt.p + r),
+            hp ? fb[(r - 1) % 3].vtx.p : nullptr, hp ? cnt.p + r - 1 : nullptr,
+            hp ? gm[(r - 1) % 3].p : nullptr, fview(r + 1, cnt.p + r + 1), b_lane.p); }
+        ++bfs_bottom_up_total;
+      }
+      CK(cudaGetLastError());
+    }
+    for (uint32_t f = maxr >= 1 ? maxr - 1 : 0; f <= maxr; ++f) clear_masks(false, f);
+    return maxr;
+  }
+
   // Round loop shared by both group widths: `launch(rr)` queues round rr.
   template <class Launch>
   uint32_t run_rounds(Launch launch, bool wide, bool &converged, int kind, double per_slot,
@@ -924,10 +1131,17 @@ struct sgs_engine {
   // PageRank rounds over the static frontier of all non-empty blocks:
   // absorb (value += residual) then push alpha*res/outdeg; stop after the
   // first round whose absorbed residual L1 is below pr_tol.
+  // Rounds of the PageRank sweep over all vertices: absorb (value +=
+  // residual, push value = alpha * residual / outdeg), then the residual of
+  // every vertex from its in-neighbours' push values -- a pull over the
+  // in-edge store when it is there (cfg.pull), else a push over the
+  // out-blocks with FP64 atomics.
   uint32_t pr_rounds(Query &q, unsigned long long *edge_stat, bool &conv, double &last_l1) {
     GraphView g = view();
+    const bool pull = (cfg.pull & 1u) && ensure_in();
+    const GraphView gi = pull ? in_view() : g;
     reset_counters(0);
-    { ++n_launch; k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(g, fview(0, cnt.p)); }
+    { ++n_launch; k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(gi, fview(0, cnt.p)); }
     const uint32_t maxr = cfg.max_rounds;
     CK(cudaMemsetAsync(l1.p, 0, sizeof(double) * (maxr + 2), s));
     std::vector<double> hl(maxr + 2);
@@ -946,8 +1160,12 @@ struct sgs_engine {
         { ++n_launch; k_pr_absorb<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(g, q.x.p, q.r.p, q.pv.p, cfg.pr_alpha,
                                                            l1.p + r + k); }
         if (ktiming) CK(cudaEventRecord(kev[2 * k], s));
-        { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, cnt.p), fview(1, cnt.p + 1), op,
-                                                     edge_stat); }
+        if (pull)
+          { ++n_launch; k_pull_pr<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, cnt.p), gi, q.pv.p, q.r.p,
+                                                         edge_stat); }
+        else
+          { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, cnt.p), fview(1, cnt.p + 1), op,
+                                                       edge_stat); }
         if (ktiming) CK(cudaEventRecord(kev[2 * k + 1], s));
       }
       CK(cudaGetLastError());
@@ -955,7 +1173,8 @@ struct sgs_engine {
       sync();
       if (ktiming)
         for (uint32_t k = 0; k < nb; ++k)
-          account(SGS_K_PR_PUSH, pr_in, pr_inst, 4.0, 16.0, kev[2 * k], kev[2 * k + 1]);
+          account(pull ? SGS_K_PR_PULL : SGS_K_PR_PUSH, pr_in, pr_inst, 4.0, 16.0, kev[2 * k],
+                  kev[2 * k + 1]);
       for (uint32_t k = 0; k < nb; ++k) {
         last_l1 = hl[k];
         if (hl[k] < cfg.pr_tol) { conv = true; return r + k + 1; }
@@ -999,6 +1218,13 @@ struct sgs_engine {
   // (InitGraph + Start for each of those queries): CC lanes start from a
   // dense frontier, BFS/SSSP lanes from their sources, then one round loop.
   void start_lanes(Group &G, uint64_t fresh, const std::vector<Query *> &qs) {
+    // a narrow group whose new lanes are all BFS: direction-optimizing
+    // rounds (the in-edge store is built here, before the frontier buffers
+    // are seeded, since building it uses them)
+    bool all_bfs = !G.wide() && fresh != 0;
+    for (int q = 0; q < G.width; ++q)
+      if ((fresh >> q & 1ull) && (G.algo_packed >> (8 * q) & 0xFFu) != (uint32_t)A_BFS) all_bfs = false;
+    const bool diropt = all_bfs && (cfg.pull & 2u) && ensure_in();
     GraphView g = view();
     CK(cudaEventRecord(ev_q.a, s));
     CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * WLANES, s));
@@ -1038,7 +1264,7 @@ struct sgs_engine {
     }
     CK(cudaGetLastError());
     bool conv = false;
-    const uint32_t rounds = group_relax(G, conv);
+    const uint32_t rounds = diropt ? run_bfs_diropt(G, (uint32_t)fresh, conv) : group_relax(G, conv);
     CK(cudaEventRecord(ev_q.b, s));
     sync();
     float ms = 0;
@@ -1757,6 +1983,7 @@ struct sgs_engine {
     unsigned long long ht = 0;
     CK(cudaMemcpyAsync(&ht, tombs, sizeof(ht), cudaMemcpyDeviceToHost, s));
     sync();
+    in_apply(ni, nd, nkept);
     ne = ne + nkept - ht;
     slots_total += nkept;
     est.last_inserted = nkept;
@@ -1936,6 +2163,7 @@ SGS_API void sgs_config_default(sgs_config *c) {
   c->arena_headroom = 0.30;
   c->group_size = 4;
   c->persistent = 2;  // invalidation phases persistent: many small rounds
+  c->pull = 1;  // PageRank sweeps as pulls; bit 1 (direction-optimizing BFS) is opt-in
 }
 
 SGS_API int sgs_create(const sgs_config *cfg, sgs_engine **out) {
@@ -2150,6 +2378,9 @@ SGS_API int sgs_get_engine_stats(sgs_engine *e, sgs_engine_stats *out) {
       e->est.cache_hit_slots = cc[CC_WALK] - std::min(cc[CC_WALK], cc[CC_MISS]);
       e->est.cache_miss_slots = cc[CC_MISS];
     }
+    e->est.in_store_bytes = e->in_built ? e->in_capslots * 4 + (uint64_t)e->nv * 20 : 0;
+    e->est.in_store_builds = e->in_builds;
+    e->est.bfs_bottom_up_rounds = e->bfs_bottom_up_total;
     *out = e->est;
   });
 }

@@ -53,9 +53,9 @@ EXPORTS = [
     "sgs_ppr_get_stats", "sgs_serve", "sgs_autotune", "sgs_cache_refresh",
 ]
 
-K_GROUP, K_GROUP_INVAL, K_PR_PUSH, K_WIDE, K_WIDE_INVAL = range(5)
+K_GROUP, K_GROUP_INVAL, K_PR_PUSH, K_WIDE, K_WIDE_INVAL, K_PR_PULL = range(6)
 KERNEL_KINDS = {"group_relax": K_GROUP, "group_invalidate": K_GROUP_INVAL, "pr_push": K_PR_PUSH,
-                "wide_relax": K_WIDE, "wide_invalidate": K_WIDE_INVAL}
+                "wide_relax": K_WIDE, "wide_invalidate": K_WIDE_INVAL, "pr_pull": K_PR_PULL}
 
 
 class SgsError(RuntimeError):
@@ -80,6 +80,7 @@ class Config(C.Structure):
         ("arena_headroom", C.c_double),
         ("group_size", C.c_uint32),
         ("persistent", C.c_uint32),
+        ("pull", C.c_uint32),
     ]
 
 
@@ -121,6 +122,9 @@ class EngineStats(C.Structure):
         ("last_evicted", C.c_uint64),
         ("cache_hit_slots", C.c_uint64),
         ("cache_miss_slots", C.c_uint64),
+        ("in_store_bytes", C.c_uint64),
+        ("in_store_builds", C.c_uint64),
+        ("bfs_bottom_up_rounds", C.c_uint64),
     ]
 
     def as_dict(self):

@@ -116,6 +116,14 @@ typedef struct sgs_config {
                              rounds launched in batches with one counter
                              read per batch.  Default 2: the invalidation's
                              many small rounds gain most                  */
+  uint32_t pull;          /* bit 0 (default on): PageRank's all-vertex
+                             sweeps as pulls over an in-edge (CSC) store
+                             kept in HBM (built by transposing the graph
+                             when first needed, then updated by every
+                             snapshot); bit 1: BFS-only starts of a narrow
+                             group run direction-optimizing (bottom-up
+                             rounds over the same store when the frontier
+                             is large); 0: push only                      */
 } sgs_config;
 
 typedef struct sgs_query_stats {
@@ -156,6 +164,10 @@ typedef struct sgs_engine_stats {
                                  from the cache (since load)               */
   uint64_t cache_miss_slots;  /* host-tier slots they read over the host link
                                  (since load)                              */
+  uint64_t in_store_bytes;    /* HBM of the in-edge store (0: not built)   */
+  uint64_t in_store_builds;   /* transpositions (first use, and rebuilds when
+                                 a snapshot's relocations did not fit)     */
+  uint64_t bfs_bottom_up_rounds; /* bottom-up BFS rounds run so far        */
 } sgs_engine_stats;
 
 /* Per-kernel-class timing of the relaxation launches (CUDA events on the
@@ -169,7 +181,8 @@ typedef struct sgs_engine_stats {
 #define SGS_K_PR_PUSH 2      /* PageRank residual push                    */
 #define SGS_K_WIDE 3         /* relaxation of a wide query group          */
 #define SGS_K_WIDE_INVAL 4   /* parent-tree invalidation of a wide group  */
-#define SGS_K_COUNT 5
+#define SGS_K_PR_PULL 5      /* PageRank sweep as a pull over in-edges    */
+#define SGS_K_COUNT 6
 typedef struct sgs_kernel_stats {
   uint64_t launches;
   uint64_t slots;      /* positions walked (edges incl. tombstones)          */
