@@ -67,7 +67,8 @@ def parse():
                          "and the launch mode by timing a probe, before the timed region)")
     ap.add_argument("--persistent", type=int, default=None,
                     help="1: each relaxation phase as one cooperative launch over rounds")
-    ap.add_argument("--workload", default="snapshot", choices=["snapshot", "ppr", "batched", "served"],
+    ap.add_argument("--workload", default="snapshot",
+                    choices=["snapshot", "ppr", "batched", "served", "pagerank", "bfs"],
                     help="snapshot: incremental SSSP/BFS/CC (the headline); ppr: weighted "
                          "personalized PageRank forward + adjoint; batched: 256 BFS + 256 SSSP "
                          "queries kept up to date together")
@@ -83,6 +84,12 @@ def parse():
     ap.add_argument("--slots", type=int, default=16)
     ap.add_argument("--plain-sample", type=int, default=32,
                     help="batched workload: queries of the sample run one per edge pass")
+    ap.add_argument("--pull", type=int, default=None,
+                    help="engine pull bits (1: PageRank pull sweeps, 2: direction-optimizing BFS); "
+                         "library default otherwise")
+    ap.add_argument("--pr-scale", type=int, default=16)
+    ap.add_argument("--pr-updates", type=int, default=20_000)
+    ap.add_argument("--bfs-sources", type=int, default=8)
     ap.add_argument("--ppr-scale", type=int, default=22)
     ap.add_argument("--ppr-vectors", type=int, default=64)
     ap.add_argument("--ppr-seeds", type=int, default=32)
@@ -193,8 +200,11 @@ def measured_peak_hbm():
 
 
 def pers(a):
-    """Engine option for --persistent (the library default otherwise)."""
-    return {} if a.persistent is None else {"persistent": int(a.persistent)}
+    """Engine options for --persistent / --pull (the library defaults otherwise)."""
+    o = {} if a.persistent is None else {"persistent": int(a.persistent)}
+    if getattr(a, "pull", None) is not None:
+        o["pull"] = int(a.pull)
+    return o
 
 
 def measure_h2d_gbs(dev, nbytes=1 << 30, reps=3):
@@ -1024,6 +1034,118 @@ def reference_arm(a, R):
     return base
 
 
+def _basic_line(a, R, metric, value, ms, cfg, extra):
+    out = {"metric": metric, "value": round(value, 3), "unit": UNIT, "n_gpus": R.world,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (device R-MAT)",
+           "config": cfg}
+    out.update(extra)
+    return out
+
+
+def pagerank_arm(a, R):
+    """Plain incremental PageRank (the survey's first configuration): R-MAT
+    scale --pr-scale, snapshots of --pr-updates updates (50/50); one step =
+    one snapshot (cancel + compensate + sweeps to the L1 tolerance).  value =
+    edges traversed (active vertices' out-degrees summed over rounds) per
+    second of device time; the static start is reported beside it."""
+    import torch
+
+    import sgs
+
+    dev = torch.device("cuda", R.local)
+    torch.cuda.set_device(dev)
+    e = sgs.Engine(device=R.local, weight_mode=sgs.W_EXPLICIT, **pers(a))
+    e.load_rmat(a.pr_scale, a.edge_factor, a.seed, 0.57, 0.19, 0.19, wseed=a.seed)
+    nv = int(e.engine_stats()["nv"])
+    row, col, _ = e.export()
+    half = a.pr_updates // 2
+    nb = a.warmup + a.steps
+    i_s, i_d, d_s, d_d = sgs.gen_update_stream(nv, row, col, a.seed * 1000003, nb * half, nb * half)
+    i_w = sgs.hash_weights(a.seed, i_s, i_d)
+    del row, col
+    e.kernel_timing(True)
+    q = e.add_query(sgs.PR)
+    st0 = q.stats()
+    kinds0 = e.kernel_stats()
+    edges, ms = 0, 0.0
+    clocks = Clocks(R.local)
+    for k in range(nb):
+        if k == a.warmup:
+            torch.cuda.synchronize()
+            clocks.start()
+        sl = slice(k * half, (k + 1) * half)
+        e.apply_batch(i_s[sl], i_d[sl], i_w[sl], d_s[sl], d_d[sl])
+        if k >= a.warmup:
+            edges += q.stats()["edges_traversed"]
+            ms += e.engine_stats()["last_batch_ms"]
+    clk = clocks.stop()
+    ks = e.kernel_stats()
+    sweep = "pr_pull" if ks["pr_pull"]["launches"] > kinds0["pr_pull"]["launches"] else "pr_push"
+    kd = {k: ks[sweep][k] - kinds0[sweep][k] for k in ("launches", "slots", "bytes_alg", "ms")}
+    peak, src = measured_peak_hbm()
+    ach = kd["bytes_alg"] / (kd["ms"] * 1e-3) / 1e9 if kd["ms"] > 0 else 0.0
+    T = R.max(ms)
+    st = e.engine_stats()
+    e.close()
+    return _basic_line(
+        a, R, f"GTEPS per snapshot (incremental PageRank, R-MAT s{a.pr_scale}, {a.pr_updates} updates/snapshot)",
+        R.sum(edges) / (T * 1e6), T / a.steps,
+        {"workload": f"incremental PageRank, R-MAT scale {a.pr_scale} ef {a.edge_factor} seed {a.seed}, "
+                     f"{a.pr_updates} updates/snapshot (50/50), alpha 0.85, L1 tolerance of the library",
+         "pull": a.pull, "sweep_kernel": sweep, "in_store_bytes": int(st["in_store_bytes"]),
+         "l2": "graph L2-resident at scale 16" if a.pr_scale <= 18 else "graph larger than L2"},
+        {"static": {"ms": round(st0["ms"], 3), "rounds": st0["rounds"],
+                    "gteps": round(st0["edges_traversed"] / (st0["ms"] * 1e6), 3) if st0["ms"] else None},
+         "sweep": {"launches": kd["launches"], "ms": round(kd["ms"], 3), "achieved_gbs": round(ach, 1),
+                   "frac_of_measured_hbm": round(ach / peak, 4), "peak_source": src},
+         "clocks": clk})
+
+
+def bfs_arm(a, R):
+    """Static BFS from scratch (the hybrid_bfs sample's Start): R-MAT scale
+    --scale, --bfs-sources sources (vertex 0 and seeded random ones), each
+    one query in its own group; value = traversed edges (frontier
+    out-degrees summed over rounds, the reference's count) per second of
+    device time.  With --pull 3 the large middle rounds run bottom-up."""
+    import torch
+
+    import sgs
+
+    dev = torch.device("cuda", R.local)
+    torch.cuda.set_device(dev)
+    e = sgs.Engine(device=R.local, weight_mode=sgs.W_EXPLICIT, group_size=1, **pers(a))
+    e.load_rmat(a.scale, a.edge_factor, a.seed, 0.57, 0.19, 0.19, wseed=a.seed)
+    nv = int(e.engine_stats()["nv"])
+    rng = np.random.default_rng(a.seed)
+    srcs = [0] + [int(x) for x in rng.integers(0, nv, a.bfs_sources - 1)]
+    for s_ in srcs[:a.warmup]:  # warm-up starts (and the in-edge store, if used)
+        e.remove_query(e.add_query(sgs.BFS, s_))
+    clocks = Clocks(R.local)
+    torch.cuda.synchronize()
+    clocks.start()
+    edges, ms, reached = 0, 0.0, []
+    for s_ in srcs:
+        q = e.add_query(sgs.BFS, s_)
+        st = q.stats()
+        edges += st["edges_traversed"]
+        ms += st["ms"]
+        reached.append(int(q.summary()[0]))
+        e.remove_query(q)
+    clk = clocks.stop()
+    est = e.engine_stats()
+    e.close()
+    T = R.max(ms)
+    return _basic_line(
+        a, R, f"GTEPS (static BFS from scratch, R-MAT s{a.scale})", R.sum(edges) / (T * 1e6),
+        T / len(srcs),
+        {"workload": f"static BFS, R-MAT scale {a.scale} ef {a.edge_factor} seed {a.seed}, "
+                     f"{len(srcs)} sources (0 and seeded random)", "pull": a.pull,
+         "reached": reached},
+        {"steps": len(srcs), "bottom_up_rounds": int(est["bfs_bottom_up_rounds"]),
+         "in_store_bytes": int(est["in_store_bytes"]), "clocks": clk})
+
+
 def main():
     a = parse()
     R = Ranks()
@@ -1046,6 +1168,10 @@ def main():
             out = batched_arm(a, R)
         elif a.workload == "served":
             out = served_arm(a, R)
+        elif a.workload == "pagerank":
+            out = pagerank_arm(a, R)
+        elif a.workload == "bfs":
+            out = bfs_arm(a, R)
         else:
             out = engine_arm(a, R)
         if R.rank == 0 and out is not None:
