@@ -336,6 +336,9 @@ struct sgs_engine {
   uint32_t grid_map() const { return (uint32_t)nsm * map_cps; }
   uint32_t grid_elem(uint64_t n) const { return blocks_for(n, (uint32_t)nsm * 8); }
   size_t wbytes() const { return cfg.weight_mode == SGS_W_EXPLICIT ? 8 : 4; }
+  // some blocks live in the pinned-host tier (the maps then compile in the
+  // host-tier logic: hotness, cache lookups, link accounting)
+  bool host_tier() const { return split < nv; }
 
   void cub_ensure(size_t bytes) { cub_tmp.ensure(bytes); }
 
@@ -851,7 +854,8 @@ struct sgs_engine {
   template <class Op>
   void launch_wide(uint32_t rr, const Op &op, unsigned long long *lane_changes) {
     const bool hp = rr >= 1;
-    { ++n_launch; wide_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
+    auto k = host_tier() ? wide_map<Op, true> : wide_map<Op, false>;
+    { ++n_launch; k<<<grid_map(), RELAX_THREADS, 0, s>>>(
         view(), fview(rr, cnt.p + rr), fview(rr + 1, cnt.p + rr + 1), op, wm[rr % 3].p,
         wm[(rr + 1) % 3].p, hp ? fb[(rr - 1) % 3].vtx.p : nullptr,
         hp ? cnt.p + rr - 1 : nullptr, hp ? wm[(rr - 1) % 3].p : nullptr, b_lane.p,
@@ -861,7 +865,8 @@ struct sgs_engine {
   template <class Op>
   void launch_group(uint32_t rr, const Op &op) {
     const bool hp = rr >= 1;
-    { ++n_launch; group_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
+    auto k = host_tier() ? group_map<Op, true> : group_map<Op, false>;
+    { ++n_launch; k<<<grid_map(), RELAX_THREADS, 0, s>>>(
         fview(rr, cnt.p + rr), fview(rr + 1, cnt.p + rr + 1), op,
         hp ? fb[(rr - 1) % 3].vtx.p : nullptr, hp ? cnt.p + rr - 1 : nullptr,
         hp ? gm[(rr - 1) % 3].p : nullptr, b_lane.p, rstat.p + rr, hstat.p + rr); }
@@ -1038,7 +1043,7 @@ struct sgs_engine {
     uint32_t *ro = d_rounds.p;
     Op o = op;
     void *args[] = {&rb, &o, &r0, &maxr, &le, &rs, &hs, &ro};
-    const void *f = (const void *)group_rounds<Op>;
+    const void *f = host_tier() ? (const void *)group_rounds<Op, true> : (const void *)group_rounds<Op, false>;
     if (ktiming) { ensure_kev(2); CK(cudaEventRecord(kev[0], s)); }
     ++n_launch;
     CK(cudaLaunchCooperativeKernel(f, coop_grid(f), RELAX_THREADS, args, 0, s));
@@ -1059,7 +1064,7 @@ struct sgs_engine {
     uint32_t *ro = d_rounds.p;
     Op o = op;
     void *args[] = {&g, &rb, &o, &r0, &maxr, &le, &lc, &rs, &ro};
-    const void *f = (const void *)wide_rounds<Op>;
+    const void *f = host_tier() ? (const void *)wide_rounds<Op, true> : (const void *)wide_rounds<Op, false>;
     if (ktiming) { ensure_kev(2); CK(cudaEventRecord(kev[0], s)); }
     ++n_launch;
     CK(cudaLaunchCooperativeKernel(f, coop_grid(f), RELAX_THREADS, args, 0, s));

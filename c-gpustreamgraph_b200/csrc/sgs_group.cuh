@@ -86,10 +86,17 @@ struct GroupRelaxOp {
   struct Quad {
     uint4 ids, ws;
   };
+  // H: the graph has a host tier (blocks may be host-resident or cached)
+  template <bool H>
   __device__ __forceinline__ Quad fetch(const Payload &p, uint32_t j0) const {
     Quad q;
-    q.ids = ld_quad(adj_at(g, p.off, j0));
-    q.ws = any_w ? ld_quad(wgt_at(g, p.off, j0)) : make_uint4(1, 1, 1, 1);
+    if constexpr (H) {
+      q.ids = ld_quad(adj_at(g, p.off, j0));
+      q.ws = any_w ? ld_quad(wgt_at(g, p.off, j0)) : make_uint4(1, 1, 1, 1);
+    } else {
+      q.ids = ld_quad(g.adj_d + p.off + j0);
+      q.ws = any_w ? ld_quad(g.wgt_d + p.off + j0) : make_uint4(1, 1, 1, 1);
+    }
     return q;
   }
   // Returns a 4-bit mask of destinations to append; dst[] holds them.
@@ -172,8 +179,10 @@ struct GroupInvalidateOp {
   struct Quad {
     uint4 ids;
   };
+  template <bool H>
   __device__ __forceinline__ Quad fetch(const Payload &p, uint32_t j0) const {
-    return Quad{ld_quad(adj_at(g, p.off, j0))};
+    if constexpr (H) return Quad{ld_quad(adj_at(g, p.off, j0))};
+    else return Quad{ld_quad(g.adj_d + p.off + j0)};
   }
   __device__ __forceinline__ uint32_t visit4(uint32_t u, const Payload &p, uint32_t j0, uint32_t len,
                                              const Quad &qd, uint32_t (&dst)[4]) const {
@@ -218,7 +227,9 @@ struct GroupInvalidateOp {
 #ifndef SGS_GROUP_MIN_BLOCKS
 #define SGS_GROUP_MIN_BLOCKS 4  // resident CTAs per SM the register budget allows
 #endif
-template <class Op>
+// H = false when every block is in HBM (no host tier): the host-tier logic
+// (hotness, cache lookups, link accounting) is compiled out.
+template <class Op, bool H>
 __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out, const Op &op,
                                                const uint32_t *prev_vtx,
                                                const unsigned long long *prev_cnt, uint32_t *prev_mask,
@@ -250,6 +261,7 @@ __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out
     uint32_t s = __ldcg(&in.ustart[ub]);
     for (;;) {
       __syncthreads();
+      bool host = false;  // this thread staged a host-tier entry
 #pragma unroll
       for (int h = 0; h < GC / RELAX_THREADS; ++h) {
         const uint32_t t = threadIdx.x + h * RELAX_THREADS;
@@ -265,12 +277,15 @@ __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out
           s_vtx[t] = v;
           s_len[t] = __ldcg(&in.len[idx]);
           P pay = op.load(v);
-          if (pay.off & HOST_BIT) {
-            if (eb >= E0) {
-              hot_bump(op.g, v, pay.off);
-              if (op.g.cstat) atomicAdd(&s_all, (unsigned long long)s_len[t]);
+          if constexpr (H) {
+            if (pay.off & HOST_BIT) {
+              host = true;
+              if (eb >= E0) {
+                hot_bump(op.g, v, pay.off);
+                if (op.g.cstat) atomicAdd(&s_all, (unsigned long long)s_len[t]);
+              }
+              pay.off = resolve_block(op.g, pay.off, s_len[t]);
             }
-            pay.off = resolve_block(op.g, pay.off, s_len[t]);
           }
           s_pay[t] = pay;
           if (eb >= E0 && pay.mask) {
@@ -280,7 +295,11 @@ __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out
           }
         }
       }
-      __syncthreads();
+      // the barrier also tells every thread whether the chunk holds
+      // host-tier entries (only then does the walk account host reads)
+      bool chunk_host = false;
+      if constexpr (H) chunk_host = __syncthreads_or(host) != 0;
+      else __syncthreads();
       const uint64_t lo = max(E0, s_eb[0]);
       const uint64_t hi = min(E1, s_eb[GC]);
       // Software pipeline: the owner search and id load of a thread's next
@@ -303,21 +322,23 @@ __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out
       uint32_t jc = 0;
       typename Op::Quad qc{};
       const bool hc0 = locate(lo + 4 * threadIdx.x, lc, jc);
-      if (hc0) qc = op.fetch(s_pay[lc], jc);
+      if (hc0) qc = op.template fetch<H>(s_pay[lc], jc);
       bool hc = hc0;
       for (uint64_t base = lo; base < hi; base += 4 * RELAX_THREADS) {
         int ln = 0;
         uint32_t jn = 0;
         typename Op::Quad qn{};
         const bool hn = locate(base + 4 * RELAX_THREADS + 4 * threadIdx.x, ln, jn);
-        if (hn) qn = op.fetch(s_pay[ln], jn);
+        if (hn) qn = op.template fetch<H>(s_pay[ln], jn);
         uint32_t app = 0;
         uint32_t dst[4] = {0, 0, 0, 0};
         if (hc) {
           app = op.visit4(s_vtx[lc], s_pay[lc], jc, s_len[lc], qc, dst);
-          const uint64_t o = s_pay[lc].off;
-          if ((o & HOST_BIT) && cache_line(op.g, (o & OFF_MASK) + jc) == NO_LINE)
-            host_acc += min(4u, s_len[lc] - jc);
+          if (H && chunk_host) {
+            const uint64_t o = s_pay[lc].off;
+            if ((o & HOST_BIT) && cache_line(op.g, (o & OFF_MASK) + jc) == NO_LINE)
+              host_acc += min(4u, s_len[lc] - jc);
+          }
         }
         lc = ln;
         jc = jn;
@@ -355,13 +376,13 @@ __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out
   __syncthreads();  // shared state is reused when the body runs again
 }
 
-template <class Op>
+template <class Op, bool H>
 __global__ void __launch_bounds__(RELAX_THREADS, SGS_GROUP_MIN_BLOCKS)
     group_map(FrontierView in, FrontierView out, Op op, const uint32_t *prev_vtx,
               const unsigned long long *prev_cnt, uint32_t *prev_mask,
               unsigned long long *lane_edges, unsigned long long *edge_stat,
               unsigned long long *host_stat) {
-  group_map_body(in, out, op, prev_vtx, prev_cnt, prev_mask, lane_edges, edge_stat, host_stat);
+  group_map_body<Op, H>(in, out, op, prev_vtx, prev_cnt, prev_mask, lane_edges, edge_stat, host_stat);
 }
 
 // The three rotating frontier buffers, their counters and lane masks, as one
@@ -394,7 +415,7 @@ struct RoundBufs {
 // nothing.  The masks of the last non-empty frontier are cleared before the
 // kernel returns; *rounds_out = the first empty frontier's index (or
 // max_rounds when the limit is hit).
-template <class Op>
+template <class Op, bool H>
 __global__ void __launch_bounds__(RELAX_THREADS, SGS_GROUP_MIN_BLOCKS)
     group_rounds(RoundBufs<uint32_t> rb, Op op, uint32_t r0, uint32_t max_rounds,
                  unsigned long long *lane_edges, unsigned long long *rstat, unsigned long long *hstat,
@@ -407,7 +428,7 @@ __global__ void __launch_bounds__(RELAX_THREADS, SGS_GROUP_MIN_BLOCKS)
     o.m_in = rb.mask[r % 3];
     o.m_out = rb.mask[(r + 1) % 3];
     const bool hp = r >= 1;
-    group_map_body(rb.view(r), rb.view(r + 1), o, hp ? rb.vtx[(r - 1) % 3] : nullptr,
+    group_map_body<Op, H>(rb.view(r), rb.view(r + 1), o, hp ? rb.vtx[(r - 1) % 3] : nullptr,
                    hp ? rb.cnt + r - 1 : nullptr, hp ? rb.mask[(r - 1) % 3] : nullptr, lane_edges,
                    rstat + r, hstat + r);
     __threadfence();

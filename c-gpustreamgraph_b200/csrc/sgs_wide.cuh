@@ -126,7 +126,8 @@ struct WideInvalidateOp {
 // lane_changes counts the lanes changed (resets for the invalidation op);
 // edge_stat receives the (lane, edge) pairs actually evaluated -- fewer than
 // the traversed count when a restricted round skips destinations.
-template <class Op>
+// H = false: every block is in HBM and the host-tier logic is compiled out.
+template <class Op, bool H>
 __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView in, FrontierView out,
                                               const Op &op, const unsigned long long *m_in,
                                               unsigned long long *m_out, const uint32_t *prev_vtx,
@@ -188,7 +189,7 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
           s_len[h] = __ldcg(&in.len[idx]);
           const uint64_t o = g.off[v];
           s_mask[h] = __ldcg(&m_in[v]);
-          if (o & HOST_BIT) {
+          if (H && (o & HOST_BIT)) {
             if (eb >= E0) {
               hot_bump(g, v, o);
               if (g.cstat) atomicAdd(&s_host, (unsigned long long)s_len[h]);
@@ -235,7 +236,7 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
             // slot position in its arena: HBM, cache line or host
             uint64_t x = s_off[l] + j;
             int tier = 0;
-            if (x & HOST_BIT) {
+            if (H && (x & HOST_BIT)) {
               x &= OFF_MASK;
               const uint32_t m = cache_line(g, x);
               tier = m != NO_LINE ? 1 : 2;
@@ -330,20 +331,20 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
   __syncthreads();  // shared state is reused when the body runs again
 }
 
-template <class Op>
+template <class Op, bool H>
 __global__ void __launch_bounds__(RELAX_THREADS, 3)
     wide_map(GraphView g, FrontierView in, FrontierView out, Op op,
              const unsigned long long *m_in, unsigned long long *m_out, const uint32_t *prev_vtx,
              const unsigned long long *prev_cnt, unsigned long long *prev_mask,
              unsigned long long *lane_edges, unsigned long long *lane_changes,
              unsigned long long *edge_stat) {
-  wide_map_body(g, in, out, op, m_in, m_out, prev_vtx, prev_cnt, prev_mask, lane_edges,
-                lane_changes, edge_stat);
+  wide_map_body<Op, H>(g, in, out, op, m_in, m_out, prev_vtx, prev_cnt, prev_mask, lane_edges,
+                       lane_changes, edge_stat);
 }
 
 // Rounds r0, r0+1, ... of a wide phase in one cooperative launch (see
 // group_rounds).
-template <class Op>
+template <class Op, bool H>
 __global__ void __launch_bounds__(RELAX_THREADS, 3)
     wide_rounds(GraphView g, RoundBufs<unsigned long long> rb, Op op, uint32_t r0, uint32_t max_rounds,
                 unsigned long long *lane_edges, unsigned long long *lane_changes,
@@ -353,7 +354,7 @@ __global__ void __launch_bounds__(RELAX_THREADS, 3)
   bool conv = false;
   for (; r < max_rounds; ++r) {
     const bool hp = r >= 1;
-    wide_map_body(g, rb.view(r), rb.view(r + 1), op, rb.mask[r % 3], rb.mask[(r + 1) % 3],
+    wide_map_body<Op, H>(g, rb.view(r), rb.view(r + 1), op, rb.mask[r % 3], rb.mask[(r + 1) % 3],
                   hp ? rb.vtx[(r - 1) % 3] : nullptr, hp ? rb.cnt + r - 1 : nullptr,
                   hp ? rb.mask[(r - 1) % 3] : nullptr, lane_edges, lane_changes, rstat + r);
     __threadfence();
