@@ -87,6 +87,9 @@ def parse():
     ap.add_argument("--pull", type=int, default=None,
                     help="engine pull bits (1: PageRank pull sweeps, 2: direction-optimizing BFS); "
                          "library default otherwise")
+    ap.add_argument("--host-policy", type=int, default=None,
+                    help="reads of the host tier in a repair (-hybrid): 0 zero-copy, 1 explicit copy "
+                         "every snapshot, 2 explicit copy for dense repairs; library default otherwise")
     ap.add_argument("--pr-scale", type=int, default=16)
     ap.add_argument("--pr-updates", type=int, default=20_000)
     ap.add_argument("--bfs-sources", type=int, default=8)
@@ -204,6 +207,8 @@ def pers(a):
     o = {} if a.persistent is None else {"persistent": int(a.persistent)}
     if getattr(a, "pull", None) is not None:
         o["pull"] = int(a.pull)
+    if getattr(a, "host_policy", None) is not None:
+        o["host_policy"] = int(a.host_policy)
     return o
 
 
@@ -435,7 +440,8 @@ def engine_arm(a, R):
                        st["arena_bytes_hbm"] / 1e9, L2_BYTES // 2**20),
                    "parallelism": "replicas" if R.world > 1 else "single GPU",
                    "queries": ["sssp:0", "bfs:0", "cc"],
-                   "autotune": tune, "persistent": a.persistent, "edge_cache": cache},
+                   "autotune": tune, "persistent": a.persistent, "edge_cache": cache,
+                   "host_policy": a.host_policy, "host_stagings": int(st["host_stagings"])},
         "e2e": e2e,
         "gpu_launches": gpu_launches,
         "roofline": roof,

@@ -131,6 +131,9 @@ int main(int argc, char **argv) {
   if (SGS_APP == SGS_PR) c.pr_tol = f.num("error", 1e-6) * (1.0 - c.pr_alpha);
   // -pull: bit 0 PageRank pull sweeps, bit 1 direction-optimizing BFS starts
   c.pull = (uint32_t)f.num("pull", SGS_APP == SGS_BFS ? 3 : 1);
+  // -hybrid: 0 zero-copy, 1 explicit copy of the host tier for every repair,
+  // 2 explicit copy for dense repairs (hybrid_policy.h:241-279)
+  c.host_policy = (uint32_t)f.num("hybrid", 0);
   try {
     using clk = std::chrono::steady_clock;
     sgs::Engine engine(SGS_APP, &c);

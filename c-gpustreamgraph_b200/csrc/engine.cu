@@ -274,6 +274,12 @@ struct sgs_engine {
   uint64_t in_builds = 0;
   DBuf<uint64_t> t_dkeys, t_ikeys, t_tmp;  // the batch's keys transposed
 
+  // explicit-copy host policy (cfg.host_policy): the used host arena copied
+  // to HBM by the copy engine for a snapshot's repair, readers pointed at it
+  DBuf<uint32_t> stage_adj, stage_wgt;
+  bool staged = false;
+  uint64_t stage_bytes_last = 0, stagings = 0;
+
   ~sgs_engine() {
     if (s2) {
       cudaStreamSynchronize(s2);
@@ -296,8 +302,8 @@ struct sgs_engine {
     g.cap = cap.p;
     g.adj_d = adj_d.p;
     g.wgt_d = wgt_d.p;
-    g.adj_h = adj_h.p;
-    g.wgt_h = wgt_h.p;
+    g.adj_h = staged ? stage_adj.p : adj_h.p;
+    g.wgt_h = staged ? stage_wgt.p : wgt_h.p;
     g.wmode = cfg.weight_mode;
     if (cache_on && h_lines) {
       g.cmap = cmap.p;
@@ -461,6 +467,47 @@ struct sgs_engine {
     CK(cudaEventRecord(ev_ccopy, s2));
     c_pending = true;
     ++c_admissions;
+  }
+
+  // ------------------------------------------------ explicit host policy
+  // The reference's -hybrid policies (framework/hybrid_policy.h:241-279,
+  // framework.cuh:2012-2180) read a segment either zero-copy or after an
+  // explicit copy of its edges into device buffers (edge_dst_exp,
+  // csr_graph.cuh:1877-1884), the explicit form chosen for every segment
+  // (-hybrid 1) or for segments whose active share exceeds alpha (-hybrid 2).
+  // Here: policy 1 copies the used host arena to HBM with the copy engine
+  // (cudaMemcpyAsync, chunks of 1 GiB) before every snapshot's repair;
+  // policy 2 only when the repair's first frontier covers more than half of
+  // the graph's slots (the dense re-push after deletions).  Relaxation rounds
+  // only read blocks, and the snapshot's writes happened before, so the
+  // copy stays exact for the whole repair.
+  bool stage_wanted() {
+    if (!cfg.host_policy || !host_tier() || staged) return false;
+    if (cfg.host_policy == 1) return true;
+    unsigned long long c = 0;
+    CK(cudaMemcpyAsync(&c, cnt.p, sizeof(c), cudaMemcpyDeviceToHost, s));
+    sync();
+    return (double)(c & EDGE_MASK) > 0.5 * (double)slots_total;
+  }
+  void stage_host() {
+    unsigned long long tops[2];
+    CK(cudaMemcpyAsync(tops, arena_top.p, sizeof(tops), cudaMemcpyDeviceToHost, s));
+    sync();
+    const uint64_t n = std::min<uint64_t>(tops[1], arena_cap[1]);
+    if (!n) return;
+    const bool ew = cfg.weight_mode == SGS_W_EXPLICIT;
+    stage_adj.ensure(n);
+    if (ew) stage_wgt.ensure(n);
+    const uint64_t chunk = (1ull << 30) / sizeof(uint32_t);
+    for (uint64_t o = 0; o < n; o += chunk) {
+      const uint64_t k = std::min(chunk, n - o);
+      CK(cudaMemcpyAsync(stage_adj.p + o, adj_h.p + o, k * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+      if (ew)
+        CK(cudaMemcpyAsync(stage_wgt.p + o, wgt_h.p + o, k * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    }
+    staged = true;
+    stage_bytes_last = n * (ew ? 8 : 4);
+    ++stagings;
   }
 
   // -------------------------------------------------------- in-edge store
@@ -1633,6 +1680,7 @@ struct sgs_engine {
     if ((ni && (!is || !id)) || (nd && (!ds || !dd))) fail(SGS_ERR_INVALID, "null batch array");
     const bool explicit_w = cfg.weight_mode == SGS_W_EXPLICIT;
     if (ni && explicit_w && !iw) fail(SGS_ERR_INVALID, "explicit weight mode needs insert weights");
+    staged = false;  // the host arena itself is what the update writes
     GraphView g = view();
     Range snap("sgs:snapshot");
     CK(cudaEventRecord(ev_batch.a, s));
@@ -1842,6 +1890,7 @@ struct sgs_engine {
             g, G.st.p, G.val.p, (uint32_t)G.used, G.algo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr,
             b_nkept.p, gm[0].p, fview(0, cnt.p), b_lane.p, resets); }
       CK(cudaGetLastError());
+      if (stage_wanted()) stage_host();  // explicit host policy: repair reads an HBM copy
       // wide: the inserted edges after the restricted round 0, into its
       // output frontier (round 0 is empty when nothing was reset)
       const std::function<void()> ins_after0 = [&] {
@@ -1857,6 +1906,7 @@ struct sgs_engine {
       CK(cudaMemcpyAsync(G.dstat.p + 2 * WLANES, b_lane.p, sizeof(unsigned long long) * WLANES,
                          cudaMemcpyDeviceToDevice, s));
     }
+    staged = false;  // back to the host arena (zero-copy) for everything else
     cache_publish();  // the snapshot ends when its line copies are visible
     // per-lane counters of every group, one read
     h_gstat.resize(3 * WLANES * std::max<size_t>(ng, 1));
@@ -2169,6 +2219,7 @@ SGS_API void sgs_config_default(sgs_config *c) {
   c->group_size = 4;
   c->persistent = 2;  // invalidation phases persistent: many small rounds
   c->pull = 1;  // PageRank sweeps as pulls; bit 1 (direction-optimizing BFS) is opt-in
+  c->host_policy = 0;  // zero-copy reads of the host tier
 }
 
 SGS_API int sgs_create(const sgs_config *cfg, sgs_engine **out) {
@@ -2386,6 +2437,8 @@ SGS_API int sgs_get_engine_stats(sgs_engine *e, sgs_engine_stats *out) {
     e->est.in_store_bytes = e->in_built ? e->in_capslots * 4 + (uint64_t)e->nv * 20 : 0;
     e->est.in_store_builds = e->in_builds;
     e->est.bfs_bottom_up_rounds = e->bfs_bottom_up_total;
+    e->est.host_stagings = e->stagings;
+    e->est.last_stage_bytes = e->stage_bytes_last;
     *out = e->est;
   });
 }

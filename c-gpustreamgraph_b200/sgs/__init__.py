@@ -81,6 +81,7 @@ class Config(C.Structure):
         ("group_size", C.c_uint32),
         ("persistent", C.c_uint32),
         ("pull", C.c_uint32),
+        ("host_policy", C.c_uint32),
     ]
 
 
@@ -125,6 +126,8 @@ class EngineStats(C.Structure):
         ("in_store_bytes", C.c_uint64),
         ("in_store_builds", C.c_uint64),
         ("bfs_bottom_up_rounds", C.c_uint64),
+        ("host_stagings", C.c_uint64),
+        ("last_stage_bytes", C.c_uint64),
     ]
 
     def as_dict(self):

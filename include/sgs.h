@@ -124,6 +124,12 @@ typedef struct sgs_config {
                              group run direction-optimizing (bottom-up
                              rounds over the same store when the frontier
                              is large); 0: push only                      */
+  uint32_t host_policy;   /* reads of the host tier during a snapshot's
+                             repair (-hybrid): 0 zero-copy (default); 1 the
+                             used host arena copied to HBM by the copy
+                             engine before every repair; 2 that copy only
+                             when the repair's first frontier covers more
+                             than half of the slots                        */
 } sgs_config;
 
 typedef struct sgs_query_stats {
@@ -168,6 +174,8 @@ typedef struct sgs_engine_stats {
   uint64_t in_store_builds;   /* transpositions (first use, and rebuilds when
                                  a snapshot's relocations did not fit)     */
   uint64_t bfs_bottom_up_rounds; /* bottom-up BFS rounds run so far        */
+  uint64_t host_stagings;     /* explicit copies of the host tier so far   */
+  uint64_t last_stage_bytes;  /* bytes of the last one                     */
 } sgs_engine_stats;
 
 /* Per-kernel-class timing of the relaxation launches (CUDA events on the

@@ -122,3 +122,28 @@ def test_cache_needs_a_budget():
         st = e.engine_stats()
         assert st["cache_lines"] == 0 and st["arena_bytes_host"] == 0
         check_query(q, Mirror(nv, row, col, w), sgs.W_EXPLICIT)
+
+
+@pytest.mark.parametrize("policy", [1, 2])
+def test_explicit_host_policy(policy):
+    """-hybrid 1/2: the repair reads an HBM copy of the host tier made by the
+    copy engine (every snapshot, or only for dense repairs); results exact."""
+    nv, row, col, w = _graph(13, 16, 4, 6)
+    gb = len(col) * 8 / 1e9
+    with sgs.Engine(hbm_budget_gb=0.2 * gb, segments=64, host_policy=policy) as e:
+        e.load_csr(nv, row, col, w)
+        m = Mirror(nv, row, col, w)
+        qs = [e.add_query(sgs.SSSP, 0), e.add_query(sgs.BFS, 3), e.add_query(sgs.CC)]
+        for k in range(3):
+            b = _batch(m.nv, m.row, m.col, 90 + k, 1500, 1500 if k != 1 else 0, 6)
+            e.apply_batch(*b)
+            m.apply(*b)
+            for q in qs:
+                check_query(q, m, sgs.W_EXPLICIT)
+        check_graph(e, m)
+        st = e.engine_stats()
+        assert st["arena_bytes_host"] > 0
+        if policy == 1:
+            assert st["host_stagings"] == 3 and st["last_stage_bytes"] > 0
+        else:
+            assert 1 <= st["host_stagings"] <= 3
