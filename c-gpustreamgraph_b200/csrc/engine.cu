@@ -280,6 +280,12 @@ struct sgs_engine {
   bool staged = false;
   uint64_t stage_bytes_last = 0, stagings = 0;
 
+  // the value vector of the last removed PageRank query: the next PageRank
+  // start continues from it (its residual on the current graph is computed
+  // first), so a query after a few updates needs few rounds
+  DBuf<double> pr_warm;
+  uint64_t pr_warm_starts = 0;
+
   ~sgs_engine() {
     if (s2) {
       cudaStreamSynchronize(s2);
@@ -516,7 +522,7 @@ struct sgs_engine {
   // in-block through a per-destination cursor.  Uses frontier buffers 0 and
   // 1 and counters special(0..1): callers build it before they seed a
   // frontier (or after the last one they use).
-  void in_build() {
+  void in_build(FrontierView f0, FrontierView f1) {
     const GraphView g = view();
     in_slots.ensure(nv);
     in_live.ensure(nv);
@@ -524,11 +530,9 @@ struct sgs_engine {
     in_off.ensure((size_t)nv + 1);
     in_top.ensure(2);
     CK(cudaMemsetAsync(in_slots.p, 0, sizeof(uint32_t) * nv, s));
-    CK(cudaMemsetAsync(special(0), 0, sizeof(unsigned long long) * 2, s));
-    FrontierView f0 = fview(0, special(0));
+    CK(cudaMemsetAsync(f0.counter, 0, sizeof(unsigned long long), s));
     { ++n_launch; k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(g, f0); }
-    { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(f0, fview(1, special(1)),
-                                                 InCountOp{g, in_slots.p}, nullptr); }
+    { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(f0, f1, InCountOp{g, in_slots.p}, nullptr); }
     { ++n_launch; k_layout_caps<<<grid_elem(nv), 256, 0, s>>>(in_slots.p, nv, cfg.slack_div, in_cap.p); }
     { ++n_launch; k_u32_to_u64<<<grid_elem(nv), 256, 0, s>>>(in_cap.p, nv, in_off.p); }
     CK(cudaMemsetAsync(in_off.p + nv, 0, sizeof(uint64_t), s));
@@ -545,7 +549,7 @@ struct sgs_engine {
     CK(cudaMemcpyAsync(in_top.p, tops, sizeof(tops), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(in_live.p, 0, sizeof(uint32_t) * nv, s));  // the fill cursors
     { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
-        f0, fview(1, special(1)), InFillOp{g, in_off.p, in_live.p, in_adj.p}, nullptr); }
+        f0, f1, InFillOp{g, in_off.p, in_live.p, in_adj.p}, nullptr); }
     CK(cudaMemcpyAsync(in_live.p, in_slots.p, sizeof(uint32_t) * nv, cudaMemcpyDeviceToDevice, s));
     CK(cudaGetLastError());
     sync();
@@ -562,11 +566,12 @@ struct sgs_engine {
   }
   // True when the in-store is there (built now if needed).  If it cannot be
   // allocated the engine keeps to push sweeps (both run on the GPU).
-  bool ensure_in() {
+  bool ensure_in() { return ensure_in(fview(0, special(0)), fview(1, special(1))); }
+  bool ensure_in(FrontierView f0, FrontierView f1) {
     if (!cfg.pull || in_failed) return false;
     if (in_built) return true;
     try {
-      in_build();
+      in_build(f0, f1);
     } catch (const SgsError &f) {
       if (f.code != SGS_ERR_OOM) throw;
       in_release();
@@ -620,7 +625,7 @@ struct sgs_engine {
     CK(cudaMemcpyAsync(tops, in_top.p, sizeof(tops), cudaMemcpyDeviceToHost, s));
     sync();
     if (tops[0] + h[0] > in_capslots) {  // no room for the relocations: transpose again
-      in_build();
+      in_build(fview(0, special(0)), fview(1, special(1)));
       return;
     }
     rl_vtx.ensure(nkept + 1);
@@ -662,6 +667,7 @@ struct sgs_engine {
     loaded = false;
     in_release();
     in_failed = false;
+    pr_warm.release();
     est = sgs_engine_stats{};
     nv = n;
     uint64_t ne_in = 0;
@@ -1189,39 +1195,49 @@ struct sgs_engine {
   // in-edge store when it is there (cfg.pull), else a push over the
   // out-blocks with FP64 atomics.
   uint32_t pr_rounds(Query &q, unsigned long long *edge_stat, bool &conv, double &last_l1) {
-    GraphView g = view();
     const bool pull = (cfg.pull & 1u) && ensure_in();
-    const GraphView gi = pull ? in_view() : g;
+    const GraphView gi = pull ? in_view() : view();
     reset_counters(0);
     { ++n_launch; k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(gi, fview(0, cnt.p)); }
     const uint32_t maxr = cfg.max_rounds;
     CK(cudaMemsetAsync(l1.p, 0, sizeof(double) * (maxr + 2), s));
-    std::vector<double> hl(maxr + 2);
+    unsigned long long pr_in = 0;
+    CK(cudaMemcpyAsync(&pr_in, cnt.p, sizeof(pr_in), cudaMemcpyDeviceToHost, s));
+    sync();
+    return pr_steps(q, fview(0, cnt.p), fview(1, cnt.p + 1), pull, l1.p, 0, maxr, edge_stat, pr_in, conv,
+                    last_l1);
+  }
+
+  // Rounds r0, r0+1, ... (at most `limit`) over a prebuilt dense frontier
+  // `fin` of the store the sweep reads (in-edge store when `pull`); per-round
+  // absorbed L1 in l1buf[r].  Returns the rounds run; conv when a round's L1
+  // falls below pr_tol.
+  uint32_t pr_steps(Query &q, FrontierView fin, FrontierView fout, bool pull, double *l1buf, uint32_t r0,
+                    uint32_t limit, unsigned long long *edge_stat, unsigned long long pr_in, bool &conv,
+                    double &last_l1) {
+    const GraphView g = view();
+    const GraphView gi = pull ? in_view() : g;
+    std::vector<double> hl(34);
     uint32_t r = 0, rb = 8;
     conv = false;
     last_l1 = 0;
     PrPushOp op{g, q.pv.p, q.r.p};
-    unsigned long long pr_in = 0;
-    CK(cudaMemcpyAsync(&pr_in, cnt.p, sizeof(pr_in), cudaMemcpyDeviceToHost, s));
-    sync();
     const unsigned long long pr_inst = (pr_in & EDGE_MASK);
-    while (r < maxr) {
-      const uint32_t nb = std::min(rb, maxr - r);
+    while (r < limit) {
+      const uint32_t nb = std::min(rb, limit - r);
       if (ktiming) ensure_kev(2 * nb);
       for (uint32_t k = 0; k < nb; ++k) {
         { ++n_launch; k_pr_absorb<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(g, q.x.p, q.r.p, q.pv.p, cfg.pr_alpha,
-                                                           l1.p + r + k); }
+                                                           l1buf + r0 + r + k); }
         if (ktiming) CK(cudaEventRecord(kev[2 * k], s));
         if (pull)
-          { ++n_launch; k_pull_pr<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, cnt.p), gi, q.pv.p, q.r.p,
-                                                         edge_stat); }
+          { ++n_launch; k_pull_pr<<<grid_map(), RELAX_THREADS, 0, s>>>(fin, gi, q.pv.p, q.r.p, edge_stat); }
         else
-          { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, cnt.p), fview(1, cnt.p + 1), op,
-                                                       edge_stat); }
+          { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fin, fout, op, edge_stat); }
         if (ktiming) CK(cudaEventRecord(kev[2 * k + 1], s));
       }
       CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(hl.data(), l1.p + r, sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(hl.data(), l1buf + r0 + r, sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
       sync();
       if (ktiming)
         for (uint32_t k = 0; k < nb; ++k)
@@ -1237,6 +1253,97 @@ struct sgs_engine {
     return r;
   }
 
+  // ------------------------------------------------------- PageRank jobs
+  // A PageRank computation the served loop advances a few rounds at a time
+  // between the steps of its query flight.  It has its own frontier buffers
+  // and counters, so its rounds do not disturb the flight's.
+  struct PrJob {
+    Query *q = nullptr;
+    bool pull = false;
+    uint32_t r = 0;
+    Frontier f;
+    uint32_t ucap = 0;
+    DBuf<unsigned long long> c;  // [0] frontier counter, [1] output counter, [2] edge count
+    DBuf<double> l1;
+    unsigned long long pr_in = 0;
+    float ms = 0;
+  } job;
+  FrontierView job_view(uint32_t k) {
+    FrontierView f;
+    f.vtx = job.f.vtx.p;
+    f.len = job.f.len.p;
+    f.ebase = job.f.ebase.p;
+    f.ustart = job.f.ustart.p;
+    f.counter = (uint64_t *)(job.c.p + k);
+    f.ucap = job.ucap;
+    return f;
+  }
+  int pr_job_start() {
+    if (job.q) fail(SGS_ERR_STATE, "a PageRank job is already running");
+    // frontier buffers of the job, sized for a dense frontier of either store
+    const uint64_t max_pos = slots_total + 3ull * nv;
+    job.ucap = (uint32_t)std::min<uint64_t>(max_pos / UNIT + 2, 0xFFFFFFF0ull);
+    job.f.vtx.ensure((size_t)nv + 1);
+    job.f.len.ensure((size_t)nv + 1);
+    job.f.ebase.ensure((size_t)nv + 1);
+    job.f.ustart.ensure(job.ucap);
+    job.c.ensure(3);
+    job.l1.ensure(cfg.max_rounds + 2);
+    job.pull = (cfg.pull & 1u) && ensure_in(job_view(0), job_view(1));
+    auto q = std::make_unique<Query>();
+    q->id = next_qid++;
+    q->algo = SGS_PR;
+    q->x.ensure(nv);
+    q->r.ensure(nv);
+    q->pv.ensure(nv);
+    CK(cudaEventRecord(ev_q.a, s));
+    pr_init(*q, job_view(0), job_view(1));
+    CK(cudaMemsetAsync(job.c.p, 0, sizeof(unsigned long long) * 3, s));
+    const GraphView gi = job.pull ? in_view() : view();
+    { ++n_launch; k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(gi, job_view(0)); }
+    CK(cudaMemsetAsync(job.l1.p, 0, sizeof(double) * (cfg.max_rounds + 2), s));
+    CK(cudaMemcpyAsync(&job.pr_in, job.c.p, sizeof(job.pr_in), cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(ev_q.b, s));
+    sync();
+    CK(cudaEventElapsedTime(&job.ms, ev_q.a, ev_q.b));
+    job.r = 0;
+    job.q = q.get();
+    q->stats = sgs_query_stats{};
+    const int id = q->id;
+    queries.push_back(std::move(q));
+    return id;
+  }
+  // Up to `rounds` more rounds; true when the job has finished (converged or
+  // at the round limit; its query then holds the result and its stats).
+  bool pr_job_advance(uint32_t rounds) {
+    if (!job.q) fail(SGS_ERR_STATE, "no PageRank job");
+    Query &q = *job.q;
+    const uint32_t lim = std::min(rounds, cfg.max_rounds - job.r);
+    bool conv = false;
+    double l1v = 0;
+    CK(cudaEventRecord(ev_q.a, s));
+    const uint32_t ran = pr_steps(q, job_view(0), job_view(1), job.pull, job.l1.p, job.r, lim, job.c.p + 2,
+                                  job.pr_in, conv, l1v);
+    CK(cudaEventRecord(ev_q.b, s));
+    sync();
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ev_q.a, ev_q.b));
+    job.ms += ms;
+    job.r += ran;
+    q.stats.pr_residual_l1 = l1v;
+    if (!conv && job.r < cfg.max_rounds) return false;
+    unsigned long long e = 0;
+    CK(cudaMemcpyAsync(&e, job.c.p + 2, sizeof(e), cudaMemcpyDeviceToHost, s));
+    sync();
+    q.stats.edges_traversed = e;
+    q.stats.edges_total += e;
+    q.stats.rounds = job.r;
+    q.stats.converged = conv ? 1 : 0;
+    q.stats.ms = job.ms;
+    job.q = nullptr;
+    return true;
+  }
+
   // ---------------------------------------------------------------- queries
   Query &find(int qid) {
     for (auto &q : queries)
@@ -1244,12 +1351,48 @@ struct sgs_engine {
     fail(SGS_ERR_INVALID, "unknown query id");
   }
 
+  // One all-vertex sweep r[v] = sum over in-edges of pv[u] (pull over the
+  // in-edge store when it is there, else a push over the out-blocks), with
+  // the frontier buffers f0 (input, counter zeroed here) and f1.
+  void pr_sweep_once(Query &q, FrontierView f0, FrontierView f1) {
+    const GraphView g = view();
+    const bool pull = (cfg.pull & 1u) && ensure_in(f0, f1);
+    const GraphView gi = pull ? in_view() : g;
+    CK(cudaMemsetAsync(f0.counter, 0, sizeof(unsigned long long), s));
+    { ++n_launch; k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(gi, f0); }
+    if (pull)
+      { ++n_launch; k_pull_pr<<<grid_map(), RELAX_THREADS, 0, s>>>(f0, gi, q.pv.p, q.r.p, nullptr); }
+    else
+      { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(f0, f1, PrPushOp{g, q.pv.p, q.r.p}, nullptr); }
+    CK(cudaGetLastError());
+  }
+
+  // Initial state of a PageRank query: the reference's value 0, residual
+  // 1 - alpha, or a warm start from the kept vector of a removed query.
+  void pr_init(Query &q, FrontierView f0, FrontierView f1) {
+    if (pr_warm.p && pr_warm.n >= nv) {
+      // warm start: take over the kept vector, residual of it on this graph
+      std::swap(q.x.p, pr_warm.p);
+      std::swap(q.x.n, pr_warm.n);
+      pr_warm.release();
+      const GraphView g = view();
+      { ++n_launch; k_pr_warm_pv<<<grid_elem(nv), 256, 0, s>>>(g, q.x.p, q.pv.p, q.r.p, cfg.pr_alpha); }
+      pr_sweep_once(q, f0, f1);
+      { ++n_launch; k_pr_warm_res<<<grid_elem(nv), 256, 0, s>>>(q.x.p, q.r.p, nv, 1.0 - cfg.pr_alpha); }
+      CK(cudaGetLastError());
+      ++pr_warm_starts;
+    } else {
+      { ++n_launch; k_pr_init<<<grid_elem(nv), 256, 0, s>>>(q.x.p, q.r.p, nv, 1.0 - cfg.pr_alpha); }
+    }
+  }
+
   void start_pr(Query &q) {
     CK(cudaEventRecord(ev_q.a, s));
     CK(cudaMemsetAsync(b_stat.p, 0, sizeof(unsigned long long) * 8, s));
     bool conv = false;
     double l1v = 0;
-    { ++n_launch; k_pr_init<<<grid_elem(nv), 256, 0, s>>>(q.x.p, q.r.p, nv, 1.0 - cfg.pr_alpha); }
+    CK(cudaMemsetAsync(special(0), 0, sizeof(unsigned long long) * 2, s));
+    pr_init(q, fview(0, special(0)), fview(1, special(1)));
     const uint32_t rounds = pr_rounds(q, b_stat.p + 4, conv, l1v);
     CK(cudaEventRecord(ev_q.b, s));
     unsigned long long e = 0;
@@ -1650,6 +1793,11 @@ struct sgs_engine {
         sync();
         Query &q = *queries[i];
         if (q.grp) q.grp->used &= ~(1ull << q.lane);
+        if (job.q == &q) job.q = nullptr;
+        if (q.algo == SGS_PR && cfg.pr_warm) {  // keep its vector for the next start
+          std::swap(pr_warm.p, q.x.p);
+          std::swap(pr_warm.n, q.x.n);
+        }
         queries.erase(queries.begin() + i);
         // an empty group keeps its state arrays for the next queries (a
         // serving loop admits and retires queries all the time); they are
@@ -2220,6 +2368,7 @@ SGS_API void sgs_config_default(sgs_config *c) {
   c->persistent = 2;  // invalidation phases persistent: many small rounds
   c->pull = 1;  // PageRank sweeps as pulls; bit 1 (direction-optimizing BFS) is opt-in
   c->host_policy = 0;  // zero-copy reads of the host tier
+  c->pr_warm = 1;
 }
 
 SGS_API int sgs_create(const sgs_config *cfg, sgs_engine **out) {
@@ -2377,6 +2526,19 @@ int flight_advance(sgs_engine *e, uint32_t rounds, std::vector<int> &done, uint6
     *running = e->frun;
   });
 }
+int pr_job_start(sgs_engine *e, int *qid) {
+  return guarded([&] {
+    if (!e->loaded) fail(SGS_ERR_STATE, "no graph loaded");
+    CK(cudaSetDevice(e->dev));
+    *qid = e->pr_job_start();
+  });
+}
+int pr_job_advance(sgs_engine *e, uint32_t rounds, int *done) {
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    *done = e->pr_job_advance(rounds) ? 1 : 0;
+  });
+}
 }  // namespace sgs
 
 extern "C" {
@@ -2438,6 +2600,7 @@ SGS_API int sgs_get_engine_stats(sgs_engine *e, sgs_engine_stats *out) {
     e->est.in_store_builds = e->in_builds;
     e->est.bfs_bottom_up_rounds = e->bfs_bottom_up_total;
     e->est.host_stagings = e->stagings;
+    e->est.pr_warm_starts = e->pr_warm_starts;
     e->est.last_stage_bytes = e->stage_bytes_last;
     *out = e->est;
   });

@@ -13,11 +13,15 @@
 //   * a query leaves as soon as no entry of the frontier carries its lane:
 //     its result is read back (summary, and optionally its value/parent
 //     vectors) and its lane freed for the next arrival;
-//   * an update batch is one snapshot, applied when the flight is empty, so
-//     every query sees exactly the updates that arrived before it (its
-//     "version"); queries behind an update wait for it;
+//   * an update batch is one snapshot, applied when the flight is empty and
+//     no PageRank job runs, so every query sees exactly the updates that
+//     arrived before it (its "version"); queries behind an update wait for it;
 //   * PageRank has no lanes (and no source): consecutive PR queries share one
-//     computation, run when the flight is empty.
+//     computation, a job that starts as soon as they reach the head of the
+//     queue and runs a few sweeps per loop iteration between the flight's
+//     steps, so lane queries behind it keep being admitted and served (the
+//     job has its own frontier buffers; a PageRank start continues from the
+//     vector of the previous one, see sgs_config.pr_warm);
 //
 // With `realtime` the loop waits for arrival times on the wall clock, and
 // latency = done_s - arrival_s includes queueing; without it every request
@@ -41,6 +45,8 @@ void set_last_error(const std::string &msg);
 int flight_free(sgs_engine *e, uint32_t *lanes);
 int flight_admit(sgs_engine *e, uint32_t n, const int *algos, const uint32_t *sources, int *ids);
 int flight_advance(sgs_engine *e, uint32_t rounds, std::vector<int> &done, uint64_t *running);
+int pr_job_start(sgs_engine *e, int *qid);
+int pr_job_advance(sgs_engine *e, uint32_t rounds, int *done);
 }  // namespace sgs
 
 namespace {
@@ -52,6 +58,7 @@ double since(clk::time_point t0) {
 }
 
 constexpr uint32_t kRoundsPerStep = 4;  // rounds between two admission points
+constexpr uint32_t kPrRoundsPerStep = 8;  // PageRank sweeps per loop iteration
 
 // Result of a finished query into its completion record.
 void finish(sgs_engine *e, int qid, const sgs_request &r, sgs_completion &c) {
@@ -104,9 +111,39 @@ SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n, uint32_
   uint64_t version = 0, running = 0;
   std::vector<int> algos, qids, fin;
   std::vector<uint32_t> sources, batch;
+  int pr_qid = 0;                 // the PageRank job, if one runs
+  std::vector<uint32_t> pr_batch;  // its requests
+  double pr_start = 0;
   while (done < n) {
     const double now = since(t0);
     while (next < n && (!realtime || req[order[next]].arrival_s <= now)) pending.push_back(order[next++]);
+
+    // 0. PageRank requests at the head start a job (one at a time)
+    if (!pr_qid && !pending.empty() && req[pending.front()].kind == SGS_REQ_QUERY &&
+        req[pending.front()].algo == SGS_PR) {
+      pr_batch.clear();
+      while (!pending.empty() && req[pending.front()].kind == SGS_REQ_QUERY &&
+             req[pending.front()].algo == SGS_PR) {
+        pr_batch.push_back(pending.front());
+        pending.pop_front();
+      }
+      pr_start = since(t0);
+      int qid = 0;
+      const int rc = sgs::pr_job_start(e, &qid);
+      for (uint32_t k : pr_batch) {
+        out[k].start_s = pr_start;
+        out[k].version = version;
+        out[k].batch = (uint32_t)pr_batch.size();
+        out[k].status = rc;
+      }
+      if (rc == SGS_OK) {
+        pr_qid = qid;
+      } else {
+        if (qid > 0) sgs_query_remove(e, qid);
+        for (uint32_t k : pr_batch) out[k].done_s = since(t0);
+        done += (uint32_t)pr_batch.size();
+      }
+    }
 
     // 1. admission: lane queries at the head of the queue into free lanes
     if (!pending.empty() && lane_query(req[pending.front()])) {
@@ -159,8 +196,29 @@ SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n, uint32_
       continue;
     }
 
-    // 2. the flight: a few rounds, then retire the lanes that finished
+    bool worked = false;
+    // 2. the PageRank job: a few sweeps
+    if (pr_qid) {
+      worked = true;
+      int fin_pr = 0;
+      const int rc = sgs::pr_job_advance(e, kPrRoundsPerStep, &fin_pr);
+      if (rc != SGS_OK || fin_pr) {
+        for (uint32_t k : pr_batch) {
+          sgs_completion &c = out[k];
+          c.status = rc;
+          if (rc == SGS_OK) finish(e, pr_qid, req[k], c);
+        }
+        sgs_query_remove(e, pr_qid);
+        const double end = since(t0);
+        for (uint32_t k : pr_batch) out[k].done_s = end;
+        done += (uint32_t)pr_batch.size();
+        pr_qid = 0;
+      }
+    }
+
+    // 3. the flight: a few rounds, then retire the lanes that finished
     if (!inflight.empty()) {
+      worked = true;
       const int rc = sgs::flight_advance(e, kRoundsPerStep, fin, &running);
       if (rc != SGS_OK) {  // fail every query in flight, keep serving
         for (auto &kv : inflight) {
@@ -181,59 +239,32 @@ SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n, uint32_
         inflight.erase(it);
         ++done;
       }
+    }
+    if (worked) continue;
+
+    // 4. nothing runs: an update at the head
+    if (!pending.empty() && req[pending.front()].kind == SGS_REQ_UPDATE) {
+      const uint32_t head = pending.front();
+      const sgs_request &r = req[head];
+      pending.pop_front();
+      sgs_completion &c = out[head];
+      c.start_s = since(t0);
+      c.status = sgs_apply_batch(e, r.ins_src, r.ins_dst, r.ins_w, r.n_ins, r.del_src, r.del_dst,
+                                 r.n_del, SGS_MEM_HOST);
+      if (c.status == SGS_OK) {
+        ++version;
+        sgs_engine_stats st;
+        if (sgs_get_engine_stats(e, &st) == SGS_OK) c.edges = st.last_batch_edges;
+      }
+      c.version = version;
+      c.batch = 1;
+      c.done_s = since(t0);
+      ++done;
       continue;
     }
 
-    // 3. the flight is empty: an update, or PageRank, at the head
-    if (!pending.empty()) {
-      const uint32_t head = pending.front();
-      const sgs_request &r = req[head];
-      if (r.kind == SGS_REQ_UPDATE) {
-        pending.pop_front();
-        sgs_completion &c = out[head];
-        c.start_s = since(t0);
-        c.status = sgs_apply_batch(e, r.ins_src, r.ins_dst, r.ins_w, r.n_ins, r.del_src, r.del_dst,
-                                   r.n_del, SGS_MEM_HOST);
-        if (c.status == SGS_OK) {
-          ++version;
-          sgs_engine_stats st;
-          if (sgs_get_engine_stats(e, &st) == SGS_OK) c.edges = st.last_batch_edges;
-        }
-        c.version = version;
-        c.batch = 1;
-        c.done_s = since(t0);
-        ++done;
-        continue;
-      }
-      if (r.kind == SGS_REQ_QUERY && r.algo == SGS_PR) {
-        // consecutive PageRank queries share one computation
-        batch.clear();
-        while (!pending.empty() && req[pending.front()].kind == SGS_REQ_QUERY &&
-               req[pending.front()].algo == SGS_PR) {
-          batch.push_back(pending.front());
-          pending.pop_front();
-        }
-        const double start = since(t0);
-        int qid = 0;
-        const int rc = sgs_query_add(e, SGS_PR, 0, &qid);
-        for (uint32_t k : batch) {
-          sgs_completion &c = out[k];
-          c.start_s = start;
-          c.version = version;
-          c.batch = (uint32_t)batch.size();
-          c.status = rc;
-          if (rc == SGS_OK) finish(e, qid, req[k], c);
-        }
-        if (qid > 0) sgs_query_remove(e, qid);
-        const double end = since(t0);
-        for (uint32_t k : batch) out[k].done_s = end;
-        done += (uint32_t)batch.size();
-        continue;
-      }
-    }
-
-    // 4. idle until the next arrival
-    if (next < n) {
+    // 5. idle until the next arrival
+    if (pending.empty() && next < n) {
       const double wait = req[order[next]].arrival_s - since(t0);
       if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait));
     }

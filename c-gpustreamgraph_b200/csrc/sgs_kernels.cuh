@@ -294,6 +294,25 @@ __global__ void k_pr_init(double *x, double *r, uint32_t nv, double r0) {
   }
 }
 
+// Warm start from a previous solution x0 (kept in x): push values
+// pv = alpha * x0 / outdeg and a zeroed residual; after one sweep
+// r = sum over in-edges of pv, k_pr_warm_res turns it into the residual of x0,
+// r = (1 - alpha) + alpha P^T x0 - x0, so that x0 + (I - alpha P^T)^-1 r is
+// the fixed point and the rounds continue from there.
+__global__ void k_pr_warm_pv(GraphView g, const double *x, double *pv, double *r, double alpha) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < g.nv; v += stride) {
+    const uint32_t l = g.live[v];
+    pv[v] = l ? alpha * x[v] / (double)l : 0.0;
+    r[v] = 0.0;
+  }
+}
+__global__ void k_pr_warm_res(const double *x, double *r, uint32_t nv, double base) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride)
+    r[v] = base + r[v] - x[v];
+}
+
 // Absorb: value += residual, residual = 0, push value alpha*res/outdeg
 // (CombineValueBuffer, hybrid_pr.cu:66-85).  Accumulates the L1 norm of the
 // absorbed residual into *l1.

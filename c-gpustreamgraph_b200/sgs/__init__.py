@@ -82,6 +82,7 @@ class Config(C.Structure):
         ("persistent", C.c_uint32),
         ("pull", C.c_uint32),
         ("host_policy", C.c_uint32),
+        ("pr_warm", C.c_uint32),
     ]
 
 
@@ -128,6 +129,7 @@ class EngineStats(C.Structure):
         ("bfs_bottom_up_rounds", C.c_uint64),
         ("host_stagings", C.c_uint64),
         ("last_stage_bytes", C.c_uint64),
+        ("pr_warm_starts", C.c_uint64),
     ]
 
     def as_dict(self):

@@ -130,6 +130,12 @@ typedef struct sgs_config {
                              engine before every repair; 2 that copy only
                              when the repair's first frontier covers more
                              than half of the slots                        */
+  uint32_t pr_warm;       /* 1 (default): a removed PageRank query leaves its
+                             vector behind and the next PageRank start
+                             continues from it (its residual on the current
+                             graph computed first; same tolerance, fewer
+                             rounds after small changes); 0: every start
+                             from scratch                                  */
 } sgs_config;
 
 typedef struct sgs_query_stats {
@@ -176,6 +182,8 @@ typedef struct sgs_engine_stats {
   uint64_t bfs_bottom_up_rounds; /* bottom-up BFS rounds run so far        */
   uint64_t host_stagings;     /* explicit copies of the host tier so far   */
   uint64_t last_stage_bytes;  /* bytes of the last one                     */
+  uint64_t pr_warm_starts;    /* PageRank starts continued from a previous
+                                 query's vector                            */
 } sgs_engine_stats;
 
 /* Per-kernel-class timing of the relaxation launches (CUDA events on the

@@ -108,3 +108,32 @@ def test_pagerank_pull_tolerance_on_skewed_graph():
         q = e.add_query(sgs.PR)
         x = O.pagerank(nv, row, col)
         assert np.max(np.abs(q.value() - x)) <= PR_TOL
+
+
+@pytest.mark.parametrize("pull", [0, 1])
+def test_pagerank_warm_start(pull):
+    """A removed PageRank query leaves its vector; the next start after a
+    snapshot continues from it (residual computed on the updated graph) and
+    meets the same tolerance in fewer rounds."""
+    nv, row, col = O.rmat_csr(13, 16, 9)
+    w = O.weights(nv, row, col, 2, 0)
+    with sgs.Engine(pull=pull) as e:
+        e.load_csr(nv, row, col, w)
+        m = Mirror(nv, row, col, w)
+        q0 = e.add_query(sgs.PR)
+        r0 = q0.stats()["rounds"]
+        check_query(q0, m, sgs.W_EXPLICIT)
+        e.remove_query(q0)
+        b = _batch(m, 99, 300, 300, 2)
+        e.apply_batch(*b)
+        m.apply(*b)
+        q1 = e.add_query(sgs.PR)
+        check_query(q1, m, sgs.W_EXPLICIT)
+        assert e.engine_stats()["pr_warm_starts"] == 1
+        assert q1.stats()["rounds"] < r0
+    with sgs.Engine(pull=pull, pr_warm=0) as e:
+        e.load_csr(nv, row, col, w)
+        e.remove_query(e.add_query(sgs.PR))
+        q = e.add_query(sgs.PR)
+        assert e.engine_stats()["pr_warm_starts"] == 0
+        assert q.stats()["rounds"] == r0
