@@ -146,19 +146,35 @@ struct TombOp {
     uint32_t *a = adj_wptr(g, p.off) + j0;
     uint32_t *ca = cache_slot_w(g, g.adj_c, p.off, j0);  // cached copy: read from it, write both
     const uint4 q = *reinterpret_cast<const uint4 *>(ca ? ca : a);
-    uint32_t c = 0;
+    uint64_t key[4];
+    bool ok[4];
+    bool any = false;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const uint32_t dst = quad_at(q, k);
-      if (j0 + k >= len || dst == SGS_TOMB) continue;
-      const uint64_t key = ((uint64_t)u << 32) | dst;
-      uint32_t l = p.gs, r = p.ge;
-      while (l < r) {
-        const uint32_t m = (l + r) >> 1;
-        if (keys[m] < key) l = m + 1;
-        else r = m;
-      }
-      if (l < p.ge && keys[l] == key) {
+      ok[k] = j0 + k < len && dst != SGS_TOMB;
+      key[k] = ((uint64_t)u << 32) | dst;
+      any |= ok[k];
+    }
+    if (!any) return 0;
+    // the four lower bounds in lockstep (branchless, the same trip count for
+    // all: it depends only on the group's length), so their dependent loads
+    // overlap instead of running one search after the other
+    uint32_t lo[4] = {p.gs, p.gs, p.gs, p.gs};
+    uint32_t n = p.ge - p.gs;  // >= 1: the entry has deletes
+    while (n > 1) {
+      const uint32_t half = n >> 1;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) lo[k] = __ldg(&keys[lo[k] + half]) < key[k] ? lo[k] + half : lo[k];
+      n -= half;
+    }
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (!ok[k]) continue;
+      const uint64_t kk = __ldg(&keys[lo[k]]);
+      const uint32_t at = kk < key[k] ? lo[k] + 1 : lo[k];
+      if (at < p.ge && (at == lo[k] ? kk : __ldg(&keys[at])) == key[k]) {
         a[k] = SGS_TOMB;
         if (ca) ca[k] = SGS_TOMB;
         ++c;
