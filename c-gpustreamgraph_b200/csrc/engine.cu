@@ -1154,7 +1154,9 @@ struct sgs_engine {
       WideRelaxOp<> op{G.st.p, G.val.p, G.walgo()};
       WideRelaxOp<true> op0{G.st.p, G.val.p, G.walgo()};
       op0.only = only0;
-      if (cfg.persistent & 1u) {
+      if (cfg.persistent & 1u) {  // (bit 2 is for narrow groups: the wide
+                                  // cooperative grid is capped at 3 CTAs/SM,
+                                  // too few for their heavier later rounds)
         if (!only0 && !after0) return run_wide_persistent(op, 0, conv, SGS_K_WIDE, anyw ? 8.0 : 4.0, nullptr);
         // round 0 (restricted) and its hook as plain launches, then one launch
         CK(cudaMemsetAsync(rstat.p, 0, sizeof(unsigned long long) * (cfg.max_rounds + 2), s));
@@ -1170,6 +1172,29 @@ struct sgs_engine {
       return run_wide_rounds(op, op, conv, SGS_K_WIDE, anyw ? 8.0 : 4.0, nullptr, round0, after0);
     }
     const uint32_t anyw = G.any_sssp(G.used | 0xF) && cfg.weight_mode == SGS_W_EXPLICIT;
+    if ((cfg.persistent & 4u) && !(cfg.persistent & 1u) && !after0) {
+      // round 0 (a snapshot's sweep, or a start's first round) as a plain
+      // launch on the large grid, the rest of the phase as one cooperative
+      // launch: the sweep wants the grid, the small later rounds want no
+      // host round trips
+      CK(cudaMemsetAsync(rstat.p, 0, sizeof(unsigned long long) * (cfg.max_rounds + 2), s));
+      CK(cudaMemsetAsync(hstat.p, 0, sizeof(unsigned long long) * (cfg.max_rounds + 2), s));
+      if (round0) nvtxRangePushA(round0);
+      if (ktiming) { ensure_kev(2); CK(cudaEventRecord(kev[0], s)); }
+      launch_group(0, GroupRelaxOp<GMAX>{g, G.st.p, G.val.p, gm[0].p, gm[1].p, G.algo(), anyw});
+      if (ktiming) {
+        CK(cudaEventRecord(kev[1], s));
+        unsigned long long c0 = 0, r0s = 0, h0 = 0;
+        CK(cudaMemcpyAsync(&c0, cnt.p, sizeof(c0), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&r0s, rstat.p, sizeof(r0s), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&h0, hstat.p, sizeof(h0), cudaMemcpyDeviceToHost, s));
+        sync();
+        account(SGS_K_GROUP, c0, r0s, anyw ? 8.0 : 4.0, 8.0, kev[0], kev[1], h0);
+      }
+      if (round0) nvtxRangePop();
+      return run_group_persistent(GroupRelaxOp<GMAX>{g, G.st.p, G.val.p, nullptr, nullptr, G.algo(), anyw}, 1,
+                                  conv, SGS_K_GROUP, anyw ? 8.0 : 4.0);
+    }
     if ((cfg.persistent & 1u) && !after0) {
       if (round0) nvtxRangePushA(round0);
       const uint32_t r = run_group_persistent(
@@ -1747,7 +1772,7 @@ struct sgs_engine {
     for (uint32_t pers = 0; pers < 2; ++pers)
       for (uint32_t c : cps) {
         map_cps = c;
-        cfg.persistent = (keep_pers & 2u) | pers;
+        cfg.persistent = (keep_pers & 6u) | pers;
         double t = 1e300;
         for (int rep = 0; rep < 2; ++rep) {  // the first run also warms up
           int ids[3];
@@ -1763,7 +1788,7 @@ struct sgs_engine {
         }
       }
     map_cps = bc;
-    cfg.persistent = (keep_pers & 2u) | bp;
+    cfg.persistent = (keep_pers & 6u) | bp;
     (void)keep_cps;
     (void)keep_pers;
     out->ctas_per_sm = bc;
@@ -2365,7 +2390,8 @@ SGS_API void sgs_config_default(sgs_config *c) {
   c->slack_div = 8;
   c->arena_headroom = 0.30;
   c->group_size = 4;
-  c->persistent = 2;  // invalidation phases persistent: many small rounds
+  c->persistent = 6;  // invalidation phases persistent (many small rounds); relaxation: round 0
+                      // (the snapshot's sweep) on the large grid, the rest persistent
   c->pull = 1;  // PageRank sweeps as pulls; bit 1 (direction-optimizing BFS) is opt-in
   c->host_policy = 0;  // zero-copy reads of the host tier
   c->pr_warm = 1;

@@ -114,8 +114,11 @@ typedef struct sgs_config {
                              over rounds with a grid barrier between them
                              (no host read per batch of rounds); a clear bit:
                              rounds launched in batches with one counter
-                             read per batch.  Default 2: the invalidation's
-                             many small rounds gain most                  */
+                             read per batch.  Bit 2 (with bit 0 clear): a
+                             narrow group's relaxation phase runs round 0 --
+                             a snapshot's sweep -- as a plain launch on the
+                             large grid and its later rounds as one
+                             cooperative launch.  Default 6               */
   uint32_t pull;          /* bit 0 (default on): PageRank's all-vertex
                              sweeps as pulls over an in-edge (CSC) store
                              kept in HBM (built by transposing the graph

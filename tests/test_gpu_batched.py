@@ -142,14 +142,16 @@ def test_add_many_narrow_groups_and_pagerank():
 
 @pytest.mark.parametrize("gs", [4, 64])
 def test_persistent_launch_matches_batched_launches(gs):
-    """persistent=1 (each phase one cooperative launch looping over rounds)
-    gives the same values as rounds launched in batches, and the oracle."""
+    """Every launch mode -- bit 0 / bit 1: relaxation / invalidation phases
+    as one cooperative launch looping over rounds; bit 2: round 0 a plain
+    launch, the rest of the relaxation phase cooperative -- gives the same
+    values as rounds launched in batches, and the oracle."""
     nv, row, col = O.rmat_csr(12, 16, 13)
     w = O.weights(nv, row, col, 5, 0)
     specs = _specs(nv, 6, 6, 2, 21)
     i_s, i_d, iw, d_s, d_d = _stream(nv, row, col, 4, 3, 900, 5)
     res = {}
-    for pers in (0, 1, 2, 3):
+    for pers in (0, 1, 2, 3, 4, 6):
         with sgs.Engine(group_size=gs, persistent=pers) as e:
             e.load_csr(nv, row, col, w)
             qs = e.add_queries(specs)
@@ -164,7 +166,7 @@ def test_persistent_launch_matches_batched_launches(gs):
                         check_query(q, m, sgs.W_EXPLICIT)
                 out.append([q.value() for q in qs])
             res[pers] = out
-    for p in (1, 2, 3):
+    for p in (1, 2, 3, 4, 6):
         for a, b in zip(res[0], res[p]):
             for x, y in zip(a, b):
                 assert np.array_equal(x, y)
@@ -178,7 +180,8 @@ def test_autotune_picks_a_setting_and_keeps_results(gs):
     with sgs.Engine(group_size=gs) as e:
         e.load_csr(nv, row, col, w)
         t = e.autotune()
-        assert t["tried"] == 8 and t["ctas_per_sm"] in (4, 8, 16, 32) and t["persistent"] in (0, 1, 2, 3)
+        # the tuner chooses bit 0 and keeps the other bits of the default (6)
+        assert t["tried"] == 8 and t["ctas_per_sm"] in (4, 8, 16, 32) and t["persistent"] in (6, 7)
         assert t["best_ms"] > 0
         qs = e.add_queries(_specs(nv, 3, 3, 1, 8))
         e.apply_batch(i_s, i_d, iw, d_s, d_d)
