@@ -195,6 +195,50 @@ def test_messy_batches():
         del srcs
 
 
+@pytest.mark.parametrize("pull", [0, 1])
+def test_hub_deletes(pull):
+    """Sources losing hundreds of edges in one batch (the shared-memory hash
+    path of the tombstoning), with parallel copies of deleted edges, repeated
+    deletes and deletes of non-edges, next to sources losing one or two; the
+    in-edge store (pull) gets the same deletes transposed."""
+    rng = np.random.default_rng(11)
+    nv = 3000
+    hubs = [0, 1, 2]
+    src = [np.full(1500, h) for h in hubs] + [rng.integers(0, nv, 20000)]
+    dst = [rng.integers(0, nv, 1500) for _ in hubs] + [rng.integers(0, nv, 20000)]
+    src = np.concatenate(src).astype(np.uint32)
+    dst = np.concatenate(dst).astype(np.uint32)
+    keep = src != dst
+    src, dst = src[keep], dst[keep]
+    order = np.lexsort((dst, src))
+    src, dst = src[order], dst[order]  # parallel copies kept
+    row = np.zeros(nv + 1, np.uint64)
+    np.add.at(row, src.astype(np.int64) + 1, 1)
+    row = np.cumsum(row).astype(np.uint64)
+    col = dst
+    w = O.weights(nv, row, col, 4, 0)
+    with sgs.Engine(pull=pull) as e:
+        e.load_csr(nv, row, col, w)
+        m = Mirror(nv, row, col, w)
+        qs = [e.add_query(sgs.SSSP, 0), e.add_query(sgs.BFS, 1), e.add_query(sgs.CC), e.add_query(sgs.PR)]
+        for k in range(3):
+            ms = _src_ids(m.row)
+            hub_rows = np.nonzero(np.isin(ms, hubs))[0]
+            pick = rng.choice(hub_rows, 900, replace=False)
+            other = rng.integers(0, len(m.col), 300)
+            d_s = np.concatenate([ms[pick], ms[pick[:50]], ms[other], [0] * 20]).astype(np.uint32)
+            d_d = np.concatenate([m.col[pick], m.col[pick[:50]], m.col[other],
+                                  rng.integers(0, nv, 20)]).astype(np.uint32)
+            i_s = rng.integers(0, nv, 500).astype(np.uint32)
+            i_d = rng.integers(0, nv, 500).astype(np.uint32)
+            iw = rng.integers(1, 65, 500).astype(np.uint32)
+            e.apply_batch(i_s, i_d, iw, d_s, d_d)
+            m.apply(i_s, i_d, iw, d_s, d_d)
+            check_graph(e, m)
+            for q in qs:
+                check_query(q, m, sgs.W_EXPLICIT)
+
+
 def test_relocation_and_repack():
     """No slack and no headroom: every insert relocates a block and the arena
     is repacked; results stay identical."""
