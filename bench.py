@@ -276,7 +276,7 @@ def engine_arm(a, R):
     nv = int(st0["nv"])
     row, col, _ = e.export()
     half = a.updates // 2
-    nbatch = a.warmup + a.steps * (1 if a.no_e2e else 2)
+    nbatch = a.warmup + a.steps * (1 if a.no_e2e else 2) + (0 if a.no_e2e else 1)
     i_s, i_d, d_s, d_d = sgs.gen_update_stream(nv, row, col, a.seed * 1000003, nbatch * half,
                                                nbatch * half)
     i_w = sgs.hash_weights(a.seed, i_s, i_d)
@@ -344,7 +344,7 @@ def engine_arm(a, R):
     e2e = None
     if not a.no_e2e:
         host = []
-        for k in range(a.steps):
+        for k in range(a.steps + 1):  # one untimed pipelined warm-up step first
             arrs = batch(a.warmup + a.steps + k)
             pinned = []
             for x in arrs:
@@ -356,15 +356,29 @@ def engine_arm(a, R):
         torch.cuda.synchronize()
         e_edges, e_ms = 0, 0.0
         out_bytes = 0
-        for k in range(a.steps):
-            isrc, idst, iw, dsrc, ddst = host[k]
-            t1 = time.perf_counter()
-            e.apply_batch_ptr(isrc.data_ptr(), idst.data_ptr(), iw.data_ptr(), half,
+
+        def stage(k):
+            isrc, idst, iw, dsrc, ddst = host[k + 1]
+            e.stage_batch_ptr(isrc.data_ptr(), idst.data_ptr(), iw.data_ptr(), half,
                               dsrc.data_ptr(), ddst.data_ptr(), half, sgs.MEM_HOST)
+
+        stage(-1)  # warm-up: copy stream, staging slots and events set up
+        e.apply_staged()
+        torch.cuda.synchronize()
+
+        # pipelined: step k's pinned-host batch is copied while step k-1 runs
+        # (sgs_stage_batch on the copy stream), then applied and every query's
+        # summary read back; all copies lie inside the timed region
+        t1 = time.perf_counter()
+        stage(0)
+        for k in range(a.steps):
+            if k + 1 < a.steps:
+                stage(k + 1)
+            e.apply_staged()
             sums = [q.summary() for q in queries]
-            e_ms += (time.perf_counter() - t1) * 1e3
             out_bytes = sum(s.nbytes for s in sums)
             e_edges += sum(q.stats()["edges_traversed"] for q in queries)
+        e_ms = (time.perf_counter() - t1) * 1e3
         R.barrier()
         e2e_ms = R.max(e_ms)
         e2e = {"value": R.sum(e_edges) / (e2e_ms * 1e6), "unit": UNIT,

@@ -286,7 +286,27 @@ struct sgs_engine {
   DBuf<double> pr_warm;
   uint64_t pr_warm_starts = 0;
 
+  // staged batches (sgs_stage_batch): two slots of device copies of a batch's
+  // arrays, filled on a copy stream while the engine's stream computes
+  struct Staged {
+    DBuf<uint32_t> a[5];  // ins src, dst, w; del src, dst
+    uint64_t ni = 0, nd = 0;
+    bool w = false;
+    bool full = false;
+    cudaEvent_t copied = nullptr, consumed = nullptr;
+  } stg[2];
+  uint32_t stg_head = 0, stg_count = 0;  // oldest full slot, full slots
+  cudaStream_t sc = nullptr;             // copy stream
+
   ~sgs_engine() {
+    if (sc) {
+      cudaStreamSynchronize(sc);
+      cudaStreamDestroy(sc);
+    }
+    for (auto &t : stg) {
+      if (t.copied) cudaEventDestroy(t.copied);
+      if (t.consumed) cudaEventDestroy(t.consumed);
+    }
     if (s2) {
       cudaStreamSynchronize(s2);
       cudaStreamDestroy(s2);
@@ -668,6 +688,8 @@ struct sgs_engine {
     in_release();
     in_failed = false;
     pr_warm.release();
+    if (sc) CK(cudaStreamSynchronize(sc));
+    stg_head = stg_count = 0;  // staged batches belonged to the old graph
     est = sgs_engine_stats{};
     nv = n;
     uint64_t ne_in = 0;
@@ -1833,6 +1855,59 @@ struct sgs_engine {
   }
 
   // ------------------------------------------------------------ snapshots
+  // Copies a batch into the next staging slot on the copy stream (from
+  // pinned host or device memory) and returns at once; apply_staged applies
+  // the oldest staged batch.  A slot is refilled only after the snapshot
+  // that consumed it has copied it out.
+  void stage_batch(const uint32_t *is, const uint32_t *id, const uint32_t *iw, uint64_t ni,
+                   const uint32_t *ds, const uint32_t *dd, uint64_t nd, int mem) {
+    if (stg_count >= 2) fail(SGS_ERR_STATE, "two batches are staged already");
+    if (ni >= (1ull << 31) || nd >= (1ull << 31)) fail(SGS_ERR_INVALID, "batch too large");
+    if ((ni && (!is || !id)) || (nd && (!ds || !dd))) fail(SGS_ERR_INVALID, "null batch array");
+    const bool ew = cfg.weight_mode == SGS_W_EXPLICIT;
+    if (ni && ew && !iw) fail(SGS_ERR_INVALID, "explicit weight mode needs insert weights");
+    if (!sc) CK(cudaStreamCreateWithFlags(&sc, cudaStreamNonBlocking));
+    Staged &t = stg[(stg_head + stg_count) % 2];
+    if (!t.copied) {
+      CK(cudaEventCreateWithFlags(&t.copied, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&t.consumed, cudaEventDisableTiming));
+      CK(cudaEventRecord(t.consumed, s));
+    }
+    CK(cudaStreamWaitEvent(sc, t.consumed, 0));  // its previous batch was copied out
+    const uint32_t *src[5] = {is, id, ew ? iw : nullptr, ds, dd};
+    const uint64_t cnt[5] = {ni, ni, ew ? ni : 0, nd, nd};
+    const cudaMemcpyKind kind = mem == SGS_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    for (int k = 0; k < 5; ++k) {
+      if (!cnt[k]) continue;
+      t.a[k].ensure(cnt[k]);
+      CK(cudaMemcpyAsync(t.a[k].p, src[k], cnt[k] * sizeof(uint32_t), kind, sc));
+    }
+    CK(cudaEventRecord(t.copied, sc));
+    t.ni = ni;
+    t.nd = nd;
+    t.w = ew;
+    t.full = true;
+    ++stg_count;
+  }
+  void apply_staged() {
+    if (!stg_count) fail(SGS_ERR_STATE, "no staged batch");
+    Staged &t = stg[stg_head];
+    CK(cudaStreamWaitEvent(s, t.copied, 0));
+    stg_head = (stg_head + 1) % 2;
+    --stg_count;
+    t.full = false;
+    staged_in = &t;
+    try {
+      apply_batch(t.a[0].p, t.a[1].p, t.w ? t.a[2].p : nullptr, t.ni, t.a[3].p, t.a[4].p, t.nd, SGS_MEM_DEVICE);
+    } catch (...) {
+      staged_in = nullptr;
+      CK(cudaEventRecord(t.consumed, s));
+      throw;
+    }
+    staged_in = nullptr;
+  }
+  Staged *staged_in = nullptr;  // the staged batch apply_batch is reading
+
   void upload(DBuf<uint32_t> &dst, const uint32_t *src, uint64_t n, int mem) {
     dst.ensure(n);
     if (n)
@@ -1863,6 +1938,7 @@ struct sgs_engine {
     if (explicit_w) upload(b_iw, iw, ni, mem);
     upload(b_dsrc, ds, nd, mem);
     upload(b_ddst, dd, nd, mem);
+    if (staged_in) CK(cudaEventRecord(staged_in->consumed, s));  // its slot may be refilled
     b_ikeys.ensure(ni); b_ikeys_s.ensure(ni); b_ikept.ensure(ni);
     b_iw_s.ensure(ni); b_iw_kept.ensure(ni); b_flag.ensure(ni);
     b_dkeys.ensure(nd); b_dkeys_s.ensure(nd);
@@ -2581,6 +2657,25 @@ SGS_API int sgs_apply_batch(sgs_engine *e, const uint32_t *ins_src, const uint32
   return guarded([&] {
     CK(cudaSetDevice(e->dev));
     e->apply_batch(ins_src, ins_dst, ins_w, n_ins, del_src, del_dst, n_del, mem);
+  });
+}
+
+SGS_API int sgs_stage_batch(sgs_engine *e, const uint32_t *ins_src, const uint32_t *ins_dst,
+                            const uint32_t *ins_w, uint64_t n_ins, const uint32_t *del_src,
+                            const uint32_t *del_dst, uint64_t n_del, int mem) {
+  if (!e) { g_last_error = "null engine"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    if (!e->loaded) fail(SGS_ERR_STATE, "no graph loaded");
+    CK(cudaSetDevice(e->dev));
+    e->stage_batch(ins_src, ins_dst, ins_w, n_ins, del_src, del_dst, n_del, mem);
+  });
+}
+
+SGS_API int sgs_apply_staged(sgs_engine *e) {
+  if (!e) { g_last_error = "null engine"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    e->apply_staged();
   });
 }
 

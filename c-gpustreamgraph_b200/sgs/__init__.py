@@ -51,6 +51,7 @@ EXPORTS = [
     "sgs_ppr_create_csr", "sgs_ppr_create", "sgs_ppr_destroy", "sgs_ppr_info",
     "sgs_ppr_export", "sgs_ppr_forward", "sgs_ppr_backward", "sgs_ppr_timing",
     "sgs_ppr_get_stats", "sgs_serve", "sgs_autotune", "sgs_cache_refresh",
+    "sgs_stage_batch", "sgs_apply_staged",
 ]
 
 K_GROUP, K_GROUP_INVAL, K_PR_PUSH, K_WIDE, K_WIDE_INVAL, K_PR_PULL = range(6)
@@ -251,6 +252,8 @@ def lib():
     L.sgs_serve.argtypes = [vp, C.POINTER(Request), u32, u32, i32, C.POINTER(Completion)]
     L.sgs_autotune.argtypes = [vp, C.POINTER(Tune)]
     L.sgs_cache_refresh.argtypes = [vp]
+    L.sgs_stage_batch.argtypes = [vp, vp, vp, vp, u64, vp, vp, u64, i32]
+    L.sgs_apply_staged.argtypes = [vp]
     L.sgs_ppr_get_stats.argtypes = [vp, C.POINTER(PprStats)]
     for name in EXPORTS:
         if name not in ("sgs_version", "sgs_last_error", "sgs_config_default",
@@ -493,6 +496,15 @@ class Engine:
 
     def remove_query(self, q):
         _check(lib().sgs_query_remove(self.h, q.qid if isinstance(q, Query) else q))
+
+    def stage_batch_ptr(self, isp, idp, iwp, ni, dsp, ddp, nd, mem):
+        """Copies a batch into a staging slot on the copy stream and returns
+        at once (raw pointers, pinned host or device); apply_staged applies it."""
+        _check(lib().sgs_stage_batch(self.h, _ptr(isp), _ptr(idp), _ptr(iwp), ni,
+                                     _ptr(dsp), _ptr(ddp), nd, mem))
+
+    def apply_staged(self):
+        _check(lib().sgs_apply_staged(self.h))
 
     def apply_batch_ptr(self, isp, idp, iwp, ni, dsp, ddp, nd, mem):
         """Raw-pointer form (host pinned or device memory, as ints)."""

@@ -267,6 +267,19 @@ SGS_API int sgs_apply_batch(sgs_engine *e, const uint32_t *ins_src,
  * static run, as the reference's do with LoadCache. */
 SGS_API int sgs_cache_refresh(sgs_engine *e);
 
+/* Pipelined snapshots.  sgs_stage_batch copies a batch (pinned host or
+ * device arrays) into one of two engine-owned device slots on a copy stream
+ * and returns at once; sgs_apply_staged applies the oldest staged batch
+ * exactly like sgs_apply_batch.  Staging batch k+1 before applying batch k
+ * overlaps its host-to-device copy with snapshot k's work.  The caller keeps
+ * the arrays unchanged until the batch has been applied.  At most two
+ * batches are staged at a time (SGS_ERR_STATE otherwise). */
+SGS_API int sgs_stage_batch(sgs_engine *e, const uint32_t *ins_src,
+                            const uint32_t *ins_dst, const uint32_t *ins_w,
+                            uint64_t n_ins, const uint32_t *del_src,
+                            const uint32_t *del_dst, uint64_t n_del, int mem);
+SGS_API int sgs_apply_staged(sgs_engine *e);
+
 /* Copies nv elements of a field (u32, or f64 for PR value/buffer). */
 SGS_API int sgs_gather(sgs_engine *e, int qid, int field, void *out, int mem);
 SGS_API int sgs_get_query_stats(sgs_engine *e, int qid, sgs_query_stats *out);

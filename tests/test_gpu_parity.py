@@ -368,3 +368,41 @@ def test_groups_match_single_lane_engine():
     for k in range(3):
         for a, b in zip(res[1][k], res[4][k]):
             assert np.array_equal(a, b)
+
+
+def test_staged_batches_pipeline():
+    """sgs_stage_batch + sgs_apply_staged (batch k+1 copied while batch k is
+    applied) give the same graph and results as sgs_apply_batch; misuse is a
+    status code."""
+    import ctypes as C
+
+    nv, row, col = O.rmat_csr(12, 16, 21)
+    w = O.weights(nv, row, col, 7, 0)
+    i_s, i_d, d_s, d_d = O.gen_updates(nv, row, col, 3, 4 * 1500, 4 * 1500)
+    iw = np.array([O.weight_of(7, u, v) for u, v in zip(i_s, i_d)], np.uint32)
+    parts = [[np.ascontiguousarray(x[k * 1500:(k + 1) * 1500]) for x in (i_s, i_d, iw, d_s, d_d)]
+             for k in range(4)]
+
+    def ptrs(p):
+        return [x.ctypes.data_as(C.c_void_p).value for x in p]
+
+    with sgs.Engine() as e:
+        e.load_csr(nv, row, col, w)
+        m = Mirror(nv, row, col, w)
+        qs = [e.add_query(sgs.SSSP, 0), e.add_query(sgs.BFS, 2), e.add_query(sgs.CC), e.add_query(sgs.PR)]
+        with pytest.raises(sgs.SgsError):
+            e.apply_staged()  # nothing staged
+        a = ptrs(parts[0])
+        e.stage_batch_ptr(a[0], a[1], a[2], 1500, a[3], a[4], 1500, sgs.MEM_HOST)
+        for k in range(4):
+            if k + 1 < 4:
+                b = ptrs(parts[k + 1])
+                e.stage_batch_ptr(b[0], b[1], b[2], 1500, b[3], b[4], 1500, sgs.MEM_HOST)
+                if k == 0:
+                    with pytest.raises(sgs.SgsError):  # a third staged batch
+                        e.stage_batch_ptr(b[0], b[1], b[2], 1500, b[3], b[4], 1500, sgs.MEM_HOST)
+            e.apply_staged()
+            m.apply(*parts[k])
+            check_graph(e, m)
+            for q in qs:
+                check_query(q, m, sgs.W_EXPLICIT)
