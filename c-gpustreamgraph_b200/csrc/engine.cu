@@ -2340,6 +2340,50 @@ struct sgs_engine {
     for (int i = 0; i < 4; ++i) out[i] = h[i];
   }
 
+  // Summaries of several queries with one read-back: a narrow group's lanes
+  // in one pass over its state rows, the others as in summary().
+  DBuf<unsigned long long> b_sum;
+  void summaries(uint32_t n, const int *qids, uint64_t *out) {
+    b_sum.ensure(4ull * std::max<uint32_t>(n, 1));
+    CK(cudaMemsetAsync(b_sum.p, 0, sizeof(unsigned long long) * 4 * n, s));
+    std::vector<Query *> qs(n);
+    for (uint32_t i = 0; i < n; ++i) qs[i] = &find(qids[i]);
+    std::vector<char> done(n, 0);
+    for (uint32_t i = 0; i < n; ++i) {
+      if (done[i]) continue;
+      Query &q = *qs[i];
+      if (q.algo == SGS_PR) {
+        { ++n_launch; k_summary_pr<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.x.p, nv,
+                                                             (double *)(b_sum.p + 4 * i) + 1); }
+      } else if (q.grp->wide()) {
+        { ++n_launch; k_group_summary<WLANES><<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.grp->st.p, nv, q.lane,
+                                                                          b_sum.p + 4 * i); }
+      } else {
+        LaneSlots ls;
+        for (int l = 0; l < GMAX; ++l) ls.slot[l] = -1;
+        for (uint32_t j = i; j < n; ++j)  // every requested lane of this group
+          if (!done[j] && qs[j]->algo != SGS_PR && qs[j]->grp == q.grp && ls.slot[qs[j]->lane] < 0) {
+            ls.slot[qs[j]->lane] = (int)j;
+            done[j] = 1;
+          }
+        { ++n_launch; k_group_summary_lanes<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.grp->st.p, nv, ls,
+                                                                       b_sum.p); }
+      }
+      done[i] = 1;
+    }
+    CK(cudaGetLastError());
+    std::vector<unsigned long long> h(4ull * n);
+    if (n) CK(cudaMemcpyAsync(h.data(), b_sum.p, sizeof(unsigned long long) * 4 * n, cudaMemcpyDeviceToHost, s));
+    sync();
+    for (uint32_t i = 0; i < n; ++i) {
+      uint32_t src = i;
+      for (uint32_t j = 0; j < i; ++j)
+        if (qids[j] == qids[i]) src = j;  // repeated id: same counters
+      for (int k = 0; k < 4; ++k) out[4 * i + k] = h[4 * src + k];
+      if (qs[i]->algo == SGS_PR) out[4 * i] = nv;
+    }
+  }
+
   void export_graph(uint64_t *row, uint32_t *col, uint32_t *w, int mem) {
     DBuf<uint64_t> drow;
     drow.ensure((size_t)nv + 1);
@@ -2744,6 +2788,14 @@ SGS_API int sgs_graph_export(sgs_engine *e, uint64_t *row, uint32_t *col, uint32
     if (!e->loaded) fail(SGS_ERR_STATE, "no graph loaded");
     CK(cudaSetDevice(e->dev));
     e->export_graph(row, col, w, mem);
+  });
+}
+
+SGS_API int sgs_query_summaries(sgs_engine *e, uint32_t n, const int *qids, uint64_t *out) {
+  if (!e || (n && (!qids || !out))) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    e->summaries(n, qids, out);
   });
 }
 

@@ -659,6 +659,51 @@ __global__ void k_group_summary(const unsigned long long *st, uint32_t nv, int l
   }
 }
 
+// The same summaries for several lanes of a narrow group in one pass over
+// the state rows (one 32-B row per vertex read once for all of them):
+// slot[q] >= 0 selects lane q and its 4 counters at out + 4 * slot[q].
+struct LaneSlots {
+  int slot[GMAX];
+};
+__global__ void k_group_summary_lanes(const unsigned long long *st, uint32_t nv, LaneSlots ls,
+                                      unsigned long long *out) {
+  unsigned long long reached[GMAX] = {}, sum[GMAX] = {}, mx[GMAX] = {}, psum[GMAX] = {};
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += stride) {
+    const ulonglong2 a = __ldcs(reinterpret_cast<const ulonglong2 *>(st + v * GMAX));
+    const ulonglong2 b = __ldcs(reinterpret_cast<const ulonglong2 *>(st + v * GMAX + 2));
+    const unsigned long long row[GMAX] = {a.x, a.y, b.x, b.y};
+#pragma unroll
+    for (int q = 0; q < GMAX; ++q) {
+      if (ls.slot[q] < 0) continue;
+      const uint32_t val = (uint32_t)(row[q] >> 32);
+      if (val == INF32) continue;
+      reached[q] += 1;
+      sum[q] += val;
+      mx[q] = val > mx[q] ? val : mx[q];
+      if ((uint32_t)row[q] != INF32) psum[q] += (uint32_t)row[q];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < GMAX; ++q) {
+    if (ls.slot[q] < 0) continue;
+    const unsigned long long r = warp_sum(reached[q]), su = warp_sum(sum[q]), ps = warp_sum(psum[q]);
+    unsigned long long m = mx[q];
+#pragma unroll
+    for (int sh = 16; sh > 0; sh >>= 1) {
+      const unsigned long long o = __shfl_xor_sync(0xFFFFFFFFu, m, sh);
+      m = o > m ? o : m;
+    }
+    if ((threadIdx.x & 31) == 0) {
+      unsigned long long *o = out + 4 * ls.slot[q];
+      if (r) atomicAdd(&o[0], r);
+      if (su) atomicAdd(&o[1], su);
+      atomicMax(&o[2], m);
+      if (ps) atomicAdd(&o[3], ps);
+    }
+  }
+}
+
 // Lanes present in a frontier: per-lane counts of its entries' mask bits
 // (narrow u32 or wide u64 masks), for a serving loop that retires a lane as
 // soon as no entry carries it.

@@ -51,7 +51,7 @@ EXPORTS = [
     "sgs_ppr_create_csr", "sgs_ppr_create", "sgs_ppr_destroy", "sgs_ppr_info",
     "sgs_ppr_export", "sgs_ppr_forward", "sgs_ppr_backward", "sgs_ppr_timing",
     "sgs_ppr_get_stats", "sgs_serve", "sgs_autotune", "sgs_cache_refresh",
-    "sgs_stage_batch", "sgs_apply_staged",
+    "sgs_stage_batch", "sgs_apply_staged", "sgs_query_summaries",
 ]
 
 K_GROUP, K_GROUP_INVAL, K_PR_PUSH, K_WIDE, K_WIDE_INVAL, K_PR_PULL = range(6)
@@ -254,6 +254,7 @@ def lib():
     L.sgs_cache_refresh.argtypes = [vp]
     L.sgs_stage_batch.argtypes = [vp, vp, vp, vp, u64, vp, vp, u64, i32]
     L.sgs_apply_staged.argtypes = [vp]
+    L.sgs_query_summaries.argtypes = [vp, u32, vp, vp]
     L.sgs_ppr_get_stats.argtypes = [vp, C.POINTER(PprStats)]
     for name in EXPORTS:
         if name not in ("sgs_version", "sgs_last_error", "sgs_config_default",
@@ -539,6 +540,13 @@ class Engine:
     def summary(self, qid):
         out = np.zeros(4, np.uint64)
         _check(lib().sgs_query_summary(self.h, qid, _ptr(out)))
+        return out
+
+    def summaries(self, queries):
+        """[n, 4] summaries of several queries (Query objects or ids), one read-back."""
+        ids = np.array([q.qid if isinstance(q, Query) else q for q in queries], np.int32)
+        out = np.zeros((len(ids), 4), np.uint64)
+        _check(lib().sgs_query_summaries(self.h, len(ids), _ptr(ids), _ptr(out)))
         return out
 
     def engine_stats(self):

@@ -296,6 +296,9 @@ SGS_API int sgs_synchronize(sgs_engine *e);
  * of finite values (PR: sum of ranks as IEEE-754 bits of a double), out[2] =
  * max finite value, out[3] = sum of parents of reached vertices. */
 SGS_API int sgs_query_summary(sgs_engine *e, int qid, uint64_t out[4]);
+/* The same for n queries with one device-to-host read (out: 4 * n values in
+ * query order); the lanes of one narrow group are summarised in one pass. */
+SGS_API int sgs_query_summaries(sgs_engine *e, uint32_t n, const int *qids, uint64_t *out);
 
 /* Synthetic update stream (host arrays, no engine needed): n_del distinct
  * existing edges sampled uniformly by edge index and n_ins distinct non-edges

@@ -406,3 +406,20 @@ def test_staged_batches_pipeline():
             check_graph(e, m)
             for q in qs:
                 check_query(q, m, sgs.W_EXPLICIT)
+
+
+@pytest.mark.parametrize("gs", [4, 64])
+def test_batched_summaries_equal_single(gs):
+    """sgs_query_summaries (one read-back; a narrow group's lanes in one
+    pass) equals sgs_query_summary query by query, PageRank and a repeated
+    id included."""
+    nv, row, col = O.rmat_csr(11, 16, 4)
+    w = O.weights(nv, row, col, 2, 0)
+    with sgs.Engine(group_size=gs) as e:
+        e.load_csr(nv, row, col, w)
+        qs = e.add_queries([(sgs.SSSP, 0), (sgs.BFS, 5), (sgs.CC, 0), (sgs.BFS, 9), (sgs.SSSP, 3)])
+        qs.append(e.add_query(sgs.PR))
+        order = qs + [qs[1]]
+        got = e.summaries(order)
+        want = np.stack([q.summary() for q in order])
+        assert np.array_equal(got, want)
