@@ -2356,8 +2356,15 @@ struct sgs_engine {
         { ++n_launch; k_summary_pr<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.x.p, nv,
                                                              (double *)(b_sum.p + 4 * i) + 1); }
       } else if (q.grp->wide()) {
-        { ++n_launch; k_group_summary<WLANES><<<grid_elem(nv), RELAX_THREADS, 0, s>>>(q.grp->st.p, nv, q.lane,
-                                                                          b_sum.p + 4 * i); }
+        WideSlots ws;
+        for (int l = 0; l < WLANES; ++l) ws.slot[l] = -1;
+        for (uint32_t j = i; j < n; ++j)  // every requested lane of this group
+          if (!done[j] && qs[j]->algo != SGS_PR && qs[j]->grp == q.grp && ws.slot[qs[j]->lane] < 0) {
+            ws.slot[qs[j]->lane] = (int)j;
+            done[j] = 1;
+          }
+        { ++n_launch; k_wide_summary_lanes<<<grid_elem((uint64_t)nv * 32), RELAX_THREADS, 0, s>>>(
+            q.grp->st.p, nv, ws, b_sum.p); }
       } else {
         LaneSlots ls;
         for (int l = 0; l < GMAX; ++l) ls.slot[l] = -1;

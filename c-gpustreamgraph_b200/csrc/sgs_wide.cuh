@@ -374,6 +374,69 @@ __global__ void __launch_bounds__(RELAX_THREADS, 3)
 // Frontier builders and per-lane helpers
 // ---------------------------------------------------------------------------
 
+// Summaries of the lanes of a wide group in one pass over its 512-B state
+// rows: a warp per vertex, thread t holding lanes t and t+32 across the
+// vertices it visits; slot[q] >= 0 selects lane q and its 4 counters at
+// out + 4 * slot[q] (reached, sum of values, max value, sum of parents).
+struct WideSlots {
+  int slot[WLANES];
+};
+__global__ void __launch_bounds__(RELAX_THREADS)
+    k_wide_summary_lanes(const unsigned long long *st, uint32_t nv, WideSlots ws,
+                         unsigned long long *out) {
+  __shared__ unsigned long long s_acc[WLANES][4];
+  for (int i = threadIdx.x; i < WLANES * 4; i += RELAX_THREADS) s_acc[i / 4][i % 4] = 0;
+  __syncthreads();
+  const int t = threadIdx.x & 31;
+  const bool on0 = ws.slot[t] >= 0, on1 = ws.slot[t + 32] >= 0;
+  unsigned long long r0 = 0, su0 = 0, m0 = 0, p0 = 0, r1 = 0, su1 = 0, m1 = 0, p1 = 0;
+  const uint32_t nwarp = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < nv; v += nwarp) {
+    const unsigned long long *row = st + (uint64_t)v * WLANES;
+    if (on0) {
+      const unsigned long long x = __ldcs(row + t);
+      const uint32_t val = (uint32_t)(x >> 32);
+      if (val != INF32) {
+        ++r0;
+        su0 += val;
+        m0 = val > m0 ? val : m0;
+        if ((uint32_t)x != INF32) p0 += (uint32_t)x;
+      }
+    }
+    if (on1) {
+      const unsigned long long x = __ldcs(row + t + 32);
+      const uint32_t val = (uint32_t)(x >> 32);
+      if (val != INF32) {
+        ++r1;
+        su1 += val;
+        m1 = val > m1 ? val : m1;
+        if ((uint32_t)x != INF32) p1 += (uint32_t)x;
+      }
+    }
+  }
+  if (on0) {
+    atomicAdd(&s_acc[t][0], r0);
+    atomicAdd(&s_acc[t][1], su0);
+    atomicMax(&s_acc[t][2], m0);
+    atomicAdd(&s_acc[t][3], p0);
+  }
+  if (on1) {
+    atomicAdd(&s_acc[t + 32][0], r1);
+    atomicAdd(&s_acc[t + 32][1], su1);
+    atomicMax(&s_acc[t + 32][2], m1);
+    atomicAdd(&s_acc[t + 32][3], p1);
+  }
+  __syncthreads();
+  if (threadIdx.x < WLANES && ws.slot[threadIdx.x] >= 0) {
+    unsigned long long *o = out + 4 * ws.slot[threadIdx.x];
+    const unsigned long long *a = s_acc[threadIdx.x];
+    if (a[0]) atomicAdd(&o[0], a[0]);
+    if (a[1]) atomicAdd(&o[1], a[1]);
+    atomicMax(&o[2], a[2]);
+    if (a[3]) atomicAdd(&o[3], a[3]);
+  }
+}
+
 // Initial state of the lanes in `lanes` on every vertex: CC lanes v's own id,
 // the others unreached; one warp per vertex row.
 __global__ void k_wide_init_lanes(unsigned long long *st, uint32_t *val, uint32_t nv,
