@@ -72,3 +72,40 @@ def test_host_update_generator_matches_oracle():
         assert np.array_equal(x, y)
     w = sgs.hash_weights(5, a[0], a[1])
     assert np.array_equal(w, [O.weight_of(5, int(u), int(v)) for u, v in zip(a[0], a[1])])
+
+
+def _c_layout(struct, fields):
+    """sizeof and field offsets of a C struct of include/sgs.h, from a tiny
+    program compiled here with the host compiler."""
+    import shutil
+    import subprocess
+    import tempfile
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        pytest.skip("no C compiler")
+    src = ["#include <stdio.h>", "#include <stddef.h>", '#include "sgs.h"', "int main(void) {",
+           f'  printf("%zu\\n", sizeof({struct}));']
+    src += [f'  printf("%zu\\n", offsetof({struct}, {f}));' for f in fields]
+    src += ["  return 0;", "}"]
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "l.c")
+        exe = os.path.join(d, "l")
+        open(c, "w").write("\n".join(src) + "\n")
+        subprocess.check_call([cc, "-std=c99", "-I", os.path.join(REPO, "include"), c, "-o", exe])
+        vals = [int(x) for x in subprocess.check_output([exe]).split()]
+    return vals[0], vals[1:]
+
+
+@pytest.mark.parametrize("py, c", [(sgs.Config, "sgs_config"), (sgs.EngineStats, "sgs_engine_stats"),
+                                   (sgs.QueryStats, "sgs_query_stats"),
+                                   (sgs.KernelStats, "sgs_kernel_stats"), (sgs.Tune, "sgs_tune"),
+                                   (sgs.Request, "sgs_request"), (sgs.Completion, "sgs_completion"),
+                                   (sgs.PprStats, "sgs_ppr_stats")])
+def test_ctypes_structs_match_the_header(py, c):
+    """The binding's ctypes mirrors have the C structs' size and field
+    offsets, so fields appended to the header cannot drift apart."""
+    names = [f for f, _ in py._fields_]
+    size, offs = _c_layout(c, names)
+    assert ctypes.sizeof(py) == size
+    assert [getattr(py, n).offset for n in names] == offs
