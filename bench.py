@@ -90,6 +90,9 @@ def parse():
     ap.add_argument("--host-policy", type=int, default=None,
                     help="reads of the host tier in a repair (-hybrid): 0 zero-copy, 1 explicit copy "
                          "every snapshot, 2 explicit copy for dense repairs; library default otherwise")
+    ap.add_argument("--repair", type=int, default=None,
+                    help="1: narrow groups repair deletions by pulling into the reset vertices (fewer edges "
+                         "read and counted); library default (0: the reference's re-push) otherwise")
     ap.add_argument("--pr-scale", type=int, default=16)
     ap.add_argument("--pr-updates", type=int, default=20_000)
     ap.add_argument("--bfs-sources", type=int, default=8)
@@ -209,6 +212,8 @@ def pers(a):
         o["pull"] = int(a.pull)
     if getattr(a, "host_policy", None) is not None:
         o["host_policy"] = int(a.host_policy)
+    if getattr(a, "repair", None) is not None:
+        o["repair"] = int(a.repair)
     return o
 
 
@@ -461,7 +466,8 @@ def engine_arm(a, R):
                    "parallelism": "replicas" if R.world > 1 else "single GPU",
                    "queries": ["sssp:0", "bfs:0", "cc"],
                    "autotune": tune, "persistent": a.persistent, "edge_cache": cache,
-                   "host_policy": a.host_policy, "host_stagings": int(st["host_stagings"])},
+                   "host_policy": a.host_policy, "host_stagings": int(st["host_stagings"]),
+                   "repair": a.repair},
         "e2e": e2e,
         "gpu_launches": gpu_launches,
         "roofline": roof,

@@ -269,10 +269,12 @@ struct sgs_engine {
   bool in_built = false, in_failed = false;
   DBuf<uint64_t> in_off;
   DBuf<uint32_t> in_slots, in_live, in_cap, in_adj;
+  DBuf<uint32_t> in_wgt;               // weights too, for the pull repair of SSSP lanes
   DBuf<unsigned long long> in_top;     // [2]; tier 1 unused
   uint64_t in_capslots = 0;
   uint64_t in_builds = 0;
   DBuf<uint64_t> t_dkeys, t_ikeys, t_tmp;  // the batch's keys transposed
+  DBuf<uint32_t> t_iw;                     // and the kept inserts' weights
 
   // explicit-copy host policy (cfg.host_policy): the used host arena copied
   // to HBM by the copy engine for a snapshot's repair, readers pointed at it
@@ -342,6 +344,8 @@ struct sgs_engine {
     }
     return g;
   }
+  // the in-edge store keeps weights when the pull repair may need them
+  bool in_w() const { return (cfg.repair & 1u) && cfg.weight_mode == SGS_W_EXPLICIT; }
   GraphView in_view() {
     GraphView g{};
     g.nv = nv;
@@ -350,7 +354,8 @@ struct sgs_engine {
     g.live = in_live.p;
     g.cap = in_cap.p;
     g.adj_d = in_adj.p;
-    g.wmode = SGS_W_UNIT;
+    g.wgt_d = in_w() ? in_wgt.p : nullptr;
+    g.wmode = in_w() ? SGS_W_EXPLICIT : SGS_W_UNIT;
     return g;
   }
   FrontierView fview(uint32_t buf, unsigned long long *counter) {
@@ -565,11 +570,12 @@ struct sgs_engine {
     sync();
     in_capslots = total + (uint64_t)(total * std::max(0.0, cfg.arena_headroom)) + 4096;
     in_adj.ensure(in_capslots);
+    if (in_w()) in_wgt.ensure(in_capslots);
     unsigned long long tops[2] = {total, 0};
     CK(cudaMemcpyAsync(in_top.p, tops, sizeof(tops), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(in_live.p, 0, sizeof(uint32_t) * nv, s));  // the fill cursors
     { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(
-        f0, f1, InFillOp{g, in_off.p, in_live.p, in_adj.p}, nullptr); }
+        f0, f1, InFillOp{g, in_off.p, in_live.p, in_adj.p, in_w() ? in_wgt.p : nullptr}, nullptr); }
     CK(cudaMemcpyAsync(in_live.p, in_slots.p, sizeof(uint32_t) * nv, cudaMemcpyDeviceToDevice, s));
     CK(cudaGetLastError());
     sync();
@@ -582,6 +588,7 @@ struct sgs_engine {
     in_live.release();
     in_cap.release();
     in_adj.release();
+    in_wgt.release();
     in_built = false;
   }
   // True when the in-store is there (built now if needed).  If it cannot be
@@ -629,9 +636,18 @@ struct sgs_engine {
     t_tmp.ensure(nkept);
     { ++n_launch; k_transpose_keys<<<grid_elem(nkept), 256, 0, s>>>(b_ikept.p, nkept, nullptr, t_tmp.p); }
     tb = 0;
-    CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, t_tmp.p, t_ikeys.p, (int)nkept, 0, eb, s));
-    cub_ensure(tb);
-    CK(cub::DeviceRadixSort::SortKeys(cub_tmp.p, tb, t_tmp.p, t_ikeys.p, (int)nkept, 0, eb, s));
+    if (in_w()) {  // the kept inserts' weights travel with their transposed keys
+      t_iw.ensure(nkept);
+      CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, t_tmp.p, t_ikeys.p, b_iw_kept.p, t_iw.p, (int)nkept, 0, eb,
+                                         s));
+      cub_ensure(tb);
+      CK(cub::DeviceRadixSort::SortPairs(cub_tmp.p, tb, t_tmp.p, t_ikeys.p, b_iw_kept.p, t_iw.p, (int)nkept, 0,
+                                         eb, s));
+    } else {
+      CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, t_tmp.p, t_ikeys.p, (int)nkept, 0, eb, s));
+      cub_ensure(tb);
+      CK(cub::DeviceRadixSort::SortKeys(cub_tmp.p, tb, t_tmp.p, t_ikeys.p, (int)nkept, 0, eb, s));
+    }
     InsertCtx c{};
     c.arena_top = in_top.p;
     c.arena_cap[0] = in_capslots;
@@ -660,7 +676,8 @@ struct sgs_engine {
     CK(cudaMemsetAsync(rl_count.p, 0, sizeof(unsigned long long), s));
     CK(cudaMemsetAsync(b_err.p, 0, sizeof(unsigned int), s));
     { ++n_launch; k_insert_plan<<<grid_elem(nkept), 256, 0, s>>>(gi, t_ikeys.p, b_nkept.p, c, 0, nullptr); }
-    { ++n_launch; k_insert_write<<<grid_elem(nkept), 256, 0, s>>>(gi, t_ikeys.p, nullptr, b_nkept.p, wbase.p); }
+    { ++n_launch; k_insert_write<<<grid_elem(nkept), 256, 0, s>>>(gi, t_ikeys.p, in_w() ? t_iw.p : nullptr,
+                                                      b_nkept.p, wbase.p); }
     CK(cudaMemsetAsync(special(6), 0, sizeof(unsigned long long) * 2, s));
     { ++n_launch; k_reloc_frontier<<<grid_elem(nkept), 256, 0, s>>>(rl_count.p, rl_len.p, fview(0, special(6))); }
     { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(6)), fview(1, special(7)),
@@ -1915,6 +1932,33 @@ struct sgs_engine {
                          mem == SGS_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
   }
 
+  // Repair of a narrow group by pull (cfg.repair bit 0): round 0 pulls over
+  // the in-edges of the vertices the invalidation reset (GroupPullOp), the
+  // kept inserted edges are relaxed into round 1's frontier, and the later
+  // rounds push from the vertices that improved (one cooperative launch).
+  // Returns the rounds run; fails on the round limit.
+  uint32_t pull_repair(Group &G, bool had_deletes, uint64_t ni, bool explicit_w) {
+    const GraphView g = view(), gi = in_view();
+    const uint32_t anyw = G.any_sssp(G.used | 0xF) && cfg.weight_mode == SGS_W_EXPLICIT;
+    CK(cudaMemsetAsync(rstat.p, 0, sizeof(unsigned long long) * (cfg.max_rounds + 2), s));
+    CK(cudaMemsetAsync(hstat.p, 0, sizeof(unsigned long long) * (cfg.max_rounds + 2), s));
+    if (had_deletes)
+      { ++n_launch; k_bits_frontier<<<grid_elem(nv), 256, 0, s>>>(G.ibits.p, gi, (uint32_t)G.used, gm[0].p,
+                                                       fview(0, cnt.p)); }
+    launch_group(0, GroupPullOp<GMAX>{gi, slots.p, G.st.p, G.val.p, gm[0].p, gm[1].p, G.algo(), cfg.weight_mode});
+    if (ni)
+      { ++n_launch; k_group_relax_inserted<GMAX><<<grid_elem(ni), 256, 0, s>>>(
+          g, G.st.p, G.val.p, (uint32_t)G.used, G.algo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr,
+          b_nkept.p, gm[1].p, fview(1, cnt.p + 1), b_lane.p, nullptr); }
+    CK(cudaGetLastError());
+    bool conv = false;
+    const uint32_t r = run_group_persistent(GroupRelaxOp<GMAX>{g, G.st.p, G.val.p, nullptr, nullptr, G.algo(),
+                                                               anyw},
+                                            1, conv, SGS_K_GROUP, anyw ? 8.0 : 4.0);
+    if (!conv) fail(SGS_ERR_NOCONV, "round limit reached before convergence");
+    return r;
+  }
+
   int sort_bits() const {
     int b = 1;
     while (b < 32 && (1ull << b) < nv) ++b;
@@ -1994,6 +2038,12 @@ struct sgs_engine {
       CK(cudaMemsetAsync(G.dstat.p, 0, sizeof(unsigned long long) * 3 * WLANES, s));
     }
 
+    // pull repair of narrow groups (cfg.repair): the in-edge store is built
+    // here if needed, before any frontier of this snapshot is seeded
+    bool any_narrow = false;
+    for (size_t i = 0; i < ng; ++i) any_narrow |= groups[i]->used && !groups[i]->wide();
+    const bool prep = (cfg.repair & 1u) && any_narrow && nd && ensure_in();
+
     // ---- PR cancel over the old out-lists of touched sources
     if (any_pr) {
       build_touched(g, ni, nd);
@@ -2016,11 +2066,12 @@ struct sgs_engine {
       CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * WLANES, s));
       CK(cudaMemsetAsync(b_inval.p, 0, sizeof(unsigned long long) * WLANES, s));
       reset_counters(0);
-      if (G.wide()) {
+      if (G.wide() || prep) {  // bitmap of the vertices this invalidation resets
         const size_t nw = (size_t)nv / 32 + 1;
         G.ibits.ensure(nw);
         CK(cudaMemsetAsync(G.ibits.p, 0, sizeof(uint32_t) * nw, s));
       }
+      uint32_t *nmark = prep ? G.ibits.p : nullptr;  // narrow groups mark only for the pull repair
       bool conv = false;
       if (G.wide()) {
         { ++n_launch; k_wide_seed_deleted<<<grid_elem(nd), 256, 0, s>>>(
@@ -2034,16 +2085,16 @@ struct sgs_engine {
       } else {
         { ++n_launch; k_group_seed_deleted<GMAX><<<grid_elem(nd), 256, 0, s>>>(
             g, G.st.p, G.val.p, (uint32_t)G.used, G.algo(), b_dkeys_s.p, (uint32_t)nd, b_inval.p,
-            nullptr, gm[0].p, fview(0, cnt.p)); }
+            nmark, gm[0].p, fview(0, cnt.p)); }
         CK(cudaGetLastError());
         if (cfg.persistent & 2u)
           run_group_persistent(GroupInvalidateOp<GMAX>{g, G.st.p, G.val.p, nullptr, nullptr, G.algo(),
-                                                       b_inval.p, nullptr},
+                                                       b_inval.p, nmark},
                                0, conv, SGS_K_GROUP_INVAL, 4.0);
         else
           run_group_rounds(
               [&](uint32_t, uint32_t *mi, uint32_t *mo) {
-                return GroupInvalidateOp<GMAX>{g, G.st.p, G.val.p, mi, mo, G.algo(), b_inval.p, nullptr};
+                return GroupInvalidateOp<GMAX>{g, G.st.p, G.val.p, mi, mo, G.algo(), b_inval.p, nmark};
               },
               conv, SGS_K_GROUP_INVAL, 4.0);
       }
@@ -2128,6 +2179,15 @@ struct sgs_engine {
       // the path is chosen on the device from the group's reset counts
       // (G.dstat[0, 64)): the dense frontier only if a lane was reset
       const unsigned long long *resets = G.dstat.p;
+      if (!G.wide() && prep) {  // work-efficient repair: pull into the reset vertices
+        bool conv = false;
+        grounds[i] = pull_repair(G, gdel[i] != 0, ni, explicit_w);
+        (void)conv;
+        CK(cudaEventRecord(gev[4 * i + 3], s));
+        CK(cudaMemcpyAsync(G.dstat.p + 2 * WLANES, b_lane.p, sizeof(unsigned long long) * WLANES,
+                           cudaMemcpyDeviceToDevice, s));
+        continue;
+      }
       if (G.wide())
         { ++n_launch; k_wide_dense<<<grid_elem(nv), RELAX_THREADS, 0, s>>>(g, G.val.p, G.used, G.cc, wm[0].p,
                                                                fview(0, cnt.p), resets); }
@@ -2522,6 +2582,7 @@ SGS_API void sgs_config_default(sgs_config *c) {
   c->pull = 1;  // PageRank sweeps as pulls; bit 1 (direction-optimizing BFS) is opt-in
   c->host_policy = 0;  // zero-copy reads of the host tier
   c->pr_warm = 1;
+  c->repair = 0;  // the reference's re-push from every reached vertex
 }
 
 SGS_API int sgs_create(const sgs_config *cfg, sgs_engine **out) {

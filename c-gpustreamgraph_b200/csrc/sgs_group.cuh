@@ -86,6 +86,8 @@ struct GroupRelaxOp {
   struct Quad {
     uint4 ids, ws;
   };
+  // slots of an appended vertex (its range in the next frontier)
+  __device__ __forceinline__ uint32_t append_len(uint32_t v) const { return g.slots[v]; }
   // H: the graph has a host tier (blocks may be host-resident or cached)
   template <bool H>
   __device__ __forceinline__ Quad fetch(const Payload &p, uint32_t j0) const {
@@ -179,6 +181,7 @@ struct GroupInvalidateOp {
   struct Quad {
     uint4 ids;
   };
+  __device__ __forceinline__ uint32_t append_len(uint32_t v) const { return g.slots[v]; }
   template <bool H>
   __device__ __forceinline__ Quad fetch(const Payload &p, uint32_t j0) const {
     if constexpr (H) return Quad{ld_quad(adj_at(g, p.off, j0))};
@@ -348,7 +351,7 @@ __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
             const bool w = app >> k & 1u;
-            frontier_append(out, w, dst[k], w ? op.g.slots[dst[k]] : 0u);
+            frontier_append(out, w, dst[k], w ? op.append_len(dst[k]) : 0u);
           }
         }
       }

@@ -59,6 +59,7 @@ struct InFillOp {
   const uint64_t *in_off;
   uint32_t *cursor;
   uint32_t *in_adj;
+  uint32_t *in_wgt;  // null: ids only
   __device__ __forceinline__ Payload load(uint32_t, uint32_t v) const { return Payload{g.off[v]}; }
   __device__ __forceinline__ uint32_t visit(uint32_t, const Payload &, uint32_t, bool &, uint32_t &,
                                             uint32_t &) const {
@@ -67,10 +68,14 @@ struct InFillOp {
   __device__ __forceinline__ uint32_t visit4(uint32_t u, const Payload &p, uint32_t j0, uint32_t len,
                                              bool (&)[4], uint32_t (&)[4], uint32_t (&)[4]) const {
     const uint4 ids = ld_quad(adj_at(g, p.off, j0));
+    const uint4 ws = in_wgt ? ld_quad(wgt_at(g, p.off, j0)) : make_uint4(0, 0, 0, 0);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const uint32_t d = quad_at(ids, k);
-      if (j0 + k < len && d != SGS_TOMB) in_adj[in_off[d] + atomicAdd(&cursor[d], 1u)] = u;
+      if (j0 + k >= len || d == SGS_TOMB) continue;
+      const uint64_t at = in_off[d] + atomicAdd(&cursor[d], 1u);
+      in_adj[at] = u;
+      if (in_wgt) in_wgt[at] = quad_at(ws, k);
     }
     return 0;
   }
@@ -278,6 +283,122 @@ __global__ void __launch_bounds__(RELAX_THREADS)
       }
     }
     frontier_append(out, want, (uint32_t)v, d);
+  }
+}
+
+// Work-efficient repair, round 0 of a narrow group after an invalidation:
+// instead of re-pushing from every reached vertex, every vertex the
+// invalidation reset pulls over its in-edges (the in-edge store, with
+// weights) and takes, per lane, the best candidate its in-neighbours give.
+// Before the repair every other edge already satisfies value(u) + w >=
+// value(v), so the edges into reset vertices (and the inserted edges, relaxed
+// right after) hold every violated edge; later rounds push from the
+// vertices that improved.  Runs in group_map with the in-edge store as the
+// map's graph; a vertex is appended with its out-slots.
+template <int S>
+struct GroupPullOp {
+  using Payload = GPay<S>;
+  GraphView g;                 // the in-edge store
+  const uint32_t *out_slots;   // out-store slots (append lengths)
+  unsigned long long *st;
+  uint32_t *val;
+  const uint32_t *m_in;
+  uint32_t *m_out;
+  LaneAlgo algo;
+  int wmode;                   // weights of the SSSP lanes (SGS_W_*)
+  __device__ __forceinline__ Payload load(uint32_t v) const {
+    Payload p;
+    p.off = g.off[v];
+    p.mask = __ldcg(&m_in[v]);
+    load_vals<S>(val, v, p.val);
+    return p;
+  }
+  struct Quad {
+    uint4 ids, ws;
+  };
+  __device__ __forceinline__ uint32_t append_len(uint32_t v) const { return out_slots[v]; }
+  template <bool H>
+  __device__ __forceinline__ Quad fetch(const Payload &p, uint32_t j0) const {
+    Quad q;
+    q.ids = ld_quad(g.adj_d + p.off + j0);
+    q.ws = wmode == W_EXPLICIT ? ld_quad(g.wgt_d + p.off + j0) : make_uint4(1, 1, 1, 1);
+    return q;
+  }
+  __device__ __forceinline__ uint32_t visit4(uint32_t v, const Payload &p, uint32_t j0, uint32_t len,
+                                             const Quad &qd, uint32_t (&dst)[4]) const {
+    uint32_t best[S], bu[S];
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      best[q] = INF32;
+      bu[q] = 0;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t u = quad_at(qd.ids, k);
+      if (j0 + k >= len || u == SGS_TOMB) continue;
+      uint32_t cu[S];
+      load_vals<S>(val, u, cu);
+#pragma unroll
+      for (int q = 0; q < S; ++q) {
+        if (!(p.mask >> q & 1u)) continue;
+        const int a = algo.at(q);
+        uint32_t cand;
+        if (a == A_CC) {
+          cand = cu[q];
+        } else {
+          if (cu[q] == INF32) continue;
+          uint32_t w = 1u;
+          if (a == A_SSSP)
+            w = wmode == W_EXPLICIT ? quad_at(qd.ws, k) : wmode == W_SYNTH ? (u + v) % 128u + 1u : 1u;
+          const uint64_t nd = (uint64_t)cu[q] + w;
+          if (nd >= INF32) continue;
+          cand = (uint32_t)nd;
+        }
+        if (cand < best[q]) {
+          best[q] = cand;
+          bu[q] = u;
+        }
+      }
+    }
+    uint32_t bits = 0;
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      if (best[q] >= p.val[q]) continue;
+      const uint64_t idx = (uint64_t)v * S + q;
+      const unsigned long long old = atomicMin(&st[idx], ((unsigned long long)best[q] << 32) | bu[q]);
+      if (best[q] < (uint32_t)(old >> 32)) {
+        atomicMin(&val[idx], best[q]);
+        bits |= 1u << q;
+      }
+    }
+    dst[0] = v;
+    dst[1] = dst[2] = dst[3] = 0;
+    return bits && out_slots[v] && atomicOr(&m_out[v], bits) == 0u ? 1u : 0u;
+  }
+};
+
+// Frontier of the vertices set in a bitmap that have in-edges (len = their
+// in-slots), with lane mask `lanes` in m_out; eight vertices per thread.
+__global__ void k_bits_frontier(const uint32_t *bits, GraphView gi, uint32_t lanes, uint32_t *m_out,
+                                FrontierView out) {
+  constexpr int N = 8;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * N;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x * N; b < gi.nv; b += stride) {
+    const uint64_t v0 = b + (uint64_t)threadIdx.x * N;
+    bool want[N];
+    uint32_t d[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      const uint64_t v = v0 + i;
+      want[i] = false;
+      d[i] = 0;
+      if (v < gi.nv && bit_at(bits, (uint32_t)v)) {
+        d[i] = gi.slots[v];
+        want[i] = d[i] > 0;
+        if (want[i]) m_out[v] = lanes;
+      }
+    }
+    frontier_append_block_n<N>(out, want, (uint32_t)v0, d);
   }
 }
 

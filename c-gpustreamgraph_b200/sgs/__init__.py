@@ -84,6 +84,7 @@ class Config(C.Structure):
         ("pull", C.c_uint32),
         ("host_policy", C.c_uint32),
         ("pr_warm", C.c_uint32),
+        ("repair", C.c_uint32),
     ]
 
 

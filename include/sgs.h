@@ -139,6 +139,13 @@ typedef struct sgs_config {
                              graph computed first; same tolerance, fewer
                              rounds after small changes); 0: every start
                              from scratch                                  */
+  uint32_t repair;        /* bit 0: narrow groups repair after deletions by
+                             pulling over the in-edges of the vertices the
+                             invalidation reset (in-edge store with
+                             weights), instead of the reference's re-push
+                             from every reached vertex: same results, far
+                             fewer edges read and counted; 0 (default): the
+                             reference's re-push                            */
 } sgs_config;
 
 typedef struct sgs_query_stats {
