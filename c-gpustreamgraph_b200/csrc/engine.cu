@@ -1899,6 +1899,16 @@ struct sgs_engine {
       t.a[k].ensure(cnt[k]);
       CK(cudaMemcpyAsync(t.a[k].p, src[k], cnt[k] * sizeof(uint32_t), kind, sc));
     }
+    // the other slot grows with it (an allocation later, while copies and
+    // snapshots are in flight, would stall the pipeline)
+    Staged &o = stg[(stg_head + stg_count + 1) % 2];
+    if (!o.copied) {
+      CK(cudaEventCreateWithFlags(&o.copied, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&o.consumed, cudaEventDisableTiming));
+      CK(cudaEventRecord(o.consumed, s));
+    }
+    for (int k = 0; k < 5; ++k)
+      if (cnt[k] && o.a[k].n < cnt[k] && !o.full) o.a[k].ensure(cnt[k]);
     CK(cudaEventRecord(t.copied, sc));
     t.ni = ni;
     t.nd = nd;
