@@ -163,6 +163,48 @@ def test_pagerank_oracle_dense_solve(seed):
     assert np.max(np.abs(x - x_ref)) < 1e-10
 
 
+@pytest.mark.parametrize("seed", [3, 4])
+def test_pagerank_warm_start_and_stop_rule(seed):
+    """The algebra of the engine's PageRank rounds, restated on the CPU: from
+    any x0 (here the fixed point of the graph before a snapshot), residual
+    r0 = (1-a) + a P^T x0 - x0, then rounds x += r, r <- a P^T r (absorb and
+    sweep) until sum|r| < tol reach the fixed point of the new graph within
+    tol / (1 - a) in L-inf, in fewer rounds than a start from x = 0,
+    r = 1 - a; signed residuals included."""
+    import scipy.sparse as sp
+
+    a, tol = 0.85, 1.5e-7
+    nv, row, col = O.rmat_csr(10, 8, seed)
+    i_s, i_d, d_s, d_d = O.gen_updates(nv, row, col, seed, 200, 200)
+    row2, col2, _ = O.apply(nv, row, col, None, i_s, i_d, None, d_s, d_d)
+
+    def pt(r_, c_):
+        src = np.repeat(np.arange(nv), np.diff(r_.astype(np.int64)))
+        deg = np.diff(r_.astype(np.int64)).astype(np.float64)
+        val = 1.0 / deg[src]
+        return sp.csr_matrix((val, (c_.astype(np.int64), src)), shape=(nv, nv))
+
+    P2 = pt(row2, col2)
+
+    def rounds(x, r):
+        k = 0
+        while True:
+            l1 = np.abs(r).sum()
+            x = x + r
+            k += 1
+            if l1 < tol:
+                return x, k
+            r = a * (P2 @ r)
+
+    x_old = O.pagerank(nv, row, col)
+    x_new = O.pagerank(nv, row2, col2)
+    xw, kw = rounds(x_old.copy(), (1 - a) + a * (P2 @ x_old) - x_old)
+    xc, kc = rounds(np.zeros(nv), np.full(nv, 1 - a))
+    assert np.max(np.abs(xw - x_new)) <= tol / (1 - a)
+    assert np.max(np.abs(xc - x_new)) <= tol / (1 - a)
+    assert kw < kc
+
+
 def test_sssp_dijkstra_vs_fifo_explicit_weights():
     nv, row, col = O.rmat_csr(11, 16, 9)
     w = O.weights(nv, row, col, 3, 0)
