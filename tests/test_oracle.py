@@ -205,6 +205,77 @@ def test_pagerank_warm_start_and_stop_rule(seed):
     assert kw < kc
 
 
+@pytest.mark.parametrize("seed", [5, 6, 7])
+def test_incremental_sssp_repair_strategies(seed):
+    """The engine's incremental SSSP after a snapshot, restated on the CPU:
+    parent-tree invalidation of the deleted tree edges (every descendant
+    reset), then either the reference's re-push from every reached vertex or
+    the pull over the in-edges of the reset vertices plus the inserted edges,
+    then rounds from the vertices that improved.  Both reach the distances of
+    a from-scratch run on the new graph."""
+    INF = 0xFFFFFFFF
+    nv, row, col = O.rmat_csr(9, 8, seed)
+    w = O.weights(nv, row, col, seed, 0)
+    d0, p0 = O.sssp(nv, row, col, w, 0)
+    i_s, i_d, d_s, d_d = O.gen_updates(nv, row, col, seed, 150, 150)
+    iw = np.array([O.weight_of(seed, u, v) for u, v in zip(i_s, i_d)], np.uint32)
+    row2, col2, w2 = O.apply(nv, row, col, w, i_s, i_d, iw, d_s, d_d)
+    want, _ = O.sssp(nv, row2, col2, w2, 0)
+
+    src2 = np.repeat(np.arange(nv), np.diff(row2.astype(np.int64)))
+
+    def relax_rounds(d, frontier):
+        d = d.copy()
+        while frontier:
+            nxt = set()
+            for u in frontier:
+                if d[u] == INF:
+                    continue
+                for e in range(int(row2[u]), int(row2[u + 1])):
+                    v, c = int(col2[e]), int(d[u]) + int(w2[e])
+                    if c < d[v]:
+                        d[v] = c
+                        nxt.add(v)
+            frontier = nxt
+        return d
+
+    # invalidation: deleted tree edges reset their child and its subtree
+    d = d0.astype(np.int64).copy()
+    par = p0.astype(np.int64)
+    deleted = set(zip(d_s.tolist(), d_d.tolist()))
+    children = {}
+    for v in range(nv):
+        if d0[v] != INF and par[v] != v:
+            children.setdefault(int(par[v]), []).append(v)
+    reset = set()
+    stack = [v for (u, v) in deleted if d0[v] != INF and par[v] == u and v != 0]
+    while stack:
+        v = stack.pop()
+        if v in reset:
+            continue
+        reset.add(v)
+        stack.extend(children.get(v, []))
+    for v in reset:
+        d[v] = INF
+    # (a) the reference's re-push from every reached vertex (and inserts)
+    da = relax_rounds(d, {v for v in range(nv) if d[v] != INF})
+    # (b) pull over the reset vertices' in-edges, then the inserted edges
+    db = d.copy()
+    improved = set()
+    for e in range(len(col2)):
+        u, v = int(src2[e]), int(col2[e])
+        if v in reset and db[u] != INF and (u not in reset) and int(db[u]) + int(w2[e]) < db[v]:
+            db[v] = int(db[u]) + int(w2[e])
+            improved.add(v)
+    for u, v, c in zip(i_s.tolist(), i_d.tolist(), iw.tolist()):
+        if db[u] != INF and int(db[u]) + c < db[v]:
+            db[v] = int(db[u]) + c
+            improved.add(v)
+    db = relax_rounds(db, improved)
+    assert np.array_equal(da.astype(np.uint32), want)
+    assert np.array_equal(db.astype(np.uint32), want)
+
+
 def test_sssp_dijkstra_vs_fifo_explicit_weights():
     nv, row, col = O.rmat_csr(11, 16, 9)
     w = O.weights(nv, row, col, 3, 0)
