@@ -66,7 +66,7 @@ const std::map<std::string, bool> &known() {
       {"residence", true}, {"sparse", false}, {"non_atomic", false}, {"cut_threshold", true},
       {"top_ranks", true}, {"print_ranks", false}, {"norm", false},
       {"hbm_budget", true}, {"weights", true}, {"snapshots", true}, {"device", true},
-      {"pull", true},
+      {"pull", true}, {"repair", true},
   };
   return k;
 }
@@ -134,6 +134,8 @@ int main(int argc, char **argv) {
   // -hybrid: 0 zero-copy, 1 explicit copy of the host tier for every repair,
   // 2 explicit copy for dense repairs (hybrid_policy.h:241-279)
   c.host_policy = (uint32_t)f.num("hybrid", 0);
+  // -repair 1: repair after deletions by pulling into the reset vertices
+  c.repair = (uint32_t)f.num("repair", 0);
   try {
     using clk = std::chrono::steady_clock;
     sgs::Engine engine(SGS_APP, &c);
