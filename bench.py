@@ -60,6 +60,8 @@ def parse():
                     help="device edge cache of the host tier, carved out of --budget-gb (0: none)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--ref-seconds", type=float, default=60.0,
+                    help="reference arm: traversal time budget over the timed snapshots")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
@@ -453,18 +455,14 @@ def engine_arm(a, R):
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(T / a.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (device R-MAT, seeded weights and update stream)",
-        "config": {"workload": f"incremental SSSP/BFS/CC, R-MAT scale {a.scale} ef {a.edge_factor} seed {a.seed}, "
-                               f"{a.updates} updates/snapshot (50/50), source 0, HBM budget {a.budget_gb} GB"
-                               + (f" ({a.cache_gb} GB of it as edge cache)" if a.cache_gb > 0 else "")
-                               + (", vertex ids randomly permuted" if getattr(a, "permute", False) else ""),
-                   "nv": nv, "ne_initial": int(st0["ne"]), "ne_final": int(st["ne"]),
+        "config": snapshot_config(a, nv, st0["ne"]),
+        "engine": {"ne_final": int(st["ne"]),
                    "hbm_resident_fraction": st["hbm_resident_vertices"] / max(nv, 1),
                    "arena_bytes_hbm": int(st["arena_bytes_hbm"]),
                    "arena_bytes_host": int(st["arena_bytes_host"]),
-                   "l2": "inputs larger than L2 (edge arena %.1f GB vs %d MB L2)" % (
+                   "edge_arena_vs_l2": "edge arena %.1f GB vs %d MB L2" % (
                        st["arena_bytes_hbm"] / 1e9, L2_BYTES // 2**20),
                    "parallelism": "replicas" if R.world > 1 else "single GPU",
-                   "queries": ["sssp:0", "bfs:0", "cc"],
                    "autotune": tune, "persistent": a.persistent, "edge_cache": cache,
                    "host_policy": a.host_policy, "host_stagings": int(st["host_stagings"]),
                    "repair": a.repair},
@@ -999,17 +997,61 @@ def ppr_cpu_baseline(g, w32, T32, a):
 
 
 # ----------------------------------------------------------------- reference arm
-def reference_arm(a, R):
-    """The reference's own CPU code for this path, on the host cores.
+class _quiet_stdout:
+    """Sends file descriptor 1 to /dev/null for the duration (native code
+    that prints would otherwise mix with the JSON line)."""
 
-    The reference computes its per-snapshot answers on the GPU; its CPU path
-    is the serial host oracles of the samples.  Each step runs the
-    reference's BFSHost (samples/hybrid_bfs/hybrid_bfs_host.cpp:33-60, built
-    from the reference sources into oracle/_ref) from scratch on that
-    snapshot's graph, once per host core with a different source, all
-    concurrently.  The snapshot's 1M updates are applied to the host graph
-    between steps, outside the timed region.  GTEPS = edges of the reached
-    vertices summed over the runs / wall time of the step."""
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+        return False
+
+
+def snapshot_config(a, nv, ne0):
+    """The `config` of the snapshot workload, identical in both arms (the
+    engine's own settings go under `engine` in its line)."""
+    return {"workload": f"incremental SSSP/BFS/CC, R-MAT scale {a.scale} ef {a.edge_factor} seed {a.seed}, "
+                        f"{a.updates} updates/snapshot (50/50), source 0, HBM budget {a.budget_gb} GB"
+                        + (f" ({a.cache_gb} GB of it as edge cache)" if a.cache_gb > 0 else "")
+                        + (", vertex ids randomly permuted" if getattr(a, "permute", False) else ""),
+            "nv": int(nv), "ne_initial": int(ne0),
+            "queries": ["sssp:0", "bfs:0", "cc"],
+            "l2": "inputs larger than L2 (the edge arena and the per-vertex state exceed the 126 MB L2)"}
+
+
+def reference_arm(a, R):
+    """The reference's own CPU path for one snapshot, on the host cores.
+
+    The reference computes its snapshots on the GPU; its CPU path is the
+    serial host PMA update plus the samples' serial host oracles.  One step =
+    one snapshot of the same update stream as the engine arm:
+
+    * the batch applied to the reference's host::PMAGraph with its own
+      insert / del_edge, inserts then deletes (include/groute/graphs/
+      csr_graph.cuh:658-811, through oracle/_ref), one thread;
+    * then, concurrently on three host threads, SSSPHostNaive from source 0
+      (samples/hybrid_sssp/hybrid_sssp_host.cu:35-63), BFSHost from source 0
+      (samples/hybrid_bfs/hybrid_bfs_host.cpp:33-60) -- both compiled from
+      the reference sources -- and the directed min-label CC (the reference
+      ships no CC host code; the oracle's restatement of hybrid_cc.cu:96-110).
+
+    Traversed edges per query = out-edges of the vertices it reached (CC: all
+    edges), the count the engine arm uses for one pass.  The host oracles
+    read a CSR, so the updated PMA is exported into one between the apply
+    and the traversals (not timed).  Every step applies its batch (timed);
+    the traversals run on the timed steps until --ref-seconds of traversal
+    time is spent, and GTEPS = their edges / (their time + the mean apply
+    time per step for each of them).  SSSPHostNaive synthesizes its weights
+    ((u+v)%128), where the engine arm stores weights uniform in [1,64]: the
+    same graph and the same per-edge work, different weight values."""
     if R.rank != 0:
         return None
     import threading as _th
@@ -1022,50 +1064,80 @@ def reference_arm(a, R):
     if O.ref_lib() is None:
         base["unavailable"] = "oracle/_ref (the reference's host code) was not built"
         return base
-    cores = os.cpu_count() or 1
     t0 = time.time()
     nv, row, col = O.rmat_csr_par(a.scale, a.edge_factor, a.seed)
+    ne0 = len(col)
     half = a.updates // 2
     nb = a.warmup + a.steps
     i_s, i_d, d_s, d_d = O.gen_updates(nv, row, col, a.seed * 1000003, nb * half, nb * half)
+    with _quiet_stdout():  # the reference's PMA Bind prints diagnostics to stdout
+        pma = O.RefPMA(nv, row, col)
+    del row, col
     setup_s = time.time() - t0
-    sources = [int(s) for s in np.linspace(0, nv - 1, cores, dtype=np.int64)]
-    sources[0] = 0
-    outs = [np.empty(nv, np.uint32) for _ in sources]
-    tot_e, tot_t, step_ms = 0, 0.0, []
+    apply_s, trav_s, trav_edges, step_ms = [], 0.0, 0, []
+    parts = {"sssp": 0.0, "bfs": 0.0, "cc": 0.0}
+    n_trav = 0
     for k in range(nb):
         s = slice(k * half, (k + 1) * half)
-        row, col, _ = O.apply(nv, row, col, None, i_s[s], i_d[s], None, d_s[s], d_d[s])
-        g = O.RefGraph(nv, row, col)
-        deg = np.diff(row)
-        ths = [_th.Thread(target=g.bfs, args=(src, out)) for src, out in zip(sources, outs)]
         t1 = time.perf_counter()
+        pma.apply(i_s[s], i_d[s], d_s[s], d_d[s])
+        ta = time.perf_counter() - t1
+        if k < a.warmup:
+            continue
+        apply_s.append(ta)
+        if trav_s >= a.ref_seconds:
+            continue
+        prow, pcol = pma.export()
+        g = O.RefGraph(nv, prow, pcol)
+        deg = np.diff(prow)
+        outs = {"sssp": np.empty(nv, np.uint32), "bfs": np.empty(nv, np.uint32)}
+        took = {}
+
+        def timed(name, fn):
+            t = time.perf_counter()
+            fn()
+            took[name] = time.perf_counter() - t
+
+        ths = [_th.Thread(target=timed, args=("sssp", lambda: g.sssp(0, outs["sssp"]))),
+               _th.Thread(target=timed, args=("bfs", lambda: g.bfs(0, outs["bfs"]))),
+               _th.Thread(target=timed, args=("cc", lambda: O.cc(nv, prow, pcol)))]
+        t2 = time.perf_counter()
         for t in ths:
             t.start()
         for t in ths:
             t.join()
-        dt = time.perf_counter() - t1
+        tt = time.perf_counter() - t2
         g.close()
-        edges = int(sum(int(deg[o != O.INF].sum()) for o in outs))
-        if k >= a.warmup:
-            tot_e += edges
-            tot_t += dt
-            step_ms.append(dt * 1e3)
-    value = tot_e / tot_t / 1e9
+        edges = int(deg[outs["sssp"] != O.INF].sum()) + int(deg[outs["bfs"] != O.INF].sum()) + int(len(pcol))
+        trav_s += tt
+        trav_edges += edges
+        n_trav += 1
+        for n in parts:
+            parts[n] += took[n]
+        step_ms.append((ta + tt) * 1e3)
+    mean_apply = statistics.mean(apply_s)
+    value = trav_edges / (trav_s + mean_apply * n_trav) / 1e9
     base.update({
         "value": round(value, 4), "ms_per_step": round(statistics.mean(step_ms), 2),
         "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (CPU R-MAT and update stream, same graph and stream as the engine arm)",
-        "config": {"workload": f"incremental SSSP/BFS/CC, R-MAT scale {a.scale} ef {a.edge_factor} seed {a.seed}, "
-                               f"{a.updates} updates/snapshot (50/50), source 0, HBM budget {a.budget_gb} GB"
-                               + (f" ({a.cache_gb} GB of it as edge cache)" if a.cache_gb > 0 else ""),
-                   "nv": nv, "setup_s": round(setup_s, 1)},
-        "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": "per snapshot: the reference's BFSHost (compiled from its sources) from "
-                                   f"scratch on the updated graph, {cores} sources run concurrently, one per "
-                                   "host core; updates applied outside the timed region"},
+        "config": snapshot_config(a, nv, ne0),
+        "reference_steps": {"applied": len(apply_s), "traversed": n_trav,
+                            "apply_ms_mean": round(mean_apply * 1e3, 1),
+                            "traversal_ms_mean": round(trav_s / max(n_trav, 1) * 1e3, 1),
+                            "per_query_ms_mean": {n: round(v / max(n_trav, 1) * 1e3, 1)
+                                                  for n, v in parts.items()},
+                            "edges_per_snapshot": round(trav_edges / max(n_trav, 1)),
+                            "setup_s": round(setup_s, 1)},
+        "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": 3, "kind": "reference",
+                         "sample": "per snapshot: the batch applied with the reference's host PMA "
+                                   "insert/del_edge (1 thread), then SSSPHostNaive(0) and BFSHost(0) "
+                                   "(reference code) and the directed CC restatement concurrently on 3 "
+                                   "threads, on %d of the %d timed snapshots (traversal budget %.0f s); "
+                                   "every snapshot's apply timed" % (n_trav, a.steps, a.ref_seconds)},
         "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     })
+    pma.close()
     return base
 
 

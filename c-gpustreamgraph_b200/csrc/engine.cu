@@ -1961,8 +1961,13 @@ struct sgs_engine {
           g, G.st.p, G.val.p, (uint32_t)G.used, G.algo(), b_ikept.p, explicit_w ? b_iw_kept.p : nullptr,
           b_nkept.p, gm[1].p, fview(1, cnt.p + 1), b_lane.p, nullptr); }
     CK(cudaGetLastError());
+    // explicit host policy (-hybrid 1/2): the push rounds after round 0 read
+    // the out-blocks, so they read an HBM copy of the host tier when the
+    // policy asks for one (policy 2 judges by round 0's frontier)
+    if (stage_wanted()) stage_host();
+    const GraphView gs = view();
     bool conv = false;
-    const uint32_t r = run_group_persistent(GroupRelaxOp<GMAX>{g, G.st.p, G.val.p, nullptr, nullptr, G.algo(),
+    const uint32_t r = run_group_persistent(GroupRelaxOp<GMAX>{gs, G.st.p, G.val.p, nullptr, nullptr, G.algo(),
                                                                anyw},
                                             1, conv, SGS_K_GROUP, anyw ? 8.0 : 4.0);
     if (!conv) fail(SGS_ERR_NOCONV, "round limit reached before convergence");

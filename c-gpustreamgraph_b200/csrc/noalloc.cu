@@ -1,9 +1,9 @@
 // noalloc.cu -- sgs_sssp_csr_noalloc: a from-scratch SSSP/BFS over a CSR that
 // the caller already holds in device memory, for callers that cannot allocate
 // device memory themselves: code running inside an allocator hook or a memory
-// pool callback, code that runs while a CUDA graph is being captured by
-// someone else, and embedders whose memory is fixed at start-up (real-time or
-// safety builds that forbid cudaMalloc after initialisation).
+// pool callback (an allocation there would re-enter the allocator), and
+// embedders whose memory is fixed at start-up (real-time or safety builds that
+// forbid cudaMalloc after initialisation).
 //
 // It runs the same relaxation kernel (seg_map) as the engine's SSSP/BFS
 // queries, but its scratch -- packed (value,parent) state, round stamps, the
@@ -18,7 +18,10 @@
 // threads on one device) race on the array and give wrong results: serialise
 // them.  The first call on a device looks up the array's device address
 // (cudaGetSymbolAddress) with that device current; make that first call
-// before any stream capture begins.
+// before any stream capture begins.  The address is cached per device ordinal
+// for the life of the process: after a cudaDeviceReset the cached address no
+// longer names the array, so the entry point must not be used on that device
+// again in the same process.
 #include <cuda_runtime.h>
 
 #include <algorithm>

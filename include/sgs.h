@@ -363,15 +363,17 @@ SGS_API int sgs_autotune(sgs_engine *e, sgs_tune *out);
  * writing dist[nv] and, if parent != NULL, parent[nv] (device pointers) on
  * `stream` (a cudaStream_t; NULL = default stream).  No counterpart in the
  * reference.  It allocates nothing: for callers that cannot call cudaMalloc
- * (allocator hooks, code running while a graph is being captured, embedders
- * whose device memory is fixed at start-up), its scratch is a fixed static
- * device array (about 36 MB, reserved on every GPU that loads the library
- * until exit), so nv <= SGS_NOALLOC_MAX_VERTICES and row[nv] <=
- * SGS_NOALLOC_MAX_EDGES, else SGS_ERR_INVALID.  Results equal those of an
- * SGS_SSSP / SGS_BFS query on the same graph (values and smallest-id tight
- * parents).  All calls on a device share the scratch: calls that overlap on
- * the GPU race and must be serialised.  The first call on a device looks up
- * the scratch address; make it before any stream capture starts. */
+ * (code inside an allocator hook or a memory-pool callback, where an
+ * allocation would re-enter the allocator; embedders whose device memory is
+ * fixed at start-up), its scratch is a fixed static device array (about
+ * 36 MB, reserved on every GPU that loads the library until exit), so nv <=
+ * SGS_NOALLOC_MAX_VERTICES and row[nv] <= SGS_NOALLOC_MAX_EDGES, else
+ * SGS_ERR_INVALID.  Results equal those of an SGS_SSSP / SGS_BFS query on the
+ * same graph (values and smallest-id tight parents).  All calls on a device
+ * share the scratch: calls that overlap on the GPU race and must be
+ * serialised.  The first call on a device looks up the scratch address; make
+ * it before any stream capture starts.  The address is kept for the life of
+ * the process, so do not call this on a device after cudaDeviceReset. */
 #define SGS_NOALLOC_MAX_VERTICES (1u << 20)
 #define SGS_NOALLOC_MAX_EDGES (1ull << 25)
 SGS_API int sgs_sssp_csr_noalloc(uint32_t nv, const uint64_t *row,

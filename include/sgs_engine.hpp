@@ -114,6 +114,15 @@ class Engine {
 
   // Snapshot k: del_edge records the deletes, add_edge applies the snapshot.
   // local_begin = (insert offset, delete offset), advanced like the reference.
+  //
+  // The whole snapshot -- inserts first, then deletes, the reference's order
+  // within a snapshot (framework.cuh:1011-1012) -- is applied by add_edge (or
+  // Compensate) in one sgs_apply_batch.  del_edge (Cancelation) changes
+  // nothing yet: results gathered between del_edge and add_edge are those of
+  // the previous snapshot.  (The reference's del_edge leaves the parent tree
+  // half invalidated on the old graph at that point, a state no caller can
+  // use; applying the deletes alone here would reverse the reference's order
+  // for an edge both inserted and deleted in one snapshot.)
   void del_edge(std::pair<uint32_t, uint32_t> &, uint32_t k) { pending_ = k; }
   void add_edge(std::pair<uint32_t, uint32_t> &local_begin, uint32_t k) {
     if (k >= adds_.size()) throw Error(SGS_ERR_INVALID, "snapshot index beyond the stream-size file");

@@ -60,6 +60,7 @@ def lib():
         "sgso_build_csr": (u64, [u32, u64, _u32p, _u32p, i32, i32, _u64p, _u32p]),
         "sgso_csr_file_order": (None, [u32, u64, _u32p, _u32p, _vp, _u64p, _u32p, _vp]),
         "sgso_weight_of": (u32, [u64, u32, u32]),
+        "sgso_weights_pairs": (None, [u64, u64, _u32p, _u32p, _u32p]),
         "sgso_weights": (None, [u32, _u64p, _u32p, u64, i32, _u32p]),
         "sgso_gen_updates": (i32, [u32, _u64p, _u32p, u64, u64, u64, _u32p, _u32p, _u32p, _u32p]),
         "sgso_apply": (u64, [u32, _u64p, _u32p, _vp, u64, _u32p, _u32p, _vp, u64,
@@ -106,6 +107,7 @@ def ref_lib():
     L.ref_pma_create.argtypes = [u32, _u64p, _u32p]
     L.ref_pma_insert.argtypes = [_vp, u32, u32]
     L.ref_pma_del.argtypes = [_vp, u32, u32]
+    L.ref_pma_apply.argtypes = [_vp, u64, _u32p, _u32p, u64, _u32p, _u32p]
     L.ref_pma_export.restype = u64
     L.ref_pma_export.argtypes = [_vp, _u64p, _u32p, u64]
     L.ref_pma_destroy.argtypes = [_vp]
@@ -182,6 +184,15 @@ def weights(nv, row, col, wseed=1, mode=0):
 
 def weight_of(wseed, u, v):
     return lib().sgso_weight_of(wseed, u, v)
+
+
+def weights_pairs(wseed, u, v):
+    """weight_of for every pair of two equal-length id arrays."""
+    u = np.ascontiguousarray(u, np.uint32)
+    v = np.ascontiguousarray(v, np.uint32)
+    w = np.empty(max(len(u), 1), np.uint32)
+    lib().sgso_weights_pairs(wseed, len(u), u, v, w)
+    return w[: len(u)].copy()
 
 
 def gen_updates(nv, row, col, seed, n_ins, n_del):
@@ -306,6 +317,13 @@ class RefPMA:
 
     def delete(self, u, v):
         self.R.ref_pma_del(self.h, int(u), int(v))
+
+    def apply(self, ins_u, ins_v, del_u, del_v):
+        """One snapshot in one call: every insert, then every delete."""
+        iu, iv = np.ascontiguousarray(ins_u, np.uint32), np.ascontiguousarray(ins_v, np.uint32)
+        du, dv = np.ascontiguousarray(del_u, np.uint32), np.ascontiguousarray(del_v, np.uint32)
+        self.R.ref_pma_apply(self.h, len(iu), iu, iv, len(du), du, dv)
+        self.cap += len(iu)
 
     def export(self):
         row = np.empty(self.nv + 1, np.uint64)

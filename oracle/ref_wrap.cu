@@ -107,6 +107,16 @@ void ref_pma_del(void *h, uint32_t u, uint32_t v) {
   p->pma.del_edge(u, v, (u + v) % 128 + 1);
 }
 
+/* One snapshot through the reference's host PMA, in the reference's order
+ * within a snapshot (framework.cuh:1011-1012): every insert, then every
+ * delete, each through its own insert / del_edge call. */
+void ref_pma_apply(void *h, uint64_t ni, const uint32_t *iu, const uint32_t *iv,
+                   uint64_t nd, const uint32_t *du, const uint32_t *dv) {
+  ref_pma *p = (ref_pma *)h;
+  for (uint64_t i = 0; i < ni; ++i) p->pma.insert(iu[i], iv[i], (iu[i] + iv[i]) % 128 + 1);
+  for (uint64_t i = 0; i < nd; ++i) p->pma.del_edge(du[i], dv[i], (du[i] + dv[i]) % 128 + 1);
+}
+
 /* Writes each vertex's live list edges_[index, index+degree) as a CSR.
  * Returns the edge count, or UINT64_MAX when cap is too small. */
 uint64_t ref_pma_export(void *h, uint64_t *row_out, uint32_t *col_out,

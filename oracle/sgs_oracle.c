@@ -232,6 +232,13 @@ uint32_t sgso_weight_of(uint64_t wseed, uint32_t u, uint32_t v) {
   return 1u + (uint32_t)(h >> 58); /* uniform in [1,64] */
 }
 
+/* The same seeded weight for each pair (u[i], v[i]) of an edge list (the
+ * weights of an update batch's inserts). */
+void sgso_weights_pairs(uint64_t wseed, uint64_t n, const uint32_t *u,
+                        const uint32_t *v, uint32_t *w) {
+  for (uint64_t i = 0; i < n; ++i) w[i] = sgso_weight_of(wseed, u[i], v[i]);
+}
+
 /* push_functor.h:306 -- the reference synthesizes (src+dst)%128+1 per edge. */
 uint32_t sgso_weight_synth(uint32_t u, uint32_t v) { return (u + v) % 128u + 1u; }
 

@@ -56,6 +56,8 @@ void sgso_csr_file_order(uint32_t nv, uint64_t ne, const uint32_t *src,
                          const uint32_t *dst, const uint32_t *w, uint64_t *row,
                          uint32_t *col, uint32_t *wout);
 uint32_t sgso_weight_of(uint64_t wseed, uint32_t u, uint32_t v);
+void sgso_weights_pairs(uint64_t wseed, uint64_t n, const uint32_t *u,
+                        const uint32_t *v, uint32_t *w);
 uint32_t sgso_weight_synth(uint32_t u, uint32_t v);
 void sgso_weights(uint32_t nv, const uint64_t *row, const uint32_t *col,
                   uint64_t wseed, int mode, uint32_t *w);

@@ -124,13 +124,16 @@ def test_cache_needs_a_budget():
         check_query(q, Mirror(nv, row, col, w), sgs.W_EXPLICIT)
 
 
+@pytest.mark.parametrize("repair", [0, 1])
 @pytest.mark.parametrize("policy", [1, 2])
-def test_explicit_host_policy(policy):
+def test_explicit_host_policy(policy, repair):
     """-hybrid 1/2: the repair reads an HBM copy of the host tier made by the
-    copy engine (every snapshot, or only for dense repairs); results exact."""
+    copy engine (every snapshot, or only for dense repairs); results exact.
+    With the pull repair (repair=1) the push rounds after its pull round read
+    the copy too."""
     nv, row, col, w = _graph(13, 16, 4, 6)
     gb = len(col) * 8 / 1e9
-    with sgs.Engine(hbm_budget_gb=0.2 * gb, segments=64, host_policy=policy) as e:
+    with sgs.Engine(hbm_budget_gb=0.2 * gb, segments=64, host_policy=policy, repair=repair) as e:
         e.load_csr(nv, row, col, w)
         m = Mirror(nv, row, col, w)
         qs = [e.add_query(sgs.SSSP, 0), e.add_query(sgs.BFS, 3), e.add_query(sgs.CC)]
