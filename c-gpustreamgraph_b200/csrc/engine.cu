@@ -236,6 +236,14 @@ struct sgs_engine {
 
   std::vector<std::unique_ptr<Query>> queries;
   std::vector<std::unique_ptr<Group>> groups;
+  // user algorithms (AppBase functors compiled in the caller's translation
+  // unit, include/sgs_app.cuh) updated by every snapshot through their hooks
+  struct AppHook {
+    int id;
+    sgs_app_hooks h;
+  };
+  std::vector<AppHook> apps;
+  int next_app = 1;
   // serving: one group kept in flight; queries join free lanes at round
   // boundaries and leave once no frontier entry carries their lane
   Group *fg = nullptr;
@@ -699,6 +707,7 @@ struct sgs_engine {
     if (n >= (1u << 27)) fail(SGS_ERR_INVALID, "more than 2^27-1 vertices is not supported");
     queries.clear();
     groups.clear();
+    apps.clear();  // user algorithms belong to the old graph
     fg = nullptr;
     frun = 0;
     loaded = false;
@@ -1980,6 +1989,52 @@ struct sgs_engine {
     return 32 + b;
   }
 
+  // The current layout as user algorithms see it (sgs_graph_view).
+  sgs_graph_view graph_view() {
+    const GraphView g = view();
+    sgs_graph_view v{};
+    v.nv = nv;
+    v.weight_mode = cfg.weight_mode;
+    v.ne = ne;
+    v.slots_total = slots_total;
+    v.off = g.off;
+    v.slots = g.slots;
+    v.live = g.live;
+    v.cap = g.cap;
+    v.adj_d = g.adj_d;
+    v.wgt_d = g.wgt_d;
+    v.adj_h = g.adj_h;
+    v.wgt_h = g.wgt_h;
+    v.cmap = g.cmap;
+    v.adj_c = g.adj_c;
+    v.wgt_c = g.wgt_c;
+    v.cbase = g.cbase;
+    v.stream = (void *)s;
+    v.device = dev;
+    return v;
+  }
+  // Runs every attached user algorithm's phase (before or after the graph
+  // update) on the engine's stream, with the snapshot's sorted device keys.
+  void run_app_hooks(bool after, uint64_t ni, uint64_t nd) {
+    if (apps.empty()) return;
+    const sgs_graph_view gv = graph_view();
+    sgs_update_view u{};
+    u.del_keys = nd ? b_dkeys_s.p : nullptr;
+    u.n_del = nd;
+    u.ins_keys = ni ? b_ikept.p : nullptr;
+    u.ins_w = ni && cfg.weight_mode == SGS_W_EXPLICIT ? b_iw_kept.p : nullptr;
+    u.n_ins = b_nkept.p;
+    u.n_ins_max = ni;
+    for (const AppHook &a : apps) {
+      sgs_app_phase_fn f = after ? a.h.after_update : a.h.before_update;
+      if (!f) continue;
+      g_last_error.clear();
+      const int rc = f(a.h.ctx, &gv, &u);
+      if (rc != SGS_OK)
+        fail(rc, g_last_error.empty() ? std::string("user algorithm phase failed") : g_last_error);
+    }
+  }
+
   void apply_batch(const uint32_t *is, const uint32_t *id, const uint32_t *iw, uint64_t ni,
                    const uint32_t *ds, const uint32_t *dd, uint64_t nd, int mem) {
     if (!loaded) fail(SGS_ERR_STATE, "no graph loaded");
@@ -2121,6 +2176,9 @@ struct sgs_engine {
                          cudaMemcpyDeviceToDevice, s));
     }
 
+    // ---- user algorithms: their deletion phase on the old graph
+    run_app_hooks(false, ni, nd);
+
     // ---- graph update
     CK(cudaEventRecord(ev_apply.a, s));
     {
@@ -2232,6 +2290,8 @@ struct sgs_engine {
     }
     staged = false;  // back to the host arena (zero-copy) for everything else
     cache_publish();  // the snapshot ends when its line copies are visible
+    // ---- user algorithms: repair and convergence on the new graph
+    run_app_hooks(true, ni, nd);
     // per-lane counters of every group, one read
     h_gstat.resize(3 * WLANES * std::max<size_t>(ng, 1));
     for (size_t i = 0; i < ng; ++i)
@@ -2990,6 +3050,34 @@ SGS_API int sgs_get_kernel_stats(sgs_engine *e, int kind, sgs_kernel_stats *out)
   *out = e->kst[kind];
   return SGS_OK;
 }
+
+SGS_API int sgs_get_graph_view(sgs_engine *e, sgs_graph_view *out) {
+  if (!e || !out) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  if (!e->loaded) { g_last_error = "no graph loaded"; return SGS_ERR_STATE; }
+  return guarded([&] { *out = e->graph_view(); });
+}
+
+SGS_API int sgs_app_attach(sgs_engine *e, const sgs_app_hooks *h, int *app_id) {
+  if (!e || !h || !app_id) { g_last_error = "null argument"; return SGS_ERR_INVALID; }
+  if (!e->loaded) { g_last_error = "no graph loaded"; return SGS_ERR_STATE; }
+  return guarded([&] {
+    e->apps.push_back({e->next_app, *h});
+    *app_id = e->next_app++;
+  });
+}
+
+SGS_API int sgs_app_detach(sgs_engine *e, int app_id) {
+  if (!e) { g_last_error = "null engine"; return SGS_ERR_INVALID; }
+  for (size_t i = 0; i < e->apps.size(); ++i)
+    if (e->apps[i].id == app_id) {
+      e->apps.erase(e->apps.begin() + i);
+      return SGS_OK;
+    }
+  g_last_error = "unknown user algorithm id";
+  return SGS_ERR_INVALID;
+}
+
+SGS_API void sgs_set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
 
 SGS_API int sgs_synchronize(sgs_engine *e) {
   if (!e) { g_last_error = "null engine"; return SGS_ERR_INVALID; }

@@ -382,6 +382,73 @@ SGS_API int sgs_sssp_csr_noalloc(uint32_t nv, const uint64_t *row,
                                  uint32_t *parent, void *stream);
 SGS_API int sgs_get_kernel_stats(sgs_engine *e, int kind, sgs_kernel_stats *out);
 
+/* ---- User algorithms (AppBase functors) on the engine's snapshot path.
+ *
+ * The reference lets a user write an algorithm as an AppBase<TValue,
+ * TBuffer, TWeight> functor struct (include/framework/variants/api.cuh:
+ * 22-160) and instantiate Engine<..., TAppImpl, ...> with it
+ * (include/framework/framework.cuh:77-140, :389-439).  Here the functor
+ * kernels are templates in include/sgs_app.cuh, compiled in the user's own
+ * translation unit; the engine (compiled once, in the library) reaches them
+ * through these plain-C hooks, so one sgs_apply_batch updates the graph, the
+ * built-in queries and every attached user algorithm together.
+ *
+ * sgs_graph_view: raw device pointers of the current graph layout (valid
+ * until the next call that changes the graph: a snapshot, a load).  Block of
+ * vertex v: off[v] (bit 63 = pinned-host arena), slots[v] used slots (live
+ * edges and tombstones 0xFFFFFFFF), live[v] live out-degree; ids in
+ * adj_d/adj_h, weights in wgt_d/wgt_h (explicit mode); cmap/adj_c/wgt_c/cbase
+ * describe the device edge cache of the host tier (NULL without one). */
+typedef struct sgs_graph_view {
+  uint32_t nv;
+  int weight_mode;          /* SGS_W_*                                       */
+  uint64_t ne;              /* live edges                                    */
+  uint64_t slots_total;     /* used slots, tombstones included               */
+  uint64_t *off;
+  uint32_t *slots, *live, *cap;
+  uint32_t *adj_d, *wgt_d, *adj_h, *wgt_h;
+  const uint32_t *cmap;
+  uint32_t *adj_c, *wgt_c;
+  uint64_t cbase;
+  void *stream;             /* the engine's cudaStream_t: hooks queue their
+                               work on it                                    */
+  int device;
+  int reserved;
+} sgs_graph_view;
+SGS_API int sgs_get_graph_view(sgs_engine *e, sgs_graph_view *out);
+
+/* The snapshot as the hooks see it (device arrays, already validated):
+ * deletes sorted by (src << 32 | dst); the inserts the engine keeps (sorted,
+ * distinct, not deleted in the same snapshot) with their weights (explicit
+ * mode; else NULL); their count on the device (*n_ins, at most n_ins_max). */
+typedef struct sgs_update_view {
+  const uint64_t *del_keys;
+  uint64_t n_del;
+  const uint64_t *ins_keys;
+  const uint32_t *ins_w;
+  const uint32_t *n_ins;
+  uint64_t n_ins_max;
+} sgs_update_view;
+
+/* before_update runs on the old graph, after the batch was validated and
+ * before any block changes (the deletion phase: parent-tree invalidation,
+ * PageRank-style cancellation); after_update runs on the new graph (the
+ * repair and convergence).  Both queue work on g->stream and may
+ * synchronise it; a non-zero return fails the snapshot with that status
+ * (the graph update itself has happened once before_update returned). */
+typedef int (*sgs_app_phase_fn)(void *ctx, const sgs_graph_view *g, const sgs_update_view *u);
+typedef struct sgs_app_hooks {
+  void *ctx;
+  sgs_app_phase_fn before_update;
+  sgs_app_phase_fn after_update;
+} sgs_app_hooks;
+/* Attaches a user algorithm; *app_id identifies it for sgs_app_detach.  The
+ * hooks stay attached until detached or the graph is reloaded. */
+SGS_API int sgs_app_attach(sgs_engine *e, const sgs_app_hooks *h, int *app_id);
+SGS_API int sgs_app_detach(sgs_engine *e, int app_id);
+/* Message for sgs_last_error() from a hook that fails. */
+SGS_API void sgs_set_last_error(const char *msg);
+
 /* Served request loop (no counterpart in the reference, whose drivers run
  * one source through a fixed snapshot list).  A trace of requests, each with
  * an arrival time in seconds, is served in arrival order on the calling

@@ -49,20 +49,21 @@ struct GraphDatum {
   std::vector<double> host_rank, host_delta;                   // PageRank
 };
 
-class Engine {
+// Graph, update stream and snapshot driving shared by the engines below: the
+// reference's Engine methods that do not depend on the algorithm.
+class EngineBase {
  public:
-  // algo: SGS_BFS, SGS_SSSP, SGS_CC or SGS_PR
-  explicit Engine(int algo, const sgs_config *cfg = nullptr) : algo_(algo) {
+  explicit EngineBase(const sgs_config *cfg = nullptr) {
     sgs_config c;
     sgs_config_default(&c);
     if (cfg) c = *cfg;
     check(sgs_create(&c, &h_));
   }
-  ~Engine() {
+  virtual ~EngineBase() {
     if (h_) sgs_destroy(h_);
   }
-  Engine(const Engine &) = delete;
-  Engine &operator=(const Engine &) = delete;
+  EngineBase(const EngineBase &) = delete;
+  EngineBase &operator=(const EngineBase &) = delete;
 
   sgs_engine *handle() const { return h_; }
 
@@ -83,13 +84,11 @@ class Engine {
     check(sgs_load_csr(h_, nv, row, col, w, SGS_MEM_HOST));
     datum_.nnodes = nv;
   }
-
-  // Engine::InitGraph(args...): the source for BFS/SSSP (clamped to
-  // [0, nnodes-1] as the samples do); PageRank's error tolerance is taken
-  // from the configuration, CC takes no argument.
-  void InitGraph(uint32_t source = 0) { source_ = source; }
-  // Engine::Start: static convergence.
-  void Start() { check(sgs_query_add(h_, algo_, source_, &qid_)); }
+  // Synthetic R-MAT graph generated on the device (sgs_load_rmat).
+  void LoadRmat(uint32_t scale, uint32_t edge_factor = 16, uint64_t seed = 1, uint64_t wseed = 1) {
+    check(sgs_load_rmat(h_, scale, edge_factor, seed, 0.57, 0.19, 0.19, wseed));
+    datum_.nnodes = 1u << scale;
+  }
 
   // Engine::get_update_file(): -update_size and -updatefile.
   void get_update_file(const std::string &update_size, const std::string &updatefile) {
@@ -117,7 +116,8 @@ class Engine {
   //
   // The whole snapshot -- inserts first, then deletes, the reference's order
   // within a snapshot (framework.cuh:1011-1012) -- is applied by add_edge (or
-  // Compensate) in one sgs_apply_batch.  del_edge (Cancelation) changes
+  // Compensate) in one sgs_apply_batch, which also updates every registered
+  // query and attached user algorithm.  del_edge (Cancelation) changes
   // nothing yet: results gathered between del_edge and add_edge are those of
   // the previous snapshot.  (The reference's del_edge leaves the parent tree
   // half invalidated on the old graph at that point, a state no caller can
@@ -138,6 +138,11 @@ class Engine {
   }
   void Cancelation(std::pair<uint32_t, uint32_t> &lb, uint32_t k) { del_edge(lb, k); }
   void Compensate(std::pair<uint32_t, uint32_t> &lb, uint32_t k) { add_edge(lb, k); }
+  // One snapshot from caller arrays (host memory).
+  void ApplyBatch(const uint32_t *ins_src, const uint32_t *ins_dst, const uint32_t *ins_w, uint64_t n_ins,
+                  const uint32_t *del_src, const uint32_t *del_dst, uint64_t n_del) {
+    check(sgs_apply_batch(h_, ins_src, ins_dst, ins_w, n_ins, del_src, del_dst, n_del, SGS_MEM_HOST));
+  }
 
   // Cache lifecycle of the reference (framework.cuh:149-308, 1304-1385):
   // hotness scoring, candidate choice, eviction and compaction are one
@@ -150,11 +155,33 @@ class Engine {
   void compact_cache() {}
   void LoadCache() { check(sgs_cache_refresh(h_)); }
 
+  uint32_t GetNodeNum() const { return datum_.nnodes; }
+
+ protected:
+  sgs_engine *h_ = nullptr;
+  GraphDatum datum_;
+  uint32_t pending_ = 0;
+  std::vector<uint64_t> adds_, dels_;
+  std::vector<uint32_t> au_, av_, aw_, du_, dv_;
+};
+
+// The engine for the four built-in algorithms of the samples.
+class Engine : public EngineBase {
+ public:
+  // algo: SGS_BFS, SGS_SSSP, SGS_CC or SGS_PR
+  explicit Engine(int algo, const sgs_config *cfg = nullptr) : EngineBase(cfg), algo_(algo) {}
+
+  // Engine::InitGraph(args...): the source for BFS/SSSP (clamped to
+  // [0, nnodes-1] as the samples do); PageRank's error tolerance is taken
+  // from the configuration, CC takes no argument.
+  void InitGraph(uint32_t source = 0) { source_ = source; }
+  // Engine::Start: static convergence.
+  void Start() { check(sgs_query_add(h_, algo_, source_, &qid_)); }
+
   void GatherValue() { gather(SGS_FIELD_VALUE); }
   void GatherParent() { gather(SGS_FIELD_PARENT); }
   void GatherBuffer() { gather(SGS_FIELD_BUFFER); }
   const GraphDatum &GetGraphDatum() const { return datum_; }
-  uint32_t GetNodeNum() const { return datum_.nnodes; }
 
   sgs_query_stats Stats() const {
     sgs_query_stats s{};
@@ -179,13 +206,8 @@ class Engine {
   }
 
   int algo_;
-  sgs_engine *h_ = nullptr;
   int qid_ = -1;
   uint32_t source_ = 0;
-  uint32_t pending_ = 0;
-  GraphDatum datum_;
-  std::vector<uint64_t> adds_, dels_;
-  std::vector<uint32_t> au_, av_, aw_, du_, dv_;
 };
 
 }  // namespace sgs

@@ -70,6 +70,7 @@ def lib():
         "sgso_bfs": (u64, [u32, _u64p, _u32p, u32, _u32p, _vp]),
         "sgso_sssp": (u64, [u32, _u64p, _u32p, _vp, u32, _u32p, _vp]),
         "sgso_cc": (u64, [u32, _u64p, _u32p, _u32p]),
+        "sgso_widest": (u64, [u32, _u64p, _u32p, _vp, u32, _u32p]),
         "sgso_pagerank": (i32, [u32, _u64p, _u32p, dbl, dbl, i32, _f64p]),
         "sgso_sssp_fifo_budget": (u64, [u32, _u64p, _u32p, _vp, u32, _u32p, u64]),
         "sgso_bfs_fifo_budget": (u64, [u32, _u64p, _u32p, u32, _u32p, u64]),
@@ -253,6 +254,14 @@ def sssp(nv, row, col, w, source):
     p = np.empty(nv, np.uint32)
     lib().sgso_sssp(nv, row, col, _ptr(w), source, d, _ptr(p))
     return d, p
+
+
+def widest(nv, row, col, w, source):
+    """Widest-path widths from source (2^32-1 at the source, 0 unreachable)."""
+    out = np.empty(max(nv, 1), np.uint32)
+    wa = None if w is None else np.ascontiguousarray(w, np.uint32)
+    lib().sgso_widest(nv, row, col, _ptr(wa), source, out)
+    return out[:nv]
 
 
 def cc(nv, row, col):

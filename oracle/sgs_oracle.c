@@ -556,6 +556,37 @@ uint64_t sgso_sssp(uint32_t nv, const uint64_t *row, const uint32_t *col,
   return edges;
 }
 
+/* Widest (maximum-bottleneck) path, a user algorithm of the functor
+ * surface with no counterpart among the reference's samples: width[s] =
+ * 2^32-1, width[v] = max over paths s -> v of the smallest weight on the
+ * path, 0 when unreachable.  Dijkstra on the max-min semiring: the heap pops
+ * the widest tentative vertex first (key = ~width). */
+uint64_t sgso_widest(uint32_t nv, const uint64_t *row, const uint32_t *col,
+                     const uint32_t *w, uint32_t source, uint32_t *width) {
+  for (uint32_t v = 0; v < nv; ++v) width[v] = 0;
+  uint64_t edges = 0;
+  if (source >= nv) return 0;
+  heap_t h = {0, 0, 0};
+  width[source] = SGSO_INF;
+  hpush(&h, ((uint64_t)(uint32_t)~SGSO_INF << 32) | source);
+  while (h.n) {
+    uint64_t x = hpop(&h);
+    uint32_t u = (uint32_t)x, b = ~(uint32_t)(x >> 32);
+    if (b != width[u]) continue;
+    for (uint64_t e = row[u]; e < row[u + 1]; ++e, ++edges) {
+      uint32_t v = col[e];
+      uint32_t we = w ? w[e] : 1u;
+      uint32_t nb = b < we ? b : we;
+      if (nb > width[v]) {
+        width[v] = nb;
+        hpush(&h, ((uint64_t)(uint32_t)~nb << 32) | v);
+      }
+    }
+  }
+  free(h.a);
+  return edges;
+}
+
 /* hybrid_cc.cu:96-110 pushes atomicMin(buffer[dst], buffer[src]) along
  * out-edges from buffer[v] = v (hybrid_cc.cu:46-49): the fixed point is the
  * smallest id that reaches v.  Computed by searching from ids in increasing

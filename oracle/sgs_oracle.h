@@ -104,6 +104,9 @@ uint64_t sgso_sssp(uint32_t nv, const uint64_t *row, const uint32_t *col,
                    uint32_t *parent);
 /* label(v) = min id over all vertices that reach v along out-edges
  * (v reaches itself). */
+/* widest (maximum-bottleneck) path from source; 0 = unreachable */
+uint64_t sgso_widest(uint32_t nv, const uint64_t *row, const uint32_t *col,
+                     const uint32_t *w, uint32_t source, uint32_t *width);
 uint64_t sgso_cc(uint32_t nv, const uint64_t *row, const uint32_t *col,
                  uint32_t *label);
 /* FP64 power iteration of x = (1-alpha) + alpha * A^T D^-1 x (dangling mass

@@ -109,3 +109,19 @@ def test_ctypes_structs_match_the_header(py, c):
     size, offs = _c_layout(c, names)
     assert ctypes.sizeof(py) == size
     assert [getattr(py, n).offset for n in names] == offs
+
+
+def test_sample_apps_library_loads_and_exports():
+    """The AppBase functor samples (include/sgs_app.cuh instantiated in
+    c-gpustreamgraph_b200/apps) build into a library that loads without a GPU
+    and exports its drivers."""
+    sgs.lib()
+    L = ctypes.CDLL(os.path.join(REPO, "c-gpustreamgraph_b200", "lib", "libsgs_apps.so"))
+    for n in ("sgs_sample_app_create", "sgs_sample_app_start", "sgs_sample_app_values",
+              "sgs_sample_app_parents", "sgs_sample_app_stats", "sgs_sample_app_destroy",
+              "sgs_sample_refstyle_sssp"):
+        assert hasattr(L, n), n
+    # without a graph (or a GPU) an attach is refused with a status, not a crash
+    L.sgs_sample_app_create.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_double,
+                                        ctypes.c_double, ctypes.POINTER(ctypes.c_void_p)]
+    assert L.sgs_sample_app_create(None, 1, 0, 0.0, 0.85, None) < 0

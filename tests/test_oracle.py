@@ -330,3 +330,27 @@ def test_rmat_generator_shape():
     # skew: vertex 0 is the heaviest source for a > d
     deg = np.diff(row)
     assert deg[0] == deg.max()
+
+
+def test_widest_path_oracle_brute_force():
+    """The widest-path oracle (user functor parity) equals a brute-force
+    fixed point of width[v] = max over in-edges of min(width[u], w)."""
+    for scale, seed in ((7, 1), (9, 4)):
+        nv, row, col = O.rmat_csr(scale, 8, seed)
+        w = O.weights(nv, row, col, seed, 0)
+        for src in (0, 3):
+            got = O.widest(nv, row, col, w, src)
+            b = np.zeros(nv, np.int64)
+            b[src] = 2**32 - 1
+            changed = True
+            while changed:
+                changed = False
+                for u in range(nv):
+                    if b[u] == 0:
+                        continue
+                    for e in range(row[u], row[u + 1]):
+                        nb = min(b[u], int(w[e]))
+                        if nb > b[col[e]]:
+                            b[col[e]] = nb
+                            changed = True
+            assert np.array_equal(got, b.astype(np.uint32))
