@@ -128,7 +128,7 @@ struct Group {
   // the end of the snapshot
   DBuf<unsigned long long> dstat;
   bool wide() const { return width == WLANES; }
-  LaneAlgo algo() const { return LaneAlgo{algo_packed}; }
+  LaneAlgo algo() const { return LaneAlgo::of(algo_packed); }
   WideAlgo walgo() const { return WideAlgo{sssp, cc}; }
   bool any_sssp(uint64_t lanes) const { return (lanes & sssp) != 0; }
   void set_lane(int l, int a) {

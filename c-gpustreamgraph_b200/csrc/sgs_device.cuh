@@ -172,6 +172,27 @@ __device__ __forceinline__ void hot_bump(const GraphView &g, uint32_t v, uint64_
   if ((h >> g.hot_sh & 0xFFu) != 0xFFu) g.hot[v] = h + (1u << g.hot_sh);
 }
 
+// One relaxation of a lane: the u32 value mirror *m first, then the packed
+// (value << 32 | parent) word *p; true when cand strictly lowered the mirror.
+// Only the thread whose atomicMin lowers the mirror to cand offers cand to
+// the packed word, so two equal candidates never both reach it, and the
+// packed word's parent changes only with a strictly better value.  (A 64-bit
+// atomicMin alone also replaces the parent when the values tie and the new
+// parent id is smaller.  CC labels are equal along tight parents, so such tie
+// swaps could close a parent cycle that the parent-tree invalidation never
+// reaches; SSSP/BFS parents have strictly smaller values.)  The packed update
+// is a reduction nobody waits for: when a smaller candidate overtakes this
+// one between the two atomics, the caller's "improved" only costs a redundant
+// frontier entry.  The mirror may run ahead of the packed value for a moment,
+// never below the value the packed word is about to take, so a pre-check
+// against it still rejects only candidates that cannot improve.
+__device__ __forceinline__ bool relax_mirror_packed(uint32_t *m, unsigned long long *p, uint32_t cand,
+                                                    uint32_t u) {
+  if (atomicMin(m, cand) <= cand) return false;
+  atomicMin(p, ((unsigned long long)cand << 32) | u);
+  return true;
+}
+
 // Weight of slot j of u's block.  Synthesized mode reproduces the
 // reference's per-edge (src+dst)%128+1 (push_functor.h:306).
 __device__ __forceinline__ uint32_t edge_weight(const GraphView &g, uint64_t o,
@@ -374,6 +395,25 @@ __device__ __forceinline__ unsigned long long warp_atomic_add(unsigned long long
 // multiples of 4 elements, so the address is 16-B aligned).
 __device__ __forceinline__ uint4 ld_quad(const uint32_t *p) {
   return __ldg(reinterpret_cast<const uint4 *>(p));
+}
+// The same for a stream read exactly once per pass (a frontier's ids and
+// weights): no L1 allocation, and the line is the first the L2 evicts, so
+// the randomly re-read per-vertex state keeps more of the L2.
+// (A 128-bit load takes its L2 priority from a cache policy operand; the
+// plain .L2::evict_first qualifier is for 256-bit loads only.)
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ uint4 ld_quad_stream(const uint32_t *p) {
+  uint4 r;
+  // (not volatile: a pure read of data no kernel writes while it runs, so
+  // the compiler may schedule it freely)
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+      : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+      : "l"(p), "l"(l2_evict_first_policy()));
+  return r;
 }
 __device__ __forceinline__ uint32_t quad_at(const uint4 &q, int k) {
   return k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w;

@@ -27,7 +27,21 @@ constexpr int GCHUNK = 512;  // entries staged per chunk by group_map
 
 struct LaneAlgo {
   uint32_t packed;  // 8 bits per lane: A_BFS / A_SSSP / A_CC
+  // the same as lane bit masks (bit q = lane q), so a relaxation picks a
+  // lane's step from kernel-parameter constants instead of decoding `packed`:
+  // candidate = source value + (w: the edge weight, inc: 1, cc: 0)
+  uint32_t cc, w, inc;
   __device__ __forceinline__ int at(int q) const { return (packed >> (8 * q)) & 0xFF; }
+  static LaneAlgo of(uint32_t packed) {
+    LaneAlgo a{packed, 0, 0, 0};
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t k = (packed >> (8 * q)) & 0xFF;
+      if (k == A_CC) a.cc |= 1u << q;
+      else if (k == A_SSSP) a.w |= 1u << q;
+      else a.inc |= 1u << q;
+    }
+    return a;
+  }
 };
 
 template <int S>
@@ -61,10 +75,10 @@ __device__ __forceinline__ void clear_prev_masks(const uint32_t *vtx, const unsi
 }
 
 // Relaxation of every active lane of every source over its out-edges.  The
-// u32 mirror `val` filters candidates with one 16-B read per destination; the
-// packed (value,parent) word is touched only by the atomic of a strict
-// improvement, after which the mirror is lowered too (it never drops below
-// the packed value, so the filter never rejects a real improvement).
+// u32 mirror `val` filters candidates with one 16-B read per destination; a
+// candidate below it lowers the mirror first and, if that strictly lowered
+// it, the packed (value,parent) word (relax_mirror_packed: equal candidates
+// never swap a parent).
 template <int S>
 struct GroupRelaxOp {
   using Payload = GPay<S>;
@@ -80,6 +94,11 @@ struct GroupRelaxOp {
     p.off = g.off[v];
     p.mask = __ldcg(&m_in[v]);
     load_vals<S>(val, v, p.val);
+    // a BFS/SSSP lane that has not reached v pushes nothing: drop it here,
+    // once per entry, instead of testing it for every edge
+#pragma unroll
+    for (int q = 0; q < S; ++q)
+      if (p.val[q] == INF32 && !(algo.cc >> q & 1u)) p.mask &= ~(1u << q);
     return p;
   }
   // The quad's ids (and weights), loaded one step ahead by group_map.
@@ -93,11 +112,11 @@ struct GroupRelaxOp {
   __device__ __forceinline__ Quad fetch(const Payload &p, uint32_t j0) const {
     Quad q;
     if constexpr (H) {
-      q.ids = ld_quad(adj_at(g, p.off, j0));
-      q.ws = any_w ? ld_quad(wgt_at(g, p.off, j0)) : make_uint4(1, 1, 1, 1);
+      q.ids = ld_quad_stream(adj_at(g, p.off, j0));
+      q.ws = any_w ? ld_quad_stream(wgt_at(g, p.off, j0)) : make_uint4(1, 1, 1, 1);
     } else {
-      q.ids = ld_quad(g.adj_d + p.off + j0);
-      q.ws = any_w ? ld_quad(g.wgt_d + p.off + j0) : make_uint4(1, 1, 1, 1);
+      q.ids = ld_quad_stream(g.adj_d + p.off + j0);
+      q.ws = any_w ? ld_quad_stream(g.wgt_d + p.off + j0) : make_uint4(1, 1, 1, 1);
     }
     return q;
   }
@@ -120,32 +139,22 @@ struct GroupRelaxOp {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       if (!(okm >> k & 1u)) continue;
+      // this edge's weight, for the lanes that use one
+      const uint32_t w = g.wmode == W_EXPLICIT ? quad_at(ws, k)
+                         : g.wmode == W_SYNTH  ? (u + dst[k]) % 128u + 1u
+                                               : 1u;
       uint32_t bits = 0;
 #pragma unroll
       for (int q = 0; q < S; ++q) {
         if (!(p.mask >> q & 1u)) continue;
-        const int a = algo.at(q);
-        uint32_t cand;
-        if (a == A_CC) {
-          cand = p.val[q];
-        } else {
-          if (p.val[q] == INF32) continue;
-          uint32_t w = 1u;
-          if (a == A_SSSP)
-            w = g.wmode == W_EXPLICIT ? quad_at(ws, k)
-                : g.wmode == W_SYNTH  ? (u + dst[k]) % 128u + 1u
-                                      : 1u;
-          const uint64_t nd = (uint64_t)p.val[q] + w;
-          if (nd >= INF32) continue;
-          cand = (uint32_t)nd;
-        }
-        if (cand >= cur[k][q]) continue;
+        // candidate = source value + weight (SSSP) / 1 (BFS) / 0 (CC); a sum
+        // at or above INF is never below the destination's value (<= INF)
+        const uint32_t step = (algo.w >> q & 1u) ? w : (algo.inc >> q & 1u);
+        const uint64_t nd = (uint64_t)p.val[q] + step;
+        if (nd >= (uint64_t)cur[k][q]) continue;
+        const uint32_t cand = (uint32_t)nd;
         const uint64_t idx = (uint64_t)dst[k] * S + q;
-        const unsigned long long old = atomicMin(&st[idx], ((unsigned long long)cand << 32) | u);
-        if (cand < (uint32_t)(old >> 32)) {
-          atomicMin(&val[idx], cand);
-          bits |= 1u << q;
-        }
+        if (relax_mirror_packed(&val[idx], &st[idx], cand, u)) bits |= 1u << q;
       }
       if (bits && g.slots[dst[k]] && atomicOr(&m_out[dst[k]], bits) == 0u) app |= 1u << k;
     }
@@ -184,8 +193,8 @@ struct GroupInvalidateOp {
   __device__ __forceinline__ uint32_t append_len(uint32_t v) const { return g.slots[v]; }
   template <bool H>
   __device__ __forceinline__ Quad fetch(const Payload &p, uint32_t j0) const {
-    if constexpr (H) return Quad{ld_quad(adj_at(g, p.off, j0))};
-    else return Quad{ld_quad(g.adj_d + p.off + j0)};
+    if constexpr (H) return Quad{ld_quad_stream(adj_at(g, p.off, j0))};
+    else return Quad{ld_quad_stream(g.adj_d + p.off + j0)};
   }
   __device__ __forceinline__ uint32_t visit4(uint32_t u, const Payload &p, uint32_t j0, uint32_t len,
                                              const Quad &qd, uint32_t (&dst)[4]) const {
@@ -251,7 +260,6 @@ __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out
   if (threadIdx.x < GMAX) s_lane[threadIdx.x] = 0;
   if (threadIdx.x == 0) s_host = s_all = 0;
   uint32_t host_acc = 0;
-  uint32_t lane_acc[GMAX] = {0, 0, 0, 0};  // (query, edge) pairs of owned entries
   const uint64_t packed = __ldcg((const unsigned long long *)in.counter);
   const uint32_t n = (uint32_t)(packed >> CNT_SHIFT);
   const uint64_t T = packed & EDGE_MASK;
@@ -265,6 +273,7 @@ __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out
     for (;;) {
       __syncthreads();
       bool host = false;  // this thread staged a host-tier entry
+      uint32_t lane_acc[GMAX] = {0, 0, 0, 0};  // (query, edge) pairs of owned entries
 #pragma unroll
       for (int h = 0; h < GC / RELAX_THREADS; ++h) {
         const uint32_t t = threadIdx.x + h * RELAX_THREADS;
@@ -298,6 +307,13 @@ __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out
           }
         }
       }
+      // the chunk's pair counts go to shared memory now, so no register
+      // holds them through the walk
+#pragma unroll
+      for (int q = 0; q < GMAX; ++q) {
+        const uint32_t x = warp_sum(lane_acc[q]);
+        if ((threadIdx.x & 31) == 0 && x) atomicAdd(&s_lane[q], (unsigned long long)x);
+      }
       // the barrier also tells every thread whether the chunk holds
       // host-tier entries (only then does the walk account host reads)
       bool chunk_host = false;
@@ -305,64 +321,90 @@ __device__ __forceinline__ void group_map_body(FrontierView in, FrontierView out
       else __syncthreads();
       const uint64_t lo = max(E0, s_eb[0]);
       const uint64_t hi = min(E1, s_eb[GC]);
-      // Software pipeline: the owner search and id load of a thread's next
-      // quad are issued before the current quad's destination reads, so the
-      // three dependent latencies (search, ids, destination state) of
-      // consecutive quads overlap.
-      auto locate = [&](uint64_t e, int &l, uint32_t &j0) -> bool {
-        if (e >= hi) return false;
-        int a = 0, b = GC - 1;
-        while (a < b) {
-          const int m = (a + b + 1) >> 1;
-          if (s_eb[m] <= e) a = m;
-          else b = m - 1;
-        }
-        l = a;
-        j0 = (uint32_t)(e - s_eb[a]);
-        return j0 < s_len[a];
-      };
-      int lc = 0;
-      uint32_t jc = 0;
-      typename Op::Quad qc{};
-      const bool hc0 = locate(lo + 4 * threadIdx.x, lc, jc);
-      if (hc0) qc = op.template fetch<H>(s_pay[lc], jc);
-      bool hc = hc0;
-      for (uint64_t base = lo; base < hi; base += 4 * RELAX_THREADS) {
-        int ln = 0;
-        uint32_t jn = 0;
-        typename Op::Quad qn{};
-        const bool hn = locate(base + 4 * RELAX_THREADS + 4 * threadIdx.x, ln, jn);
-        if (hn) qn = op.template fetch<H>(s_pay[ln], jn);
-        uint32_t app = 0;
-        uint32_t dst[4] = {0, 0, 0, 0};
-        if (hc) {
-          app = op.visit4(s_vtx[lc], s_pay[lc], jc, s_len[lc], qc, dst);
-          if (H && chunk_host) {
-            const uint64_t o = s_pay[lc].off;
-            if ((o & HOST_BIT) && cache_line(op.g, (o & OFF_MASK) + jc) == NO_LINE)
-              host_acc += min(4u, s_len[lc] - jc);
+      // Each warp walks its own contiguous share of the chunk's positions,
+      // one window of 32 quads (128 slots) per step, lane i on quad i of the
+      // window (coalesced 512-B id reads).  Owners need no search: lane j
+      // holds the start of entry s0 + j (s0 = owner of the window's first
+      // quad), every start inside the window sets bit (start - window) / 4
+      // of a warp-wide OR, and a lane's owner is s0 plus the set bits at or
+      // below its quad.  This relies on every frontier entry having at least
+      // one slot (every append site checks it), so a window meets at most 32
+      // entries and no two starts share a bit.  The same bits give the next
+      // window's first owner.  Software pipeline: the next window's owners
+      // and id loads are issued before the current window's state reads.
+      constexpr uint32_t NW = RELAX_THREADS / 32;
+      const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+      const uint64_t nq = hi > lo ? (hi - lo) >> 2 : 0;
+      uint64_t wq = (lo >> 2) + nq * wid / NW;  // this warp's share [wq, wqe) in quads
+      const uint64_t wqe = (lo >> 2) + nq * (wid + 1) / NW;
+      if (wq < wqe) {
+        int s0;
+        {  // owner of the share's first quad: one warp-uniform search per chunk
+          const uint64_t e = wq << 2;
+          int a = 0, b = GC - 1;
+          while (a < b) {
+            const int m = (a + b + 1) >> 1;
+            if (s_eb[m] <= e) a = m;
+            else b = m - 1;
           }
+          s0 = a;
         }
-        lc = ln;
-        jc = jn;
-        qc = qn;
-        hc = hn;
-        if (__ballot_sync(0xFFFFFFFFu, app != 0u)) {
+        // Owner and first slot of this lane's quad in the window at quad q
+        // (called for consecutive windows, all lanes together); true when
+        // the quad holds slots.  Leaves s0 at the next window's first owner.
+        auto window = [&](uint64_t q, int &own, uint32_t &j0) -> bool {
+          const uint64_t p0 = q << 2, pe = p0 + 4 * 32;
+          const int j = s0 + (int)lane;
+          const uint64_t bj = j <= GC ? s_eb[j] : ~0ull;
+          const uint32_t bit = (lane >= 1 && bj < pe) ? 1u << (uint32_t)((bj - p0) >> 2) : 0u;
+          const uint32_t m = __reduce_or_sync(0xFFFFFFFFu, bit);
+          own = s0 + __popc(m & (0xFFFFFFFFu >> (31 - lane)));
+          int ns = s0 + __popc(m);
+          if (ns < GC && s_eb[ns + 1] <= pe) ++ns;  // an entry starting exactly at pe
+          s0 = ns;
+          j0 = (uint32_t)(p0 + 4 * lane - s_eb[own]);
+          return q + lane < wqe && j0 < s_len[own];
+        };
+        int oc = 0;
+        uint32_t jc = 0;
+        typename Op::Quad qc{};
+        bool hc = window(wq, oc, jc);
+        if (hc) qc = op.template fetch<H>(s_pay[oc], jc);
+        for (; wq < wqe; wq += 32) {
+          int on = 0;
+          uint32_t jn = 0;
+          typename Op::Quad qn{};
+          bool hn = false;
+          if (wq + 32 < wqe) {
+            hn = window(wq + 32, on, jn);
+            if (hn) qn = op.template fetch<H>(s_pay[on], jn);
+          }
+          uint32_t app = 0;
+          uint32_t dst[4] = {0, 0, 0, 0};
+          if (hc) {
+            app = op.visit4(s_vtx[oc], s_pay[oc], jc, s_len[oc], qc, dst);
+            if (H && chunk_host) {
+              const uint64_t o = s_pay[oc].off;
+              if ((o & HOST_BIT) && cache_line(op.g, (o & OFF_MASK) + jc) == NO_LINE)
+                host_acc += min(4u, s_len[oc] - jc);
+            }
+          }
+          oc = on;
+          jc = jn;
+          qc = qn;
+          hc = hn;
+          if (__ballot_sync(0xFFFFFFFFu, app != 0u)) {
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const bool w = app >> k & 1u;
-            frontier_append(out, w, dst[k], w ? op.append_len(dst[k]) : 0u);
+            for (int k = 0; k < 4; ++k) {
+              const bool w = app >> k & 1u;
+              frontier_append(out, w, dst[k], w ? op.append_len(dst[k]) : 0u);
+            }
           }
         }
       }
       if (s_eb[GC] >= E1 || s + GC >= n) break;
       s += GC;
     }
-  }
-#pragma unroll
-  for (int q = 0; q < GMAX; ++q) {
-    const unsigned long long x = warp_sum((unsigned long long)lane_acc[q]);
-    if ((threadIdx.x & 31) == 0 && x) atomicAdd(&s_lane[q], x);
   }
   const unsigned long long hs = warp_sum((unsigned long long)host_acc);
   if ((threadIdx.x & 31) == 0 && hs) atomicAdd(&s_host, hs);
@@ -601,11 +643,7 @@ __global__ void k_group_relax_inserted(GraphView g, unsigned long long *st, uint
         }
         if (cand >= sv[q]) continue;
         const uint64_t idx = (uint64_t)v * S + q;
-        const unsigned long long old = atomicMin(&st[idx], ((unsigned long long)cand << 32) | u);
-        if (cand < (uint32_t)(old >> 32)) {
-          atomicMin(&val[idx], cand);
-          bits |= 1u << q;
-        }
+        if (relax_mirror_packed(&val[idx], &st[idx], cand, u)) bits |= 1u << q;
       }
       if (bits) {
         d = g.slots[v];

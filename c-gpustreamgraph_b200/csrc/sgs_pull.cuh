@@ -365,11 +365,7 @@ struct GroupPullOp {
     for (int q = 0; q < S; ++q) {
       if (best[q] >= p.val[q]) continue;
       const uint64_t idx = (uint64_t)v * S + q;
-      const unsigned long long old = atomicMin(&st[idx], ((unsigned long long)best[q] << 32) | bu[q]);
-      if (best[q] < (uint32_t)(old >> 32)) {
-        atomicMin(&val[idx], best[q]);
-        bits |= 1u << q;
-      }
+      if (relax_mirror_packed(&val[idx], &st[idx], best[q], bu[q])) bits |= 1u << q;
     }
     dst[0] = v;
     dst[1] = dst[2] = dst[3] = 0;

@@ -80,12 +80,7 @@ struct WideRelaxOp {
     }
     if (cand >= cur) return false;
     const uint64_t idx = (uint64_t)v * WLANES + q;
-    const unsigned long long old = atomicMin(&st[idx], ((unsigned long long)cand << 32) | u);
-    if (cand < (uint32_t)(old >> 32)) {
-      atomicMin(&val[idx], cand);
-      return true;
-    }
-    return false;
+    return relax_mirror_packed(&val[idx], &st[idx], cand, u);
   }
 };
 
