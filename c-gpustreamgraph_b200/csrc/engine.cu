@@ -122,7 +122,8 @@ struct Group {
   uint32_t algo_packed = 0;     // narrow: 8 bits per lane
   uint64_t sssp = 0, cc = 0;    // lanes per algorithm (both widths)
   uint64_t inval[WLANES] = {};  // resets per lane in the last deletion phase
-  DBuf<uint32_t> ibits;         // bitmap of vertices reset in the last deletion phase
+  DBuf<uint32_t> ibits;         // narrow: bitmap of vertices reset in the last deletion phase
+  DBuf<unsigned long long> wreset;  // wide: per vertex, the lanes reset in the last deletion phase
   // per-lane device counters of the last snapshot: [0,64) resets, [64,128)
   // edges of the invalidation, [128,192) edges of the repair; read once at
   // the end of the snapshot
@@ -1191,10 +1192,11 @@ struct sgs_engine {
   }
 
   // Relaxation rounds for the lanes whose frontier is in buffer 0.  With
-  // `only0` (wide groups), round 0 relaxes only edges into vertices of that
+  // `only0` (wide groups: per vertex the lanes reset there), round 0 relaxes
+  // an edge only in the lanes its destination had reset, i.e. only edges into
   // bitmap; `after0` runs right after round 0 (it may append to frontier 1).
   uint32_t group_relax(Group &G, bool &conv, const char *round0 = nullptr,
-                       const uint32_t *only0 = nullptr,
+                       const unsigned long long *only0 = nullptr,
                        const std::function<void()> *after0 = nullptr) {
     GraphView g = view();
     if (G.wide()) {
@@ -2136,7 +2138,10 @@ struct sgs_engine {
       CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * WLANES, s));
       CK(cudaMemsetAsync(b_inval.p, 0, sizeof(unsigned long long) * WLANES, s));
       reset_counters(0);
-      if (G.wide() || prep) {  // bitmap of the vertices this invalidation resets
+      if (G.wide()) {  // the lanes this invalidation resets, per vertex
+        G.wreset.ensure(nv);
+        CK(cudaMemsetAsync(G.wreset.p, 0, sizeof(unsigned long long) * nv, s));
+      } else if (prep) {  // bitmap of the vertices this invalidation resets
         const size_t nw = (size_t)nv / 32 + 1;
         G.ibits.ensure(nw);
         CK(cudaMemsetAsync(G.ibits.p, 0, sizeof(uint32_t) * nw, s));
@@ -2145,11 +2150,11 @@ struct sgs_engine {
       bool conv = false;
       if (G.wide()) {
         { ++n_launch; k_wide_seed_deleted<<<grid_elem(nd), 256, 0, s>>>(
-            g, G.st.p, G.val.p, G.used, G.cc, b_dkeys_s.p, (uint32_t)nd, b_inval.p, G.ibits.p, wm[0].p,
+            g, G.st.p, G.val.p, G.used, G.cc, b_dkeys_s.p, (uint32_t)nd, b_inval.p, G.wreset.p, wm[0].p,
             fview(0, cnt.p)); }
         CK(cudaGetLastError());
         WideInvalidateOp op{G.st.p, G.val.p, WideAlgo{0ull, G.cc}};  // no weights needed
-        op.mark = G.ibits.p;
+        op.mark = G.wreset.p;
         if (cfg.persistent & 2u) run_wide_persistent(op, 0, conv, SGS_K_WIDE_INVAL, 4.0, b_inval.p);
         else run_wide_rounds(op, op, conv, SGS_K_WIDE_INVAL, 4.0, b_inval.p);
       } else {
@@ -2244,10 +2249,9 @@ struct sgs_engine {
       CK(cudaEventRecord(gev[4 * i + 2], s));
       CK(cudaMemsetAsync(b_lane.p, 0, sizeof(unsigned long long) * WLANES, s));
       reset_counters(0);
-      if (G.wide() && !gdel[i]) {  // no deletion phase ran: an empty reset bitmap
-        const size_t nw = (size_t)nv / 32 + 1;
-        G.ibits.ensure(nw);
-        CK(cudaMemsetAsync(G.ibits.p, 0, sizeof(uint32_t) * nw, s));
+      if (G.wide() && !gdel[i]) {  // no deletion phase ran: no lane was reset
+        G.wreset.ensure(nv);
+        CK(cudaMemsetAsync(G.wreset.p, 0, sizeof(unsigned long long) * nv, s));
       }
       // the path is chosen on the device from the group's reset counts
       // (G.dstat[0, 64)): the dense frontier only if a lane was reset
@@ -2281,7 +2285,7 @@ struct sgs_engine {
             b_nkept.p, wm[1].p, fview(1, cnt.p + 1), b_lane.p); }
       };
       bool conv = false;
-      grounds[i] = G.wide() ? group_relax(G, conv, "sgs:sweep", G.ibits.p, ni ? &ins_after0 : nullptr)
+      grounds[i] = G.wide() ? group_relax(G, conv, "sgs:sweep", G.wreset.p, ni ? &ins_after0 : nullptr)
                             : group_relax(G, conv, "sgs:sweep");
       if (!conv) fail(SGS_ERR_NOCONV, "round limit reached before convergence");
       CK(cudaEventRecord(gev[4 * i + 3], s));

@@ -25,6 +25,9 @@ namespace sgs {
 
 constexpr int WLANES = 64;
 constexpr int WCHUNK = 256;  // entries staged per chunk by wide_map
+// a window with more (edge, lane) pairs than this many per edge on average
+// takes the per-edge path of wide_map, a sparser one the per-pair path
+constexpr uint32_t WIDE_DENSE_LANES = 12;
 
 // Lane algorithms of a wide group as bit masks (a lane in neither is BFS).
 struct WideAlgo {
@@ -56,8 +59,10 @@ struct WideRelaxOp {
   unsigned long long *st;
   uint32_t *val;
   WideAlgo algo;
-  const uint32_t *only = nullptr;  // restrict to destinations in this bitmap
-  uint32_t *mark = nullptr;
+  // restricted rounds: per vertex, the lanes the last invalidation reset
+  // there; an edge is relaxed only in those lanes of its destination
+  const unsigned long long *only = nullptr;
+  unsigned long long *mark = nullptr;
   // the destination's current value (loaded ahead of the decision)
   __device__ __forceinline__ Pre pre(uint32_t v, int q) const {
     return __ldcg(&val[(uint64_t)v * WLANES + q]);
@@ -93,8 +98,8 @@ struct WideInvalidateOp {
   unsigned long long *st;
   uint32_t *val;
   WideAlgo algo;
-  const uint32_t *only = nullptr;
-  uint32_t *mark = nullptr;  // bitmap of reset vertices
+  const unsigned long long *only = nullptr;
+  unsigned long long *mark = nullptr;  // per vertex: the lanes reset there (OR-ed in)
   __device__ __forceinline__ Pre pre(uint32_t v, int q) const {
     return __ldcg(&st[(uint64_t)v * WLANES + q]);
   }
@@ -213,21 +218,37 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
       }
       const uint64_t lo = max(E0, s_eb[0]);
       const uint64_t hi = min(E1, s_eb[GC]);
-      for (uint64_t base = lo + (uint64_t)warp * 32; base < hi; base += (uint64_t)NW * 32) {
-        const uint64_t e = base + t;
-        bool ok = false;
-        int le = 0;
-        uint32_t v = 0, w = 1;
-        if (e < hi) {
-          int l = 0, r = GC - 1;
-          while (l < r) {
-            const int m = (l + r + 1) >> 1;
-            if (s_eb[m] <= e) l = m;
-            else r = m - 1;
+      // Windows of 32 slots, lane t on slot t (one coalesced id read), dealt
+      // round-robin to the warps so that they share the chunk's heavy and
+      // light entries evenly.  A window's first owner s0 comes from one
+      // warp-uniform search; the others need none (as in group_map): lane j
+      // holds the start of entry s0 + j, every start inside the window sets
+      // bit (start - window) of a warp-wide OR, and a slot's owner is s0 plus
+      // the set bits at or below it (every entry has at least one slot).
+      for (uint64_t wb = lo + (uint64_t)warp * 32; wb < hi; wb += (uint64_t)NW * 32) {
+        int le;
+        {
+          int a = 0, b = GC - 1;
+          while (a < b) {
+            const int m = (a + b + 1) >> 1;
+            if (s_eb[m] <= wb) a = m;
+            else b = m - 1;
           }
+          const int s0 = a;
+          const int j = s0 + t;
+          const uint64_t bj = j <= GC ? s_eb[j] : ~0ull;
+          const uint32_t bit = (t >= 1 && bj < wb + 32) ? 1u << (uint32_t)(bj - wb) : 0u;
+          const uint32_t m = __reduce_or_sync(0xFFFFFFFFu, bit);
+          le = s0 + __popc(m & (0xFFFFFFFFu >> (31 - t)));
+        }
+        const uint64_t e = wb + t;
+        bool ok = false;
+        uint32_t v = 0, w = 1;
+        unsigned long long rl = ~0ull;  // the lanes this edge may relax
+        if (e < hi) {
+          const int l = le;
           const uint32_t j = (uint32_t)(e - s_eb[l]);
           if (j < s_len[l]) {
-            le = l;
             // slot position in its arena: HBM, cache line or host
             uint64_t x = s_off[l] + j;
             int tier = 0;
@@ -240,66 +261,122 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
             }
             v = __ldcg((tier == 0 ? g.adj_d : tier == 1 ? g.adj_c : g.adj_h) + x);
             ok = v != SGS_TOMB;
-            if constexpr (Op::kRestrict) ok = ok && bit_at(op.only, v);
+            if constexpr (Op::kRestrict) {
+              if (ok) rl = __ldcg(&op.only[v]);
+              ok = ok && rl != 0ull;
+            }
             if (ok && op.algo.sssp && s_mask[l] & op.algo.sssp)
               w = g.wmode == W_EXPLICIT ? __ldcg((tier == 0 ? g.wgt_d : tier == 1 ? g.wgt_c : g.wgt_h) + x)
                   : g.wmode == W_SYNTH  ? (s_vtx[l] + v) % 128u + 1u
                                         : 1u;
           }
         }
-        bool want = false;
-        // four edges per step: their destination rows (and source rows) are
-        // all requested before any decision, so a warp keeps 16 loads per
-        // thread in flight instead of waiting once per edge
-        constexpr int D = 4;
-        uint32_t rem = __ballot_sync(0xFFFFFFFFu, ok);
-        while (rem) {
-          int ii[D], li[D];
-          uint32_t vi[D], wi[D], uu[D];
-          bool a0[D], a1[D];
+        // The window's work: (edge, active lane) pairs.  Dense windows (many
+        // lanes per edge) take the per-edge path, every thread on two lanes of
+        // each edge; sparse ones -- the common case after the first rounds --
+        // spread the pairs over the warp's threads, one pair per thread per
+        // step, so no thread idles on an inactive lane.
+        const unsigned long long mk = ok ? s_mask[le] & rl : 0ull;
+        const uint32_t c = (uint32_t)__popcll(mk);
+        uint32_t incl = c;
 #pragma unroll
-          for (int q = 0; q < D; ++q) {
-            ii[q] = rem ? __ffs(rem) - 1 : -1;
-            rem = rem ? rem & (rem - 1) : 0u;
-            const int src = ii[q] < 0 ? 0 : ii[q];
-            li[q] = __shfl_sync(0xFFFFFFFFu, le, src);
-            vi[q] = __shfl_sync(0xFFFFFFFFu, v, src);
-            wi[q] = __shfl_sync(0xFFFFFFFFu, w, src);
-            uu[q] = s_vtx[li[q]];
-            const unsigned long long mk = ii[q] < 0 ? 0ull : s_mask[li[q]];
-            a0[q] = mk >> t & 1ull;
-            a1[q] = mk >> (t + 32) & 1ull;
-          }
-          typename Op::Pre c0[D], c1[D];
-          uint32_t vu0[D], vu1[D];
+        for (int d = 1; d < 32; d <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+          if (t >= d) incl += y;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        const uint32_t excl = incl - c;
+        if (total > 32u * WIDE_DENSE_LANES) {
+          bool want = false;
+          // two edges per step: their destination rows (and source rows) are
+          // all requested before any decision, so a thread keeps 8 loads in
+          // flight instead of waiting once per edge
+          constexpr int D = 2;
+          uint32_t rem = __ballot_sync(0xFFFFFFFFu, ok);
+          while (rem) {
+            int ii[D], li[D];
+            uint32_t vi[D], wi[D], uu[D];
+            bool a0[D], a1[D];
 #pragma unroll
-          for (int q = 0; q < D; ++q) {
-            c0[q] = a0[q] ? op.pre(vi[q], t) : typename Op::Pre(0);
-            c1[q] = a1[q] ? op.pre(vi[q], t + 32) : typename Op::Pre(0);
-            vu0[q] = INF32;
-            vu1[q] = INF32;
-            if (Op::kNeedsSourceValues) {
-              // a stale (higher) source value is harmless: a source that
-              // improves during this round is appended and pushes again
-              const uint32_t *row = op.val + (uint64_t)uu[q] * WLANES;
-              if (a0[q]) vu0[q] = __ldg(row + t);
-              if (a1[q]) vu1[q] = __ldg(row + t + 32);
+            for (int q = 0; q < D; ++q) {
+              ii[q] = rem ? __ffs(rem) - 1 : -1;
+              rem = rem ? rem & (rem - 1) : 0u;
+              const int src = ii[q] < 0 ? 0 : ii[q];
+              li[q] = __shfl_sync(0xFFFFFFFFu, le, src);
+              vi[q] = __shfl_sync(0xFFFFFFFFu, v, src);
+              wi[q] = __shfl_sync(0xFFFFFFFFu, w, src);
+              uu[q] = s_vtx[li[q]];
+              const unsigned long long mkq = __shfl_sync(0xFFFFFFFFu, mk, src);
+              a0[q] = mkq >> t & 1ull;
+              a1[q] = mkq >> (t + 32) & 1ull;
+            }
+            typename Op::Pre c0[D], c1[D];
+            uint32_t vu0[D], vu1[D];
+#pragma unroll
+            for (int q = 0; q < D; ++q) {
+              c0[q] = a0[q] ? op.pre(vi[q], t) : typename Op::Pre(0);
+              c1[q] = a1[q] ? op.pre(vi[q], t + 32) : typename Op::Pre(0);
+              vu0[q] = INF32;
+              vu1[q] = INF32;
+              if (Op::kNeedsSourceValues) {
+                // a stale (higher) source value is harmless: a source that
+                // improves during this round is appended and pushes again
+                const uint32_t *row = op.val + (uint64_t)uu[q] * WLANES;
+                if (a0[q]) vu0[q] = __ldg(row + t);
+                if (a1[q]) vu1[q] = __ldg(row + t + 32);
+              }
+            }
+#pragma unroll
+            for (int q = 0; q < D; ++q) {
+              evald += (uint32_t)a0[q] + (uint32_t)a1[q];
+              const bool x0 = a0[q] && op.fin(uu[q], vi[q], wi[q], vu0[q], t, sssp0, cc0, c0[q]);
+              const bool x1 = a1[q] && op.fin(uu[q], vi[q], wi[q], vu1[q], t + 32, sssp1, cc1, c1[q]);
+              chg0 += x0;
+              chg1 += x1;
+              const unsigned long long bits = ballot64(x0, x1);
+              if (bits && t == ii[q] && op.mark) atomicOr(&op.mark[vi[q]], bits);
+              if (bits && t == ii[q] && g.slots[vi[q]])
+                want = atomicOr(&m_out[vi[q]], bits) == 0ull;
             }
           }
-#pragma unroll
-          for (int q = 0; q < D; ++q) {
-            evald += (uint32_t)a0[q] + (uint32_t)a1[q];
-            const bool x0 = a0[q] && op.fin(uu[q], vi[q], wi[q], vu0[q], t, sssp0, cc0, c0[q]);
-            const bool x1 = a1[q] && op.fin(uu[q], vi[q], wi[q], vu1[q], t + 32, sssp1, cc1, c1[q]);
-            chg0 += x0;
-            chg1 += x1;
-            const unsigned long long bits = ballot64(x0, x1);
-            if (bits && t == ii[q] && op.mark) bit_set(op.mark, vi[q]);
-            if (bits && t == ii[q] && g.slots[vi[q]])
-              want = atomicOr(&m_out[vi[q]], bits) == 0ull;
+          frontier_append(out, want, v, want ? g.slots[v] : 0u);
+        } else if (total) {
+          const uint32_t nonempty = __ballot_sync(0xFFFFFFFFu, c > 0);
+          for (uint32_t ib = 0; ib < total; ib += 32) {
+            // the pair of this thread: item ib + t belongs to the nonempty
+            // edge whose items start last at or before it -- the edge that
+            // covers item ib (carry) plus the starts inside this step
+            const uint32_t item = ib + t;
+            const uint32_t carry = __popc(__ballot_sync(0xFFFFFFFFu, c > 0 && excl <= ib)) - 1u;
+            const uint32_t sb = (c > 0 && excl > ib && excl < ib + 32) ? 1u << (excl - ib) : 0u;
+            const uint32_t ms = __reduce_or_sync(0xFFFFFFFFu, sb);
+            const bool has = item < total;
+            const uint32_t rank = carry + __popc(ms & (0xFFFFFFFFu >> (31 - t)));
+            const int sl = has ? (int)__fns(nonempty, 0, (int)rank + 1) : 0;
+            const uint32_t r = item - __shfl_sync(0xFFFFFFFFu, excl, sl);
+            const unsigned long long mj = __shfl_sync(0xFFFFFFFFu, mk, sl);
+            const uint32_t vj = __shfl_sync(0xFFFFFFFFu, v, sl);
+            const uint32_t wj = __shfl_sync(0xFFFFFFFFu, w, sl);
+            const int lej = __shfl_sync(0xFFFFFFFFu, le, sl);
+            bool want = false;
+            if (has) {
+              // lane = the r-th active lane of the edge's source
+              const uint32_t m0 = (uint32_t)mj, m1 = (uint32_t)(mj >> 32);
+              const uint32_t p0 = __popc(m0);
+              const int q = r < p0 ? (int)__fns(m0, 0, (int)r + 1) : 32 + (int)__fns(m1, 0, (int)(r - p0) + 1);
+              const uint32_t u = s_vtx[lej];
+              uint32_t vu = INF32;
+              if (Op::kNeedsSourceValues) vu = __ldg(op.val + (uint64_t)u * WLANES + q);
+              ++evald;
+              if (op.lane(u, vj, wj, vu, q, op.algo.sssp >> q & 1ull, op.algo.cc >> q & 1ull)) {
+                atomicAdd(&s_chg[q], 1ull);
+                if (op.mark) atomicOr(&op.mark[vj], 1ull << q);
+                want = g.slots[vj] && atomicOr(&m_out[vj], 1ull << q) == 0ull;
+              }
+            }
+            frontier_append(out, want, vj, want ? g.slots[vj] : 0u);
           }
         }
-        frontier_append(out, want, v, want ? g.slots[v] : 0u);
       }
       if (s_eb[GC] >= E1 || s + GC >= n) break;
       s += GC;
@@ -512,7 +589,7 @@ __global__ void k_wide_dense(GraphView g, const uint32_t *val, unsigned long lon
 __global__ void k_wide_seed_deleted(GraphView g, unsigned long long *st, uint32_t *val,
                                     unsigned long long lanes, unsigned long long cc,
                                     const uint64_t *keys, uint32_t n, unsigned long long *inval,
-                                    uint32_t *mark, unsigned long long *m_out, FrontierView out) {
+                                    unsigned long long *mark, unsigned long long *m_out, FrontierView out) {
   const int t = threadIdx.x & 31;
   const bool l0 = lanes >> t & 1ull, l1 = lanes >> (t + 32) & 1ull;
   const bool c0 = cc >> t & 1ull, c1 = cc >> (t + 32) & 1ull;
@@ -534,7 +611,7 @@ __global__ void k_wide_seed_deleted(GraphView g, unsigned long long *st, uint32_
       r0 += x0;
       r1 += x1;
       const unsigned long long bits = ballot64(x0, x1);
-      if (bits && t == i) bit_set(mark, v);
+      if (bits && t == i) atomicOr(&mark[v], bits);
       if (bits && t == i && g.slots[v]) want = atomicOr(&m_out[v], bits) == 0ull;
     }
     const uint32_t v = (uint32_t)key;
