@@ -221,6 +221,8 @@ struct sgs_engine {
   DBuf<uint32_t> b_nkept;
   DBuf<unsigned int> b_err;
   DBuf<unsigned long long> b_stat;  // [0] demand d, [1] demand h, [2] tombs, [3] inval
+  DBuf<unsigned long long> b_reclaim;  // slots reclaimed by block compaction: [0] out-, [1] in-store
+  uint64_t reclaimed_total = 0;
   DBuf<uint64_t> wbase;
   DBuf<uint32_t> rl_vtx, rl_len;
   DBuf<uint64_t> rl_from, rl_to;
@@ -406,6 +408,7 @@ struct sgs_engine {
     arena_top.ensure(2);
     b_err.ensure(1);
     b_stat.ensure(8);
+    b_reclaim.ensure(2);
     b_nkept.ensure(1);
     rl_count.ensure(1);
     l1.ensure(cfg.max_rounds + 2);
@@ -638,6 +641,7 @@ struct sgs_engine {
       TombOp op{gi, t_dkeys.p, b_gstart.p, (uint32_t)nd};
       { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(4)), fview(1, special(5)), op,
                                                    nullptr); }
+      { ++n_launch; k_compact_blocks<<<(uint32_t)nsm * 8, 256, 0, s>>>(gi, fview(0, special(4)), b_reclaim.p + 1); }
       CK(cudaGetLastError());
     }
     if (!ni || !nkept) return;
@@ -2361,6 +2365,7 @@ struct sgs_engine {
     GraphView g = view();
     unsigned long long *tombs = b_stat.p + 2;
     CK(cudaMemsetAsync(tombs, 0, sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(b_reclaim.p, 0, sizeof(unsigned long long) * 2, s));
     if (nd) {
       CK(cudaMemsetAsync(special(4), 0, sizeof(unsigned long long), s));
       b_gstart.ensure((size_t)nv + 1);
@@ -2369,6 +2374,9 @@ struct sgs_engine {
       TombOp op{g, b_dkeys_s.p, b_gstart.p, (uint32_t)nd};
       { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(4)), fview(1, special(5)), op,
                                                    tombs); }
+      // the touched blocks that now hold a sixteenth or more of dead slots are
+      // compacted in place before the inserts append to them
+      { ++n_launch; k_compact_blocks<<<(uint32_t)nsm * 8, 256, 0, s>>>(g, fview(0, special(4)), b_reclaim.p); }
       CK(cudaGetLastError());
     }
     uint32_t nkept = 0;
@@ -2423,12 +2431,14 @@ struct sgs_engine {
       if (herr) fail(SGS_ERR_OOM, "edge arena exhausted while inserting");
       nreloc = hrl;
     }
-    unsigned long long ht = 0;
+    unsigned long long ht = 0, hrc = 0;
     CK(cudaMemcpyAsync(&ht, tombs, sizeof(ht), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&hrc, b_reclaim.p, sizeof(hrc), cudaMemcpyDeviceToHost, s));
     sync();
     in_apply(ni, nd, nkept);
     ne = ne + nkept - ht;
-    slots_total += nkept;
+    slots_total = slots_total + nkept - hrc;
+    reclaimed_total += hrc;
     est.last_inserted = nkept;
     est.last_deleted = ht;
     est.last_relocated = nreloc;
@@ -2913,6 +2923,7 @@ SGS_API int sgs_get_engine_stats(sgs_engine *e, sgs_engine_stats *out) {
     e->est.bfs_bottom_up_rounds = e->bfs_bottom_up_total;
     e->est.host_stagings = e->stagings;
     e->est.pr_warm_starts = e->pr_warm_starts;
+    e->est.reclaimed_slots = e->reclaimed_total;
     e->est.last_stage_bytes = e->stage_bytes_last;
     *out = e->est;
   });

@@ -559,6 +559,53 @@ __global__ void k_reloc_frontier(const unsigned long long *rl_count, const uint3
 }
 
 // Copy op over relocation entries: vertex field = relocation list index.
+// Tombstone reclamation.  The reference's del_edge shifts the rest of the
+// list left on every delete (csr_graph.cuh:789-811) and its PMA rebalances
+// windows by density (:813-933).  Here a snapshot's deletes only write
+// tombstones, and then every block they touched whose dead slots reach a
+// sixteenth of its live ones is compacted in place: one warp per block reads 32
+// slots at a time, keeps the live ones (ballot + prefix) and writes them
+// forward, so the block's used slots become its live count and the next
+// inserts append right after them.  Each compaction costs at most 17 times
+// the slots it reclaims, and no block walked by a relaxation keeps more than
+// a sixteenth of dead slots.  Input: the frontier of the touched blocks (one
+// entry per source); reclaimed slots are added to *reclaimed.
+__global__ void k_compact_blocks(GraphView g, FrontierView f, unsigned long long *reclaimed) {
+  const uint32_t n = (uint32_t)(__ldcg((const unsigned long long *)f.counter) >> CNT_SHIFT);
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const bool ew = g.wmode == W_EXPLICIT;
+  unsigned long long got = 0;
+  for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+    const uint32_t v = __ldcg(&f.vtx[i]);
+    const uint32_t sl = g.slots[v], lv = g.live[v];
+    const uint32_t dead = sl - lv;
+    if (dead == 0 || (uint64_t)dead * 16 < lv) continue;  // warp-uniform
+    const uint64_t o = g.off[v];
+    const uint32_t *a = adj_wptr(g, o);
+    const uint32_t *wt = ew ? wgt_wptr(g, o) : nullptr;
+    uint32_t out = 0;
+    for (uint32_t j = 0; j < sl; j += 32) {
+      const uint32_t k = j + lane;
+      const uint32_t id = k < sl ? __ldcg(a + k) : SGS_TOMB;
+      const uint32_t w = (ew && k < sl) ? __ldcg(wt + k) : 0u;
+      const bool keep = id != SGS_TOMB;
+      const uint32_t b = __ballot_sync(0xFFFFFFFFu, keep);
+      // every lane's reads of this step are done before any write; writes
+      // land at or below the positions just read, never on unread slots
+      __syncwarp();
+      if (keep) store_slot(g, o, out + __popc(b & ((1u << lane) - 1u)), id, ew, w);
+      out += __popc(b);
+      __syncwarp();
+    }
+    if (lane == 0) {
+      g.slots[v] = out;
+      got += sl - out;
+    }
+  }
+  if (lane == 0 && got) atomicAdd(reclaimed, got);
+}
+
 struct RelocCopyOp {
   static constexpr bool kAppends = false;
   static constexpr bool kQuad = false;

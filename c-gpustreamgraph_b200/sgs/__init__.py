@@ -132,6 +132,7 @@ class EngineStats(C.Structure):
         ("host_stagings", C.c_uint64),
         ("last_stage_bytes", C.c_uint64),
         ("pr_warm_starts", C.c_uint64),
+        ("reclaimed_slots", C.c_uint64),
     ]
 
     def as_dict(self):

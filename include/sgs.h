@@ -194,6 +194,10 @@ typedef struct sgs_engine_stats {
   uint64_t last_stage_bytes;  /* bytes of the last one                     */
   uint64_t pr_warm_starts;    /* PageRank starts continued from a previous
                                  query's vector                            */
+  uint64_t reclaimed_slots;   /* tombstoned slots reclaimed so far: every
+                                 block a snapshot's deletes touch is
+                                 compacted in place once its dead slots
+                                 reach a sixteenth of its live ones        */
 } sgs_engine_stats;
 
 /* Per-kernel-class timing of the relaxation launches (CUDA events on the
