@@ -81,9 +81,12 @@ def parse():
     ap.add_argument("--group-size", type=int, default=64)
     ap.add_argument("--served-scale", type=int, default=26)
     ap.add_argument("--served-seconds", type=float, default=30.0)
-    ap.add_argument("--served-rate", type=float, default=6.0, help="requests per second (Poisson)")
+    ap.add_argument("--served-rate", type=float, default=12.0, help="requests per second (Poisson)")
     ap.add_argument("--served-budget-gb", type=float, default=16.0)
-    ap.add_argument("--slots", type=int, default=16)
+    ap.add_argument("--slots", type=int, default=64)
+    ap.add_argument("--served-group-size", type=int, default=64)
+    ap.add_argument("--served-plain", type=int, default=16,
+                    help="served workload: queries of the trace timed alone on the plain engine")
     ap.add_argument("--plain-sample", type=int, default=32,
                     help="batched workload: queries of the sample run one per edge pass")
     ap.add_argument("--pull", type=int, default=None,
@@ -761,7 +764,7 @@ def served_arm(a, R):
     torch.cuda.set_device(dev)
     t0 = time.time()
     e = sgs.Engine(device=R.local, weight_mode=sgs.W_EXPLICIT, hbm_budget_gb=a.served_budget_gb,
-                   group_size=4)
+                   group_size=a.served_group_size)
     e.load_rmat(a.served_scale, a.edge_factor, a.seed, 0.57, 0.19, 0.19, wseed=a.seed)
     st0 = e.engine_stats()
     nv = int(st0["nv"])
@@ -784,6 +787,7 @@ def served_arm(a, R):
     launches = int(e.engine_stats()["kernel_launches"] - l0)
     st = e.engine_stats()
     e.close()
+    plain = served_plain(a, R, reqs) if a.served_plain else None
     ok = [c["status"] == 0 for c in res]
     # busy time: union of the steps' [start, done] intervals
     steps = sorted({(c["start_s"], c["done_s"]) for c in res})
@@ -814,7 +818,8 @@ def served_arm(a, R):
         "data": "synthetic (device R-MAT, seeded update stream, Poisson arrivals)",
         "config": {"workload": f"served loop, R-MAT scale {a.served_scale} ef {a.edge_factor} seed {a.seed}, "
                                f"HBM budget {a.served_budget_gb} GB, {a.served_seconds} s of Poisson "
-                               f"arrivals at {a.served_rate}/s, slots {a.slots}, group_size 4",
+                               f"arrivals at {a.served_rate}/s, slots {a.slots}, "
+                               f"group_size {a.served_group_size}",
                    "nv": nv, "ne_initial": int(st0["ne"]), "ne_final": int(st["ne"]),
                    "hbm_resident_fraction": st["hbm_resident_vertices"] / max(nv, 1),
                    "requests": len(reqs), "updates": n_upd, "queries": len(reqs) - n_upd,
@@ -830,8 +835,50 @@ def served_arm(a, R):
                                                   "summaries out, wall clock"},
         "gpu_launches": launches, "clocks": clk, "gen_s": round(t_gen, 2),
         "roofline": None,
+        "plain": plain,
     }
     return out
+
+
+def served_plain(a, R, reqs):
+    """The plain per-query engine on the same graph and request mix: a sample
+    of the trace's BFS and SSSP queries, each alone (group_size 1, one query
+    per edge pass) from scratch on the initial graph, plus one PageRank from
+    scratch; the mix's GTEPS weights them by the trace's composition (its
+    BFS/SSSP and PageRank counts): total edges / total device time."""
+    import sgs
+
+    e = sgs.Engine(device=R.local, weight_mode=sgs.W_EXPLICIT, hbm_budget_gb=a.served_budget_gb,
+                   group_size=1, pr_warm=0)
+    e.load_rmat(a.served_scale, a.edge_factor, a.seed, 0.57, 0.19, 0.19, wseed=a.seed)
+    lane = [r for r in reqs if r["kind"] == "query" and r["algo"] in (sgs.BFS, sgs.SSSP)]
+    n_pr = sum(1 for r in reqs if r["kind"] == "query" and r["algo"] == sgs.PR)
+    qs = lane[:a.served_plain]
+    e.remove_query(e.add_query(qs[0]["algo"], qs[0]["source"]))  # warm-up
+    edges, ms = 0, 0.0
+    for r in qs:
+        q = e.add_query(r["algo"], r["source"])
+        st = q.stats()
+        edges += st["edges_traversed"]
+        ms += st["ms"]
+        e.remove_query(q)
+    pr_e = pr_ms = 0.0
+    if n_pr:
+        q = e.add_query(sgs.PR, 0)
+        st = q.stats()
+        pr_e, pr_ms = float(st["edges_traversed"]), float(st["ms"])
+        e.remove_query(q)
+    e.close()
+    k = len(qs)
+    lane_e, lane_ms = edges / max(k, 1), ms / max(k, 1)
+    mix_e = len(lane) * lane_e + n_pr * pr_e
+    mix_ms = len(lane) * lane_ms + n_pr * pr_ms
+    return {"queries_timed": k, "bfs_sssp_gteps": round(edges / (ms * 1e6), 3) if ms > 0 else None,
+            "bfs_sssp_ms_per_query": round(lane_ms, 3),
+            "pagerank_ms": round(pr_ms, 1) if n_pr else None,
+            "gteps": round(mix_e / (mix_ms * 1e6), 3) if mix_ms > 0 else None,
+            "note": "plain engine (group_size 1, each query alone, from scratch) on the initial graph, "
+                    "weighted by the trace's %d BFS/SSSP and %d PageRank queries" % (len(lane), n_pr)}
 
 
 # ----------------------------------------------------------------- PPR adjoint arm

@@ -1346,6 +1346,10 @@ struct sgs_engine {
     DBuf<double> l1;
     unsigned long long pr_in = 0;
     float ms = 0;
+    // a snapshot was applied while the job ran: its residual was amended
+    // like any PageRank query's, and its dense frontier (block sizes of the
+    // old graph) is rebuilt before the next sweep
+    bool stale = false;
   } job;
   FrontierView job_view(uint32_t k) {
     FrontierView f;
@@ -1356,6 +1360,18 @@ struct sgs_engine {
     f.counter = (uint64_t *)(job.c.p + k);
     f.ucap = job.ucap;
     return f;
+  }
+  // The job's dense frontier over the store its sweeps read, for the current
+  // graph (buffers sized for a dense frontier of either store).
+  void job_frontier() {
+    const uint64_t max_pos = std::max<uint64_t>(slots_total, in_capslots) + 3ull * nv;
+    job.ucap = (uint32_t)std::min<uint64_t>(max_pos / UNIT + 2, 0xFFFFFFF0ull);
+    job.f.ustart.ensure(job.ucap);
+    CK(cudaMemsetAsync(job.c.p, 0, sizeof(unsigned long long) * 2, s));
+    const GraphView gi = job.pull ? in_view() : view();
+    { ++n_launch; k_dense_frontier<<<grid_elem(nv), 256, 0, s>>>(gi, job_view(0)); }
+    CK(cudaMemcpyAsync(&job.pr_in, job.c.p, sizeof(job.pr_in), cudaMemcpyDeviceToHost, s));
+    sync();
   }
   int pr_job_start() {
     if (job.q) fail(SGS_ERR_STATE, "a PageRank job is already running");
@@ -1368,6 +1384,7 @@ struct sgs_engine {
     job.f.ustart.ensure(job.ucap);
     job.c.ensure(3);
     job.l1.ensure(cfg.max_rounds + 2);
+    job.stale = false;
     job.pull = (cfg.pull & 1u) && ensure_in(job_view(0), job_view(1));
     auto q = std::make_unique<Query>();
     q->id = next_qid++;
@@ -1396,6 +1413,10 @@ struct sgs_engine {
   // at the round limit; its query then holds the result and its stats).
   bool pr_job_advance(uint32_t rounds) {
     if (!job.q) fail(SGS_ERR_STATE, "no PageRank job");
+    if (job.stale) {
+      job_frontier();
+      job.stale = false;
+    }
     Query &q = *job.q;
     const uint32_t lim = std::min(rounds, cfg.max_rounds - job.r);
     bool conv = false;
@@ -2213,6 +2234,10 @@ struct sgs_engine {
       for (auto &qp : queries) {
         Query &q = *qp;
         if (q.algo != SGS_PR) continue;
+        if (&q == job.q) {  // a served PageRank job converges at its own pace
+          job.stale = true;
+          continue;
+        }
         CK(cudaEventRecord(ev_q.a, s));
         CK(cudaMemsetAsync(b_stat.p + 4, 0, sizeof(unsigned long long), s));
         bool conv = false;

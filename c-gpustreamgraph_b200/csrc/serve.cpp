@@ -13,15 +13,20 @@
 //   * a query leaves as soon as no entry of the frontier carries its lane:
 //     its result is read back (summary, and optionally its value/parent
 //     vectors) and its lane freed for the next arrival;
-//   * an update batch is one snapshot, applied when the flight is empty and
-//     no PageRank job runs, so every query sees exactly the updates that
+//   * an update batch is one snapshot, applied when no lane query is in
+//     flight, so every BFS/SSSP/CC query sees exactly the updates that
 //     arrived before it (its "version"); queries behind an update wait for it;
 //   * PageRank has no lanes (and no source): consecutive PR queries share one
 //     computation, a job that starts as soon as they reach the head of the
 //     queue and runs a few sweeps per loop iteration between the flight's
 //     steps, so lane queries behind it keep being admitted and served (the
 //     job has its own frontier buffers; a PageRank start continues from the
-//     vector of the previous one, see sgs_config.pr_warm);
+//     vector of the previous one, see sgs_config.pr_warm).  Updates do not
+//     wait for it: a snapshot amends the job's residual for the out-lists it
+//     changes (the cancel/compensate of every PageRank query) and the job
+//     continues on the new graph, so its result reflects every update applied
+//     before it finished -- at least those that arrived before its requests --
+//     and its completions report that version;
 //
 // With `realtime` the loop waits for arrival times on the wall clock, and
 // latency = done_s - arrival_s includes queueing; without it every request
@@ -206,6 +211,7 @@ SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n, uint32_
         for (uint32_t k : pr_batch) {
           sgs_completion &c = out[k];
           c.status = rc;
+          c.version = version;  // the snapshots applied while it ran included
           if (rc == SGS_OK) finish(e, pr_qid, req[k], c);
         }
         sgs_query_remove(e, pr_qid);
@@ -240,10 +246,9 @@ SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n, uint32_
         ++done;
       }
     }
-    if (worked) continue;
-
-    // 4. nothing runs: an update at the head
-    if (!pending.empty() && req[pending.front()].kind == SGS_REQ_UPDATE) {
+    // 4. an update at the head, once no lane query is in flight (a PageRank
+    // job may be running: the snapshot amends it)
+    if (inflight.empty() && !pending.empty() && req[pending.front()].kind == SGS_REQ_UPDATE) {
       const uint32_t head = pending.front();
       const sgs_request &r = req[head];
       pending.pop_front();
@@ -262,6 +267,7 @@ SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n, uint32_
       ++done;
       continue;
     }
+    if (worked) continue;
 
     // 5. idle until the next arrival
     if (pending.empty() && next < n) {

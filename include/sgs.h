@@ -463,9 +463,12 @@ SGS_API void sgs_set_last_error(const char *msg);
  * their edge passes; a query leaves as soon as no frontier entry carries its
  * lane (summary, and the value / parent vectors when buffers are given, read
  * back) and frees the lane.  An update batch is one snapshot, applied when
- * the flight is empty, so every query sees exactly the updates that arrived
- * before it (its `version`).  PageRank queries (no lanes, no source) share
- * one computation per run of consecutive PR requests.  With `realtime` the
+ * the flight is empty, so every BFS/SSSP/CC query sees exactly the updates
+ * that arrived before it (its `version`).  PageRank queries (no lanes, no
+ * source) share one computation per run of consecutive PR requests; updates
+ * do not wait for it: a snapshot amends its residual and it continues on the
+ * new graph, so a PageRank result reflects at least the updates that arrived
+ * before its requests, and its `version` says how many.  With `realtime` the
  * loop waits for arrival times on the wall clock (latency = done_s -
  * arrival_s, queueing included); otherwise every request is taken at once, in
  * arrival order (a closed loop: latency = done_s).  out[i] describes req[i];
