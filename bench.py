@@ -64,6 +64,8 @@ def parse():
                     help="reference arm: traversal time budget over the timed snapshots")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations' sub-records after the headline")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="skip sgs_autotune (by default it picks the relaxation map's CTAs per SM "
                          "and the launch mode by timing a probe, before the timed region)")
@@ -681,7 +683,14 @@ def batched_arm(a, R):
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "peak_source": peak_src, "traffic": None, "launches": kd["launches"],
             "avg_launch_ms": round(kd["ms"] / max(kd["launches"], 1), 4),
-            "alg_bytes_per_launch": kd["bytes_alg"] / max(kd["launches"], 1)}
+            "alg_bytes_per_launch": kd["bytes_alg"] / max(kd["launches"], 1),
+            # the bytes count the (lane, edge) pairs the kernel evaluates: a
+            # repair's first round walks every reached vertex's out-edges but
+            # evaluates only the lanes reset at each destination, so its time
+            # goes to the walk (4-B ids, 8-B reset-lane probes of the L2), which
+            # this model counts at 4 B per slot
+            "slots_walked_per_s": round(kd["slots"] / (kd["ms"] * 1e-3), 1) if kd["ms"] > 0 else None,
+            "pairs_evaluated": int(max(0.0, (kd["bytes_alg"] - 4.0 * kd["slots"] - 20.0 * kd["entries"]) / 8.0))}
     out = {
         "metric": BATCHED_METRIC.format(nb=a.batched_bfs, ns=a.batched_sssp, scale=a.batched_scale,
                                         upd=a.batched_updates),
@@ -779,13 +788,29 @@ def served_arm(a, R):
     R.barrier()
     torch.cuda.synchronize()
     l0 = e.engine_stats()["kernel_launches"]
+    e.kernel_timing(True)
     clocks.start()
     w0 = time.perf_counter()
     res = e.serve(reqs, slots=a.slots, realtime=True)
     wall = time.perf_counter() - w0
     clk = clocks.stop()
+    kst = e.kernel_stats()
+    e.kernel_timing(False)
     launches = int(e.engine_stats()["kernel_launches"] - l0)
     st = e.engine_stats()
+    # roofline of the kernel class with the most timed device time (the
+    # flight's round launches are not timed per launch; updates' repairs and
+    # the PageRank job's sweeps are)
+    roof = None
+    timed = {k: v for k, v in kst.items() if v["ms"] > 0}
+    if timed:
+        dom = max(timed, key=lambda k: timed[k]["ms"])
+        kd = timed[dom]
+        peak, src = measured_peak_hbm()
+        ach = kd["bytes_alg"] / (kd["ms"] * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(ach / peak, 4), "peak_source": src, "traffic": None,
+                "launches": kd["launches"], "avg_launch_ms": round(kd["ms"] / max(kd["launches"], 1), 4)}
     e.close()
     plain = served_plain(a, R, reqs) if a.served_plain else None
     ok = [c["status"] == 0 for c in res]
@@ -834,7 +859,7 @@ def served_arm(a, R):
                 "d2h_bytes_per_step": 32, "note": "the served loop is end to end: host batches in, "
                                                   "summaries out, wall clock"},
         "gpu_launches": launches, "clocks": clk, "gen_s": round(t_gen, 2),
-        "roofline": None,
+        "roofline": roof,
         "plain": plain,
     }
     return out
@@ -1253,6 +1278,11 @@ def pagerank_arm(a, R):
                     "gteps": round(st0["edges_traversed"] / (st0["ms"] * 1e6), 3) if st0["ms"] else None},
          "sweep": {"launches": kd["launches"], "ms": round(kd["ms"], 3), "achieved_gbs": round(ach, 1),
                    "frac_of_measured_hbm": round(ach / peak, 4), "peak_source": src},
+         "roofline": {"bound": "hbm", "kernel": sweep, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                      "frac": round(ach / peak, 4), "peak_source": src, "traffic": None,
+                      "launches": kd["launches"],
+                      "note": "graph L2-resident at this scale: the HBM fraction is not a bound"
+                              if a.pr_scale <= 18 else None},
          "clocks": clk})
 
 
@@ -1300,6 +1330,63 @@ def bfs_arm(a, R):
          "in_store_bytes": int(est["in_store_bytes"]), "clocks": clk})
 
 
+def _condense(out):
+    """The figures of a workload's line kept in the headline's sub-record."""
+    keep = ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "roofline", "clocks", "gpu_launches",
+            "latency", "plain", "utilisation", "lanes_in_flight_at_admission", "static", "sweep",
+            "selfcheck_incremental_eq_static", "static_start", "failed", "grad_check")
+    rec = {k: out[k] for k in keep if k in out}
+    cfg = out.get("config") or {}
+    rec["workload"] = cfg.get("workload")
+    e2e = out.get("e2e")
+    if isinstance(e2e, dict):
+        rec["e2e"] = {k: e2e[k] for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step",
+                                          "ms_per_step") if k in e2e}
+    eng = out.get("engine") or {}
+    for k in ("hbm_resident_fraction", "arena_bytes_host", "repair"):
+        if k in eng:
+            rec[k] = eng[k]
+    if isinstance(rec.get("roofline"), dict):
+        rec["roofline"] = {k: v for k, v in rec["roofline"].items() if not isinstance(v, (dict, list))
+                           or k == "largest_launch"}
+    return rec
+
+
+def config_records(a, R):
+    """The benchmark's other configurations, each run after the headline in
+    its own engine (with its own clocks and roofline) and kept as a
+    sub-record of the one JSON line: the first (incremental PageRank, R-MAT
+    s16, 2 snapshots of 10k inserts + 10k deletes), the headline's
+    out-of-HBM regime (0.5 GB budget: most blocks host-resident) and its
+    work-efficient pull repair, the batched third (256 BFS + 256 SSSP at
+    s22), the fourth (PPR adjoint at s22, K = 64) and the served fifth (s26,
+    16 GB budget, Poisson arrivals), each at its own default sizes."""
+    import copy
+
+    recs = {}
+
+    def sub(name, fn, **kw):
+        b = copy.copy(a)
+        for k, v in kw.items():
+            setattr(b, k, v)
+        t = time.time()
+        try:
+            rec = _condense(fn(b, R))
+        except Exception as ex:  # a failing sub-workload is reported, not fatal
+            rec = {"error": repr(ex)[:400]}
+        rec["wall_s"] = round(time.time() - t, 1)
+        recs[name] = rec
+
+    base = dict(no_e2e=True, no_cpu=True, autotune=False)
+    sub("pagerank_cfg1", pagerank_arm, steps=2, warmup=1, pr_scale=16, pr_updates=20_000, workload="pagerank")
+    sub("out_of_hbm_cfg2", engine_arm, budget_gb=0.5, steps=5, warmup=2, **base)
+    sub("repair1_cfg2", engine_arm, repair=1, steps=10, warmup=3, **base)
+    sub("batched_cfg3", batched_arm, steps=4, warmup=1, no_e2e=True, workload="batched")
+    sub("ppr_cfg4", ppr_arm, steps=2, warmup=1, no_e2e=True, no_cpu=True, workload="ppr")
+    sub("served_cfg5", served_arm, served_seconds=15.0, workload="served")
+    return recs
+
+
 def main():
     a = parse()
     R = Ranks()
@@ -1328,6 +1415,8 @@ def main():
             out = bfs_arm(a, R)
         else:
             out = engine_arm(a, R)
+            if R.world == 1 and not a.no_configs:
+                out["configs"] = config_records(a, R)
         if R.rank == 0 and out is not None:
             print(json.dumps(out), flush=True)
     finally:

@@ -63,7 +63,11 @@ double since(clk::time_point t0) {
 }
 
 constexpr uint32_t kRoundsPerStep = 4;  // rounds between two admission points
-constexpr uint32_t kPrRoundsPerStep = 8;  // PageRank sweeps per loop iteration
+// PageRank sweeps per loop iteration: a long job yields to the lane queries
+// (and to the updates waiting for them to drain) while any are in flight,
+// and runs in longer steps when it has the GPU to itself
+constexpr uint32_t kPrRoundsPerStep = 8;
+constexpr uint32_t kPrRoundsPerStepShared = 1;
 
 // Result of a finished query into its completion record.
 void finish(sgs_engine *e, int qid, const sgs_request &r, sgs_completion &c) {
@@ -206,7 +210,8 @@ SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n, uint32_
     if (pr_qid) {
       worked = true;
       int fin_pr = 0;
-      const int rc = sgs::pr_job_advance(e, kPrRoundsPerStep, &fin_pr);
+      const int rc =
+          sgs::pr_job_advance(e, inflight.empty() ? kPrRoundsPerStep : kPrRoundsPerStepShared, &fin_pr);
       if (rc != SGS_OK || fin_pr) {
         for (uint32_t k : pr_batch) {
           sgs_completion &c = out[k];
