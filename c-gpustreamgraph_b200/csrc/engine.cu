@@ -1243,7 +1243,7 @@ struct sgs_engine {
         CK(cudaMemcpyAsync(&r0s, rstat.p, sizeof(r0s), cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(&h0, hstat.p, sizeof(h0), cudaMemcpyDeviceToHost, s));
         sync();
-        account(SGS_K_GROUP, c0, r0s, anyw ? 8.0 : 4.0, 8.0, kev[0], kev[1], h0);
+        account(SGS_K_GROUP_SWEEP, c0, r0s, anyw ? 8.0 : 4.0, 8.0, kev[0], kev[1], h0);
       }
       if (round0) nvtxRangePop();
       return run_group_persistent(GroupRelaxOp<GMAX>{g, G.st.p, G.val.p, nullptr, nullptr, G.algo(), anyw}, 1,

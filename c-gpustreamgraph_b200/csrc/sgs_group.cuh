@@ -79,9 +79,23 @@ __device__ __forceinline__ void clear_prev_masks(const uint32_t *vtx, const unsi
 // candidate below it lowers the mirror first and, if that strictly lowered
 // it, the packed (value,parent) word (relax_mirror_packed: equal candidates
 // never swap a parent).
+//
+// Per entry the payload holds each lane's candidate base -- the source's
+// value, plus 1 in BFS lanes -- and INF32 in the lanes that do not push, so
+// the per-edge test is compare-only: candidate = base (+ the weight in SSSP
+// lanes, saturating at INF32) against the destination's mirror.  Most edges
+// of a sweep improve nothing; only the quads with some candidate below the
+// mirror take the atomic path.
+template <int S>
+struct RPay {
+  uint64_t off;
+  uint32_t mask;     // lanes that push from this vertex
+  uint32_t base[S];  // candidate base per lane (INF32: the lane does not push)
+};
+
 template <int S>
 struct GroupRelaxOp {
-  using Payload = GPay<S>;
+  using Payload = RPay<S>;
   GraphView g;
   unsigned long long *st;
   uint32_t *val;
@@ -93,12 +107,17 @@ struct GroupRelaxOp {
     Payload p;
     p.off = g.off[v];
     p.mask = __ldcg(&m_in[v]);
-    load_vals<S>(val, v, p.val);
+    uint32_t x[S];
+    load_vals<S>(val, v, x);
     // a BFS/SSSP lane that has not reached v pushes nothing: drop it here,
-    // once per entry, instead of testing it for every edge
+    // once per entry, instead of testing it for every edge.  A reached BFS
+    // value is below INF32, so value + 1 does not wrap.
 #pragma unroll
-    for (int q = 0; q < S; ++q)
-      if (p.val[q] == INF32 && !(algo.cc >> q & 1u)) p.mask &= ~(1u << q);
+    for (int q = 0; q < S; ++q) {
+      const bool on = (p.mask >> q & 1u) && (x[q] != INF32 || (algo.cc >> q & 1u));
+      if (!on) p.mask &= ~(1u << q);
+      p.base[q] = on ? x[q] + (algo.inc >> q & 1u) : INF32;
+    }
     return p;
   }
   // The quad's ids (and weights), loaded one step ahead by group_map.
@@ -120,8 +139,18 @@ struct GroupRelaxOp {
     }
     return q;
   }
+  // candidate of lane q for an edge of weight w: base + w in SSSP lanes,
+  // saturating (min(base, INF32 - w) + w), else base; INF32 is never below
+  // a mirror value
+  __device__ __forceinline__ uint32_t cand_of(uint32_t base, uint32_t w, int q) const {
+    const uint32_t wq = w & (0u - (algo.w >> q & 1u));
+    return min(base, ~wq) + wq;
+  }
+  __device__ __forceinline__ uint32_t weight_of(const uint4 &ws, int k, uint32_t u, uint32_t d) const {
+    return g.wmode == W_EXPLICIT ? quad_at(ws, k) : g.wmode == W_SYNTH ? (u + d) % 128u + 1u : 1u;
+  }
   // Returns a 4-bit mask of destinations to append; dst[] holds them.
-  __device__ __forceinline__ uint32_t visit4(uint32_t u, const Payload &p, uint32_t j0, uint32_t len,
+  __device__ __forceinline__ uint32_t visit4(uint32_t u, const Payload &pr, uint32_t j0, uint32_t len,
                                              const Quad &qd, uint32_t (&dst)[4]) const {
     const uint4 ids = qd.ids;
     const uint4 ws = qd.ws;
@@ -135,26 +164,30 @@ struct GroupRelaxOp {
 #pragma unroll
     for (int k = 0; k < 4; ++k)
       if (okm >> k & 1u) load_vals<S>(val, dst[k], cur[k]);
-    uint32_t app = 0;
+    // compare-only pass: bit 4k+q = lane q's candidate is below the mirror
+    // of destination k
+    uint32_t lt = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       if (!(okm >> k & 1u)) continue;
-      // this edge's weight, for the lanes that use one
-      const uint32_t w = g.wmode == W_EXPLICIT ? quad_at(ws, k)
-                         : g.wmode == W_SYNTH  ? (u + dst[k]) % 128u + 1u
-                                               : 1u;
+      const uint32_t w = weight_of(ws, k, u, dst[k]);
+#pragma unroll
+      for (int q = 0; q < S; ++q)
+        lt |= (cand_of(pr.base[q], w, q) < cur[k][q] ? 1u : 0u) << (4 * k + q);
+    }
+    if (!lt) return 0;
+    uint32_t app = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t lk = lt >> (4 * k) & 0xFu;
+      if (!lk) continue;
+      const uint32_t w = weight_of(ws, k, u, dst[k]);
       uint32_t bits = 0;
 #pragma unroll
       for (int q = 0; q < S; ++q) {
-        if (!(p.mask >> q & 1u)) continue;
-        // candidate = source value + weight (SSSP) / 1 (BFS) / 0 (CC); a sum
-        // at or above INF is never below the destination's value (<= INF)
-        const uint32_t step = (algo.w >> q & 1u) ? w : (algo.inc >> q & 1u);
-        const uint64_t nd = (uint64_t)p.val[q] + step;
-        if (nd >= (uint64_t)cur[k][q]) continue;
-        const uint32_t cand = (uint32_t)nd;
+        if (!(lk >> q & 1u)) continue;
         const uint64_t idx = (uint64_t)dst[k] * S + q;
-        if (relax_mirror_packed(&val[idx], &st[idx], cand, u)) bits |= 1u << q;
+        if (relax_mirror_packed(&val[idx], &st[idx], cand_of(pr.base[q], w, q), u)) bits |= 1u << q;
       }
       if (bits && g.slots[dst[k]] && atomicOr(&m_out[dst[k]], bits) == 0u) app |= 1u << k;
     }

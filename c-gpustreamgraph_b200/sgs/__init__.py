@@ -54,9 +54,10 @@ EXPORTS = [
     "sgs_stage_batch", "sgs_apply_staged", "sgs_query_summaries",
 ]
 
-K_GROUP, K_GROUP_INVAL, K_PR_PUSH, K_WIDE, K_WIDE_INVAL, K_PR_PULL = range(6)
+K_GROUP, K_GROUP_INVAL, K_PR_PUSH, K_WIDE, K_WIDE_INVAL, K_PR_PULL, K_GROUP_SWEEP = range(7)
 KERNEL_KINDS = {"group_relax": K_GROUP, "group_invalidate": K_GROUP_INVAL, "pr_push": K_PR_PUSH,
-                "wide_relax": K_WIDE, "wide_invalidate": K_WIDE_INVAL, "pr_pull": K_PR_PULL}
+                "wide_relax": K_WIDE, "wide_invalidate": K_WIDE_INVAL, "pr_pull": K_PR_PULL,
+                "group_sweep": K_GROUP_SWEEP}
 
 
 class SgsError(RuntimeError):

@@ -206,13 +206,18 @@ typedef struct sgs_engine_stats {
  * a lane needs stored weights) read once for all lanes of a group, per
  * (query, edge) relaxation 8 B of state read+write (PageRank: 16 B FP64
  * residual), plus 20 B per active vertex. */
-#define SGS_K_GROUP 0        /* BFS/SSSP/CC relaxation of a query group   */
+#define SGS_K_GROUP 0        /* BFS/SSSP/CC relaxation of a query group
+                                (its rounds after SGS_K_GROUP_SWEEP's)    */
 #define SGS_K_GROUP_INVAL 1  /* parent-tree invalidation of a query group */
 #define SGS_K_PR_PUSH 2      /* PageRank residual push                    */
 #define SGS_K_WIDE 3         /* relaxation of a wide query group          */
 #define SGS_K_WIDE_INVAL 4   /* parent-tree invalidation of a wide group  */
 #define SGS_K_PR_PULL 5      /* PageRank sweep as a pull over in-edges    */
-#define SGS_K_COUNT 6
+#define SGS_K_GROUP_SWEEP 6  /* the first round of a narrow group's phase
+                                launched alone on the full grid: after a
+                                snapshot's deletions, the re-push from every
+                                reached vertex (persistent bit 2)         */
+#define SGS_K_COUNT 7
 typedef struct sgs_kernel_stats {
   uint64_t launches;
   uint64_t slots;      /* positions walked (edges incl. tombstones)          */
