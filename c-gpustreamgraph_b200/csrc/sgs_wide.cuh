@@ -218,65 +218,14 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
       }
       const uint64_t lo = max(E0, s_eb[0]);
       const uint64_t hi = min(E1, s_eb[GC]);
-      // Windows of 32 slots, lane t on slot t (one coalesced id read), dealt
-      // round-robin to the warps so that they share the chunk's heavy and
-      // light entries evenly.  A window's first owner s0 comes from one
-      // warp-uniform search; the others need none (as in group_map): lane j
-      // holds the start of entry s0 + j, every start inside the window sets
-      // bit (start - window) of a warp-wide OR, and a slot's owner is s0 plus
-      // the set bits at or below it (every entry has at least one slot).
-      for (uint64_t wb = lo + (uint64_t)warp * 32; wb < hi; wb += (uint64_t)NW * 32) {
-        int le;
-        {
-          int a = 0, b = GC - 1;
-          while (a < b) {
-            const int m = (a + b + 1) >> 1;
-            if (s_eb[m] <= wb) a = m;
-            else b = m - 1;
-          }
-          const int s0 = a;
-          const int j = s0 + t;
-          const uint64_t bj = j <= GC ? s_eb[j] : ~0ull;
-          const uint32_t bit = (t >= 1 && bj < wb + 32) ? 1u << (uint32_t)(bj - wb) : 0u;
-          const uint32_t m = __reduce_or_sync(0xFFFFFFFFu, bit);
-          le = s0 + __popc(m & (0xFFFFFFFFu >> (31 - t)));
-        }
-        const uint64_t e = wb + t;
-        bool ok = false;
-        uint32_t v = 0, w = 1;
-        unsigned long long rl = ~0ull;  // the lanes this edge may relax
-        if (e < hi) {
-          const int l = le;
-          const uint32_t j = (uint32_t)(e - s_eb[l]);
-          if (j < s_len[l]) {
-            // slot position in its arena: HBM, cache line or host
-            uint64_t x = s_off[l] + j;
-            int tier = 0;
-            if (H && (x & HOST_BIT)) {
-              x &= OFF_MASK;
-              const uint32_t m = cache_line(g, x);
-              tier = m != NO_LINE ? 1 : 2;
-              if (m != NO_LINE) x = ((uint64_t)m << CLINE_SHIFT) + (x & (CLINE - 1));
-              miss_acc += tier == 2;
-            }
-            v = __ldcg((tier == 0 ? g.adj_d : tier == 1 ? g.adj_c : g.adj_h) + x);
-            ok = v != SGS_TOMB;
-            if constexpr (Op::kRestrict) {
-              if (ok) rl = __ldcg(&op.only[v]);
-              ok = ok && rl != 0ull;
-            }
-            if (ok && op.algo.sssp && s_mask[l] & op.algo.sssp)
-              w = g.wmode == W_EXPLICIT ? __ldcg((tier == 0 ? g.wgt_d : tier == 1 ? g.wgt_c : g.wgt_h) + x)
-                  : g.wmode == W_SYNTH  ? (s_vtx[l] + v) % 128u + 1u
-                                        : 1u;
-          }
-        }
-        // The window's work: (edge, active lane) pairs.  Dense windows (many
-        // lanes per edge) take the per-edge path, every thread on two lanes of
-        // each edge; sparse ones -- the common case after the first rounds --
-        // spread the pairs over the warp's threads, one pair per thread per
-        // step, so no thread idles on an inactive lane.
-        const unsigned long long mk = ok ? s_mask[le] & rl : 0ull;
+      // The work of 32 slots, one per thread: the slot (ok: it holds an edge)
+      // of entry le leads to v with weight w, and mk holds the lanes to
+      // evaluate on it -- (edge, active lane) pairs.  Dense windows (many
+      // lanes per edge) take the per-edge path, every thread on two lanes of
+      // each edge; sparse ones -- the common case after the first rounds --
+      // spread the pairs over the warp's threads, one pair per thread per
+      // step, so no thread idles on an inactive lane.
+      auto pairs = [&](bool ok, uint32_t v, uint32_t w, int le, unsigned long long mk) {
         const uint32_t c = (uint32_t)__popcll(mk);
         uint32_t incl = c;
 #pragma unroll
@@ -306,7 +255,11 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
               vi[q] = __shfl_sync(0xFFFFFFFFu, v, src);
               wi[q] = __shfl_sync(0xFFFFFFFFu, w, src);
               uu[q] = s_vtx[li[q]];
-              const unsigned long long mkq = __shfl_sync(0xFFFFFFFFu, mk, src);
+              // no edge left for this step (ii < 0): evaluate nothing.  (A
+              // repeat of edge 0 here could succeed with no thread to append
+              // its destination, and the improvement would never be pushed.)
+              unsigned long long mkq = __shfl_sync(0xFFFFFFFFu, mk, src);
+              if (ii[q] < 0) mkq = 0ull;
               a0[q] = mkq >> t & 1ull;
               a1[q] = mkq >> (t + 32) & 1ull;
             }
@@ -319,11 +272,13 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
               vu0[q] = INF32;
               vu1[q] = INF32;
               if (Op::kNeedsSourceValues) {
-                // a stale (higher) source value is harmless: a source that
-                // improves during this round is appended and pushes again
+                // read through L2 (not the non-coherent path: this kernel
+                // writes the rows, and a persistent launch runs every round
+                // in one kernel).  A value that drops after this read is
+                // harmless: its vertex is appended and pushes again.
                 const uint32_t *row = op.val + (uint64_t)uu[q] * WLANES;
-                if (a0[q]) vu0[q] = __ldg(row + t);
-                if (a1[q]) vu1[q] = __ldg(row + t + 32);
+                if (a0[q]) vu0[q] = __ldcg(row + t);
+                if (a1[q]) vu1[q] = __ldcg(row + t + 32);
               }
             }
 #pragma unroll
@@ -366,7 +321,7 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
               const int q = r < p0 ? (int)__fns(m0, 0, (int)r + 1) : 32 + (int)__fns(m1, 0, (int)(r - p0) + 1);
               const uint32_t u = s_vtx[lej];
               uint32_t vu = INF32;
-              if (Op::kNeedsSourceValues) vu = __ldg(op.val + (uint64_t)u * WLANES + q);
+              if (Op::kNeedsSourceValues) vu = __ldcg(op.val + (uint64_t)u * WLANES + q);
               ++evald;
               if (op.lane(u, vj, wj, vu, q, op.algo.sssp >> q & 1ull, op.algo.cc >> q & 1ull)) {
                 atomicAdd(&s_chg[q], 1ull);
@@ -376,6 +331,152 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
             }
             frontier_append(out, want, vj, want ? g.slots[vj] : 0u);
           }
+        }
+      };
+      if constexpr (Op::kRestrict && !H) {
+        // Restricted round (the repair's first), every block in HBM: almost
+        // no edge leads into a vertex reset in one of its source's lanes, so
+        // the round is a walk of ids and reset-lane probes.  It walks like
+        // group_map: each warp its own contiguous share of the chunk, 32
+        // quads (128 slots) per window, lane i on quad i (coalesced 512-B id
+        // reads), owners from the OR of entry starts, the next window's ids
+        // loaded before this window's probes; the four probes of a quad are
+        // issued together.  Only a slot whose probe meets a lane of its
+        // source takes the pair path above, one slot of the quad at a time.
+        const uint64_t nq = hi > lo ? (hi - lo) >> 2 : 0;
+        uint64_t wq = (lo >> 2) + nq * (uint64_t)warp / NW;
+        const uint64_t wqe = (lo >> 2) + nq * (uint64_t)(warp + 1) / NW;
+        if (wq < wqe) {
+          int s0;
+          {  // owner of the share's first quad
+            const uint64_t e = wq << 2;
+            int a = 0, b = GC - 1;
+            while (a < b) {
+              const int m = (a + b + 1) >> 1;
+              if (s_eb[m] <= e) a = m;
+              else b = m - 1;
+            }
+            s0 = a;
+          }
+          // owner and first slot of this thread's quad in the window at
+          // quad q (consecutive windows, all threads together); true when the
+          // quad holds slots.  Leaves s0 at the next window's first owner.
+          auto window = [&](uint64_t q, int &own, uint32_t &j0) -> bool {
+            const uint64_t p0 = q << 2, pe = p0 + 4 * 32;
+            const int j = s0 + t;
+            const uint64_t bj = j <= GC ? s_eb[j] : ~0ull;
+            const uint32_t bit = (t >= 1 && bj < pe) ? 1u << (uint32_t)((bj - p0) >> 2) : 0u;
+            const uint32_t m = __reduce_or_sync(0xFFFFFFFFu, bit);
+            own = s0 + __popc(m & (0xFFFFFFFFu >> (31 - t)));
+            int ns = s0 + __popc(m);
+            if (ns < GC && s_eb[ns + 1] <= pe) ++ns;  // an entry starting exactly at pe
+            s0 = ns;
+            j0 = (uint32_t)(p0 + 4 * (uint32_t)t - s_eb[own]);
+            return q + (uint64_t)t < wqe && j0 < s_len[own];
+          };
+          const uint4 none = make_uint4(SGS_TOMB, SGS_TOMB, SGS_TOMB, SGS_TOMB);
+          int oc = 0;
+          uint32_t jc = 0;
+          bool hc = window(wq, oc, jc);
+          uint4 ic = hc ? ld_quad_stream(g.adj_d + s_off[oc] + jc) : none;
+          for (; wq < wqe; wq += 32) {
+            int on = 0;
+            uint32_t jn = 0;
+            bool hn = false;
+            uint4 in4 = none;
+            if (wq + 32 < wqe) {
+              hn = window(wq + 32, on, jn);
+              if (hn) in4 = ld_quad_stream(g.adj_d + s_off[on] + jn);
+            }
+            const unsigned long long sm = hc ? s_mask[oc] : 0ull;
+            const uint32_t ln = hc ? s_len[oc] : 0u;
+            uint32_t d[4];
+            unsigned long long mk[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              d[k] = quad_at(ic, k);
+              const bool okk = jc + k < ln && d[k] != SGS_TOMB;
+              mk[k] = okk ? __ldcg(&op.only[d[k]]) : 0ull;
+            }
+            uint32_t hitm = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              mk[k] &= sm;
+              hitm |= (mk[k] != 0ull ? 1u : 0u) << k;
+            }
+            const uint32_t wh = __reduce_or_sync(0xFFFFFFFFu, hitm);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              if (!(wh >> k & 1u)) continue;
+              uint32_t w = 1;
+              if (mk[k] & op.algo.sssp)
+                w = g.wmode == W_EXPLICIT ? __ldcg(g.wgt_d + s_off[oc] + jc + k)
+                    : g.wmode == W_SYNTH  ? (s_vtx[oc] + d[k]) % 128u + 1u
+                                          : 1u;
+              pairs(mk[k] != 0ull, d[k], w, oc, mk[k]);
+            }
+            oc = on;
+            jc = jn;
+            ic = in4;
+            hc = hn;
+          }
+        }
+      } else {
+        // Windows of 32 slots, lane t on slot t (one coalesced id read), dealt
+        // round-robin to the warps so that they share the chunk's heavy and
+        // light entries evenly.  A window's first owner s0 comes from one
+        // warp-uniform search; the others need none (as in group_map): lane j
+        // holds the start of entry s0 + j, every start inside the window sets
+        // bit (start - window) of a warp-wide OR, and a slot's owner is s0 plus
+        // the set bits at or below it (every entry has at least one slot).
+        for (uint64_t wb = lo + (uint64_t)warp * 32; wb < hi; wb += (uint64_t)NW * 32) {
+          int le;
+          {
+            int a = 0, b = GC - 1;
+            while (a < b) {
+              const int m = (a + b + 1) >> 1;
+              if (s_eb[m] <= wb) a = m;
+              else b = m - 1;
+            }
+            const int s0 = a;
+            const int j = s0 + t;
+            const uint64_t bj = j <= GC ? s_eb[j] : ~0ull;
+            const uint32_t bit = (t >= 1 && bj < wb + 32) ? 1u << (uint32_t)(bj - wb) : 0u;
+            const uint32_t m = __reduce_or_sync(0xFFFFFFFFu, bit);
+            le = s0 + __popc(m & (0xFFFFFFFFu >> (31 - t)));
+          }
+          const uint64_t e = wb + t;
+          bool ok = false;
+          uint32_t v = 0, w = 1;
+          unsigned long long rl = ~0ull;  // the lanes this edge may relax
+          if (e < hi) {
+            const int l = le;
+            const uint32_t j = (uint32_t)(e - s_eb[l]);
+            if (j < s_len[l]) {
+              // slot position in its arena: HBM, cache line or host
+              uint64_t x = s_off[l] + j;
+              int tier = 0;
+              if (H && (x & HOST_BIT)) {
+                x &= OFF_MASK;
+                const uint32_t m = cache_line(g, x);
+                tier = m != NO_LINE ? 1 : 2;
+                if (m != NO_LINE) x = ((uint64_t)m << CLINE_SHIFT) + (x & (CLINE - 1));
+                miss_acc += tier == 2;
+              }
+              v = __ldcg((tier == 0 ? g.adj_d : tier == 1 ? g.adj_c : g.adj_h) + x);
+              ok = v != SGS_TOMB;
+              if constexpr (Op::kRestrict) {
+                if (ok) rl = __ldcg(&op.only[v]);
+                ok = ok && rl != 0ull;
+              }
+              if (ok && op.algo.sssp && s_mask[l] & op.algo.sssp)
+                w = g.wmode == W_EXPLICIT ? __ldcg((tier == 0 ? g.wgt_d : tier == 1 ? g.wgt_c : g.wgt_h) + x)
+                    : g.wmode == W_SYNTH  ? (s_vtx[l] + v) % 128u + 1u
+                                          : 1u;
+            }
+          }
+          const unsigned long long mk = ok ? s_mask[le] & rl : 0ull;
+          pairs(ok, v, w, le, mk);
         }
       }
       if (s_eb[GC] >= E1 || s + GC >= n) break;

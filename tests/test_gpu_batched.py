@@ -189,3 +189,19 @@ def test_autotune_picks_a_setting_and_keeps_results(gs):
         m.apply(i_s, i_d, iw, d_s, d_d)
         for q in qs:
             check_query(q, m, sgs.W_EXPLICIT)
+
+
+def test_wide_static_start_is_repeatable():
+    """The same 64-lane start (28 BFS, 30 SSSP, 6 CC lanes, so most windows
+    take the per-edge path) converges to the oracle's values every time: a
+    relaxation that succeeds must always leave its destination in the next
+    frontier, whatever the order in which the warps meet the edges."""
+    nv, row, col = O.rmat_csr(12, 16, 5)
+    w = O.weights(nv, row, col, 2, 0)
+    specs = _specs(nv, 28, 30, 6, 64)
+    m = Mirror(nv, row, col, w)
+    for _ in range(16):
+        with sgs.Engine(group_size=64) as e:
+            e.load_csr(nv, row, col, w)
+            for q in e.add_queries(specs):
+                check_query(q, m, sgs.W_EXPLICIT)
