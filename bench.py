@@ -86,7 +86,11 @@ def parse():
     ap.add_argument("--served-rate", type=float, default=12.0, help="requests per second (Poisson)")
     ap.add_argument("--served-budget-gb", type=float, default=16.0)
     ap.add_argument("--slots", type=int, default=64)
-    ap.add_argument("--served-group-size", type=int, default=64)
+    ap.add_argument("--served-group-size", type=int, default=4,
+                    help="lanes of the served flight: 1-4 a narrow group (16-B state rows), 5-64 a wide one")
+    ap.add_argument("--serve-restarts", type=int, default=2,
+                    help="served loop: times an update may preempt (restart) one query in flight; "
+                         "0: updates wait for the flight to drain")
     ap.add_argument("--served-plain", type=int, default=16,
                     help="served workload: queries of the trace timed alone on the plain engine")
     ap.add_argument("--plain-sample", type=int, default=32,
@@ -773,7 +777,7 @@ def served_arm(a, R):
     torch.cuda.set_device(dev)
     t0 = time.time()
     e = sgs.Engine(device=R.local, weight_mode=sgs.W_EXPLICIT, hbm_budget_gb=a.served_budget_gb,
-                   group_size=a.served_group_size)
+                   group_size=a.served_group_size, serve_restarts=a.serve_restarts)
     e.load_rmat(a.served_scale, a.edge_factor, a.seed, 0.57, 0.19, 0.19, wseed=a.seed)
     st0 = e.engine_stats()
     nv = int(st0["nv"])
@@ -853,6 +857,9 @@ def served_arm(a, R):
                     "sssp": pct("query", sgs.SSSP), "pr": pct("query", sgs.PR)},
         "lanes_in_flight_at_admission": {"mean": round(float(np.mean(qb)), 2) if qb else 0,
                                          "max": int(max(qb)) if qb else 0},
+        "restarts": {"allowed_per_query": a.serve_restarts,
+                     "queries_restarted": int(sum(1 for c in res if c["restarts"])),
+                     "total": int(sum(c["restarts"] for c in res))},
         "failed": int(len(res) - sum(ok)),
         "busy_s": round(busy, 3), "wall_s": round(wall, 3), "utilisation": round(busy / wall, 3),
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d / max(len(reqs), 1)),
@@ -1333,7 +1340,7 @@ def bfs_arm(a, R):
 def _condense(out):
     """The figures of a workload's line kept in the headline's sub-record."""
     keep = ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "roofline", "clocks", "gpu_launches",
-            "latency", "plain", "utilisation", "lanes_in_flight_at_admission", "static", "sweep",
+            "latency", "plain", "utilisation", "lanes_in_flight_at_admission", "restarts", "static", "sweep",
             "selfcheck_incremental_eq_static", "static_start", "failed", "grad_check")
     rec = {k: out[k] for k in keep if k in out}
     cfg = out.get("config") or {}

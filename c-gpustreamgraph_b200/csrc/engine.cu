@@ -83,6 +83,16 @@ struct DBuf {
   ~DBuf() { release(); }
 };
 
+// Capacity for a batch-sized buffer of n items: the next power of two (at
+// least 4096), so buffers that follow the batch size grow a few times at
+// most instead of at every larger batch (each growth frees and allocates).
+static inline size_t batch_cap(uint64_t n) {
+  if (n == 0) return 0;
+  size_t c = 4096;
+  while (c < n) c <<= 1;
+  return c;
+}
+
 template <class T>
 struct HBuf {  // pinned, mapped host memory
   T *p = nullptr;
@@ -252,6 +262,7 @@ struct sgs_engine {
   Group *fg = nullptr;
   uint32_t fr = 0;                   // next round; its input is buffer fr % 3 / cnt[fr]
   uint64_t frun = 0;                 // lanes with work in flight
+  uint64_t fsusp = 0;                // lanes suspended while an update applies
   uint32_t fadmit[WLANES] = {};      // round at which each lane joined
   DBuf<unsigned long long> flc;      // per-lane entry counts of the next frontier
   int next_qid = 1;
@@ -388,7 +399,7 @@ struct sgs_engine {
   // host-tier logic: hotness, cache lookups, link accounting)
   bool host_tier() const { return split < nv; }
 
-  void cub_ensure(size_t bytes) { cub_tmp.ensure(bytes); }
+  void cub_ensure(size_t bytes) { cub_tmp.ensure(batch_cap(bytes)); }
 
   void sync() { CK(cudaStreamSynchronize(s)); }
 
@@ -628,8 +639,8 @@ struct sgs_engine {
     const int eb = sort_bits();
     size_t tb = 0;
     if (nd) {
-      t_dkeys.ensure(nd);
-      t_tmp.ensure(std::max<uint64_t>(nd, nkept));
+      t_dkeys.ensure(batch_cap(nd));
+      t_tmp.ensure(batch_cap(std::max<uint64_t>(nd, nkept)));
       { ++n_launch; k_transpose_keys<<<grid_elem(nd), 256, 0, s>>>(b_dkeys_s.p, (uint32_t)nd, nullptr, t_tmp.p); }
       CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, t_tmp.p, t_dkeys.p, (int)nd, 0, eb, s));
       cub_ensure(tb);
@@ -645,12 +656,12 @@ struct sgs_engine {
       CK(cudaGetLastError());
     }
     if (!ni || !nkept) return;
-    t_ikeys.ensure(nkept);
-    t_tmp.ensure(nkept);
+    t_ikeys.ensure(batch_cap(nkept));
+    t_tmp.ensure(batch_cap(nkept));
     { ++n_launch; k_transpose_keys<<<grid_elem(nkept), 256, 0, s>>>(b_ikept.p, nkept, nullptr, t_tmp.p); }
     tb = 0;
     if (in_w()) {  // the kept inserts' weights travel with their transposed keys
-      t_iw.ensure(nkept);
+      t_iw.ensure(batch_cap(nkept));
       CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, t_tmp.p, t_ikeys.p, b_iw_kept.p, t_iw.p, (int)nkept, 0, eb,
                                          s));
       cub_ensure(tb);
@@ -677,10 +688,10 @@ struct sgs_engine {
       in_build(fview(0, special(0)), fview(1, special(1)));
       return;
     }
-    rl_vtx.ensure(nkept + 1);
-    rl_len.ensure(nkept + 1);
-    rl_from.ensure(nkept + 1);
-    rl_to.ensure(nkept + 1);
+    rl_vtx.ensure(batch_cap(nkept + 1));
+    rl_len.ensure(batch_cap(nkept + 1));
+    rl_from.ensure(batch_cap(nkept + 1));
+    rl_to.ensure(batch_cap(nkept + 1));
     c.rl_vtx = rl_vtx.p;
     c.rl_from = rl_from.p;
     c.rl_to = rl_to.p;
@@ -714,7 +725,7 @@ struct sgs_engine {
     groups.clear();
     apps.clear();  // user algorithms belong to the old graph
     fg = nullptr;
-    frun = 0;
+    frun = fsusp = 0;
     loaded = false;
     in_release();
     in_failed = false;
@@ -1630,7 +1641,7 @@ struct sgs_engine {
                 for (size_t j = groups.size(); j-- > 0;) {
                   bool pend = false;
                   for (auto &t : touched) pend |= t.first == groups[j].get();
-                  if (groups[j]->used == 0 && !pend && !(groups[j].get() == fg && frun)) {
+                  if (groups[j]->used == 0 && !pend && !(groups[j].get() == fg && (frun || fsusp))) {
                     if (groups[j].get() == fg) fg = nullptr;
                     groups.erase(groups.begin() + j);
                     freed = true;
@@ -1706,7 +1717,6 @@ struct sgs_engine {
       reset_counters(0);
       fr = 0;
     }
-    GraphView g = view();
     uint64_t fresh = 0, cc = 0;
     std::vector<Query *> qs;
     for (uint32_t i = 0; i < n; ++i) {
@@ -1728,6 +1738,15 @@ struct sgs_engine {
       queries.push_back(std::move(q));
       CK(cudaMemsetAsync(b_lane.p + l, 0, sizeof(unsigned long long), s));
     }
+    seed_flight_lanes(G, qs, fresh, cc);
+    frun |= fresh;
+  }
+
+  // Lane state of the flight's queries `qs` (lanes `fresh`, the CC ones in
+  // `cc`) initialised, and their sources (CC: every vertex) seeded into
+  // frontier fr.
+  void seed_flight_lanes(Group &G, const std::vector<Query *> &qs, uint64_t fresh, uint64_t cc) {
+    GraphView g = view();
     const uint32_t b = fr % 3;
     if (G.wide()) {
       { ++n_launch; k_wide_init_lanes<<<grid_elem((uint64_t)nv * 32), 256, 0, s>>>(G.st.p, G.val.p, nv, fresh, G.cc); }
@@ -1761,7 +1780,49 @@ struct sgs_engine {
           { ++n_launch; k_group_seed_one<<<1, 32, 0, s>>>(g, q->source, 1u << q->lane, gm[b].p, fview(fr, cnt.p + fr)); }
     }
     CK(cudaGetLastError());
-    frun |= fresh;
+  }
+
+  // An update preempts the flight (served loop): the lanes in flight stop at
+  // this round boundary, their live frontiers (fr - 1 and fr) lose their
+  // masks, and the lanes leave the group's used set, so the snapshot neither
+  // invalidates nor repairs their partial state.  flight_resume restarts
+  // them on the updated graph.
+  void flight_suspend() {
+    if (!frun || !fg) return;
+    Group &G = *fg;
+    if (fr >= 1) clear_masks(G.wide(), fr - 1);
+    clear_masks(G.wide(), fr);
+    CK(cudaGetLastError());
+    G.used &= ~frun;
+    fsusp = frun;
+    frun = 0;
+  }
+
+  // Restarts the suspended lanes from their sources on the current graph as
+  // a new flight (round 0, counters and per-lane edge counts cleared): their
+  // results are those of the snapshot they restart on.
+  void flight_resume() {
+    if (!fsusp || !fg) {
+      fsusp = 0;
+      return;
+    }
+    Group &G = *fg;
+    reset_counters(0);
+    fr = 0;
+    std::vector<Query *> qs;
+    uint64_t cc = 0;
+    for (auto &q : queries) {
+      if (q->grp != &G || !(fsusp >> q->lane & 1ull)) continue;
+      qs.push_back(q.get());
+      if (q->algo == SGS_CC) cc |= 1ull << q->lane;
+      fadmit[q->lane] = 0;
+      CK(cudaMemsetAsync(b_lane.p + q->lane, 0, sizeof(unsigned long long), s));
+    }
+    G.used |= fsusp;
+    const uint64_t lanes = fsusp;
+    fsusp = 0;
+    seed_flight_lanes(G, qs, lanes, cc);
+    frun = lanes;
   }
 
   // Runs up to `rounds` relaxation rounds of the flight and returns the
@@ -1878,7 +1939,7 @@ struct sgs_engine {
     for (size_t j = groups.size(); j-- > 0;)
       if (groups[j]->used == 0) {
         if (groups[j].get() == fg) {
-          if (frun) continue;
+          if (frun || fsusp) continue;
           fg = nullptr;
         }
         groups.erase(groups.begin() + j);
@@ -1971,8 +2032,41 @@ struct sgs_engine {
   }
   Staged *staged_in = nullptr;  // the staged batch apply_batch is reading
 
+  // Batch-sized buffers (and the sort's temporary storage) for batches of up
+  // to ni inserts and nd deletes, at the capacities apply_batch grows them
+  // to, so that a later batch of at most that size allocates nothing (a
+  // growth frees and allocates, and a free waits for the whole device).
+  void reserve_batch(uint64_t ni, uint64_t nd) {
+    const size_t ci = batch_cap(ni), cd = batch_cap(nd), cm = batch_cap(std::max(ni, nd));
+    for (DBuf<uint32_t> *b : {&b_isrc, &b_idst, &b_iw, &b_iw_s, &b_iw_kept, &t_iw}) b->ensure(ci);
+    for (DBuf<uint32_t> *b : {&b_dsrc, &b_ddst}) b->ensure(cd);
+    for (DBuf<uint64_t> *b : {&b_ikeys, &b_ikeys_s, &b_ikept, &t_ikeys}) b->ensure(ci);
+    for (DBuf<uint64_t> *b : {&b_dkeys, &b_dkeys_s, &t_dkeys}) b->ensure(cd);
+    t_tmp.ensure(cm);
+    b_flag.ensure(ci);
+    const size_t cr = batch_cap(ni + 1);
+    rl_vtx.ensure(cr);
+    rl_len.ensure(cr);
+    rl_from.ensure(cr);
+    rl_to.ensure(cr);
+    // the sorts and the selection of apply_batch and of the in-edge store's
+    // update, at the largest sizes
+    const int eb = sort_bits();
+    size_t tb = 0, t2 = 0, t3 = 0, t4 = 0;
+    if (nd || ni)
+      CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, b_dkeys.p, b_dkeys_s.p, (int)std::max(ni, nd), 0, eb, s));
+    if (ni) {
+      CK(cub::DeviceRadixSort::SortPairs(nullptr, t2, b_ikeys.p, b_ikeys_s.p, b_iw.p, b_iw_s.p, (int)ni, 0,
+                                         eb, s));
+      CK(cub::DeviceSelect::Flagged(nullptr, t3, b_ikeys_s.p, b_flag.p, b_ikept.p, b_nkept.p, (int)ni, s));
+      CK(cub::DeviceRadixSort::SortPairs(nullptr, t4, t_tmp.p, t_ikeys.p, b_iw_kept.p, t_iw.p, (int)ni, 0,
+                                         eb, s));
+    }
+    cub_ensure(std::max(std::max(tb, t2), std::max(t3, t4)));
+  }
+
   void upload(DBuf<uint32_t> &dst, const uint32_t *src, uint64_t n, int mem) {
-    dst.ensure(n);
+    dst.ensure(batch_cap(n));
     if (n)
       CK(cudaMemcpyAsync(dst.p, src, n * sizeof(uint32_t),
                          mem == SGS_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
@@ -2080,9 +2174,10 @@ struct sgs_engine {
     upload(b_dsrc, ds, nd, mem);
     upload(b_ddst, dd, nd, mem);
     if (staged_in) CK(cudaEventRecord(staged_in->consumed, s));  // its slot may be refilled
-    b_ikeys.ensure(ni); b_ikeys_s.ensure(ni); b_ikept.ensure(ni);
-    b_iw_s.ensure(ni); b_iw_kept.ensure(ni); b_flag.ensure(ni);
-    b_dkeys.ensure(nd); b_dkeys_s.ensure(nd);
+    const size_t ci = batch_cap(ni), cd = batch_cap(nd);
+    b_ikeys.ensure(ci); b_ikeys_s.ensure(ci); b_ikept.ensure(ci);
+    b_iw_s.ensure(ci); b_iw_kept.ensure(ci); b_flag.ensure(ci);
+    b_dkeys.ensure(cd); b_dkeys_s.ensure(cd);
     CK(cudaMemsetAsync(b_err.p, 0, sizeof(unsigned int), s));
     CK(cudaMemsetAsync(b_stat.p, 0, sizeof(unsigned long long) * 8, s));
     if (ni)
@@ -2428,10 +2523,10 @@ struct sgs_engine {
         c.arena_cap[0] = arena_cap[0];
         c.arena_cap[1] = arena_cap[1];
       }
-      rl_vtx.ensure(nkept + 1);
-      rl_len.ensure(nkept + 1);
-      rl_from.ensure(nkept + 1);
-      rl_to.ensure(nkept + 1);
+      rl_vtx.ensure(batch_cap(nkept + 1));
+      rl_len.ensure(batch_cap(nkept + 1));
+      rl_from.ensure(batch_cap(nkept + 1));
+      rl_to.ensure(batch_cap(nkept + 1));
       c.rl_vtx = rl_vtx.p;
       c.rl_from = rl_from.p;
       c.rl_to = rl_to.p;
@@ -2697,6 +2792,7 @@ SGS_API void sgs_config_default(sgs_config *c) {
   c->host_policy = 0;  // zero-copy reads of the host tier
   c->pr_warm = 1;
   c->repair = 0;  // the reference's re-push from every reached vertex
+  c->serve_restarts = 2;  // served loop: an update may restart a lane query twice
 }
 
 SGS_API int sgs_create(const sgs_config *cfg, sgs_engine **out) {
@@ -2852,6 +2948,26 @@ int flight_advance(sgs_engine *e, uint32_t rounds, std::vector<int> &done, uint6
     CK(cudaSetDevice(e->dev));
     e->flight_advance(rounds, done);
     *running = e->frun;
+  });
+}
+int flight_suspend(sgs_engine *e) {
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    e->flight_suspend();
+  });
+}
+int flight_resume(sgs_engine *e) {
+  return guarded([&] {
+    CK(cudaSetDevice(e->dev));
+    e->flight_resume();
+  });
+}
+uint32_t serve_restarts(sgs_engine *e) { return e->cfg.serve_restarts; }
+int reserve_batch(sgs_engine *e, uint64_t ni, uint64_t nd) {
+  return guarded([&] {
+    if (!e->loaded) fail(SGS_ERR_STATE, "no graph loaded");
+    CK(cudaSetDevice(e->dev));
+    e->reserve_batch(ni, nd);
   });
 }
 int pr_job_start(sgs_engine *e, int *qid) {

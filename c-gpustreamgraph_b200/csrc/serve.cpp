@@ -13,12 +13,19 @@
 //   * a query leaves as soon as no entry of the frontier carries its lane:
 //     its result is read back (summary, and optionally its value/parent
 //     vectors) and its lane freed for the next arrival;
-//   * an update batch is one snapshot, applied when no lane query is in
-//     flight, so every BFS/SSSP/CC query sees exactly the updates that
-//     arrived before it (its "version"); queries behind an update wait for it;
-//   * PageRank has no lanes (and no source): consecutive PR queries share one
+//   * an update batch is one snapshot.  When it reaches the head of the
+//     queue while lane queries are in flight, it preempts them: it is applied
+//     at the next round boundary and the queries in flight restart from
+//     their sources on the new snapshot (sgs_config.serve_restarts bounds
+//     how often one query may be restarted; once a query in flight has used
+//     its restarts, the update waits for the flight to drain).  A query's
+//     "version" is the snapshot of its last run: at least the updates that
+//     arrived before it, exactly those with serve_restarts = 0.  Queries
+//     behind an update wait for it;
+//   * PageRank has no lanes (and no source): PR queries share one
 //     computation, a job that starts as soon as they reach the head of the
-//     queue and runs a few sweeps per loop iteration between the flight's
+//     queue (later PR queries join it when they reach the head while it
+//     runs) and runs a few sweeps per loop iteration between the flight's
 //     steps, so lane queries behind it keep being admitted and served (the
 //     job has its own frontier buffers; a PageRank start continues from the
 //     vector of the previous one, see sgs_config.pr_warm).  Updates do not
@@ -44,12 +51,20 @@
 
 #include "../../include/sgs.h"
 
+#ifndef SGS_PR_SHARE_EVERY
+#define SGS_PR_SHARE_EVERY 4
+#endif
+
 namespace sgs {
 void set_last_error(const std::string &msg);
 // flight interface (engine.cu)
 int flight_free(sgs_engine *e, uint32_t *lanes);
 int flight_admit(sgs_engine *e, uint32_t n, const int *algos, const uint32_t *sources, int *ids);
 int flight_advance(sgs_engine *e, uint32_t rounds, std::vector<int> &done, uint64_t *running);
+int flight_suspend(sgs_engine *e);
+int flight_resume(sgs_engine *e);
+uint32_t serve_restarts(sgs_engine *e);
+int reserve_batch(sgs_engine *e, uint64_t ni, uint64_t nd);
 int pr_job_start(sgs_engine *e, int *qid);
 int pr_job_advance(sgs_engine *e, uint32_t rounds, int *done);
 }  // namespace sgs
@@ -62,12 +77,17 @@ double since(clk::time_point t0) {
   return std::chrono::duration<double>(clk::now() - t0).count();
 }
 
-constexpr uint32_t kRoundsPerStep = 4;  // rounds between two admission points
+// Rounds between two admission points (and points where an update may
+// preempt the flight)
+constexpr uint32_t kRoundsPerStep = 2;
 // PageRank sweeps per loop iteration: a long job yields to the lane queries
-// (and to the updates waiting for them to drain) while any are in flight,
-// and runs in longer steps when it has the GPU to itself
-constexpr uint32_t kPrRoundsPerStep = 8;
+// while any are in flight -- one sweep every kPrShareEvery iterations, so
+// the short queries keep most of the GPU -- and runs in longer steps when it
+// has the GPU to itself, short enough that an arriving update waits for a
+// few sweeps at most
+constexpr uint32_t kPrRoundsPerStep = 2;
 constexpr uint32_t kPrRoundsPerStepShared = 1;
+constexpr uint32_t kPrShareEvery = SGS_PR_SHARE_EVERY;
 
 // Result of a finished query into its completion record.
 void finish(sgs_engine *e, int qid, const sgs_request &r, sgs_completion &c) {
@@ -113,6 +133,16 @@ SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n, uint32_
                    [&](uint32_t a, uint32_t b) { return req[a].arrival_s < req[b].arrival_s; });
   for (uint32_t i = 0; i < n; ++i) std::memset(&out[i], 0, sizeof(sgs_completion));
 
+  // batch buffers for the trace's largest update, before the clock starts
+  // (if that fails, e.g. no graph is loaded, each update reports its error)
+  uint64_t max_ni = 0, max_nd = 0;
+  for (uint32_t i = 0; i < n; ++i)
+    if (req[i].kind == SGS_REQ_UPDATE) {
+      max_ni = std::max(max_ni, req[i].n_ins);
+      max_nd = std::max(max_nd, req[i].n_del);
+    }
+  if (max_ni || max_nd) (void)sgs::reserve_batch(e, max_ni, max_nd);
+
   const clk::time_point t0 = clk::now();
   std::deque<uint32_t> pending;
   std::map<int, uint32_t> inflight;  // query id -> request
@@ -120,19 +150,68 @@ SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n, uint32_
   uint64_t version = 0, running = 0;
   std::vector<int> algos, qids, fin;
   std::vector<uint32_t> sources, batch;
+  const uint32_t max_restarts = sgs::serve_restarts(e);
+  uint32_t pr_turn = 0;  // loop iterations with lane queries in flight
   int pr_qid = 0;                 // the PageRank job, if one runs
   std::vector<uint32_t> pr_batch;  // its requests
   double pr_start = 0;
+  // Applies the update at the head of the queue (one snapshot).
+  auto apply_head_update = [&]() {
+    const uint32_t head = pending.front();
+    const sgs_request &r = req[head];
+    pending.pop_front();
+    sgs_completion &c = out[head];
+    c.start_s = since(t0);
+    c.status = sgs_apply_batch(e, r.ins_src, r.ins_dst, r.ins_w, r.n_ins, r.del_src, r.del_dst,
+                               r.n_del, SGS_MEM_HOST);
+    if (c.status == SGS_OK) {
+      ++version;
+      sgs_engine_stats st;
+      if (sgs_get_engine_stats(e, &st) == SGS_OK) c.edges = st.last_batch_edges;
+    }
+    c.version = version;
+    c.batch = 1;
+    c.done_s = since(t0);
+    ++done;
+  };
+  // Fails every lane query in flight with `rc` (the flight could not go on).
+  auto fail_flight = [&](int rc) {
+    for (auto &kv : inflight) {
+      out[kv.second].status = rc;
+      out[kv.second].done_s = since(t0);
+      sgs_query_remove(e, kv.first);
+      ++done;
+    }
+    inflight.clear();
+  };
+  auto update_at_head = [&]() {
+    return !pending.empty() && req[pending.front()].kind == SGS_REQ_UPDATE;
+  };
+  auto pr_at_head = [&]() {
+    return !pending.empty() && req[pending.front()].kind == SGS_REQ_QUERY &&
+           req[pending.front()].algo == SGS_PR;
+  };
   while (done < n) {
     const double now = since(t0);
     while (next < n && (!realtime || req[order[next]].arrival_s <= now)) pending.push_back(order[next++]);
 
-    // 0. PageRank requests at the head start a job (one at a time)
-    if (!pr_qid && !pending.empty() && req[pending.front()].kind == SGS_REQ_QUERY &&
-        req[pending.front()].algo == SGS_PR) {
+    // 0. PageRank requests at the head join the job that runs -- its result
+    // reflects every update applied before it finishes, so at least those
+    // that arrived before them -- or start one
+    if (pr_qid && pr_at_head()) {
+      const double now_s = since(t0);
+      while (pr_at_head()) {
+        const uint32_t k = pending.front();
+        pending.pop_front();
+        pr_batch.push_back(k);
+        out[k].start_s = now_s;
+        out[k].status = SGS_OK;
+      }
+      for (uint32_t k : pr_batch) out[k].batch = (uint32_t)pr_batch.size();
+    }
+    if (!pr_qid && pr_at_head()) {
       pr_batch.clear();
-      while (!pending.empty() && req[pending.front()].kind == SGS_REQ_QUERY &&
-             req[pending.front()].algo == SGS_PR) {
+      while (pr_at_head()) {
         pr_batch.push_back(pending.front());
         pending.pop_front();
       }
@@ -205,9 +284,35 @@ SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n, uint32_
       continue;
     }
 
+    // 1b. an update at the head preempts the lane queries in flight, unless
+    // one of them has used up its restarts: the flight stops at this round
+    // boundary, the snapshot is applied, and the queries restart on it
+    if (!inflight.empty() && update_at_head() && max_restarts) {
+      bool can = true;
+      for (auto &kv : inflight) can = can && out[kv.second].restarts < max_restarts;
+      if (can) {
+        int rc = sgs::flight_suspend(e);
+        if (rc != SGS_OK) {
+          fail_flight(rc);
+          continue;
+        }
+        apply_head_update();
+        rc = sgs::flight_resume(e);
+        if (rc != SGS_OK) {
+          fail_flight(rc);
+          continue;
+        }
+        for (auto &kv : inflight) {
+          ++out[kv.second].restarts;
+          out[kv.second].version = version;
+        }
+        continue;
+      }
+    }
+
     bool worked = false;
     // 2. the PageRank job: a few sweeps
-    if (pr_qid) {
+    if (pr_qid && (inflight.empty() || ++pr_turn % kPrShareEvery == 0)) {
       worked = true;
       int fin_pr = 0;
       const int rc =
@@ -232,13 +337,7 @@ SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n, uint32_
       worked = true;
       const int rc = sgs::flight_advance(e, kRoundsPerStep, fin, &running);
       if (rc != SGS_OK) {  // fail every query in flight, keep serving
-        for (auto &kv : inflight) {
-          out[kv.second].status = rc;
-          out[kv.second].done_s = since(t0);
-          sgs_query_remove(e, kv.first);
-          ++done;
-        }
-        inflight.clear();
+        fail_flight(rc);
         continue;
       }
       for (int qid : fin) {
@@ -253,23 +352,8 @@ SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n, uint32_
     }
     // 4. an update at the head, once no lane query is in flight (a PageRank
     // job may be running: the snapshot amends it)
-    if (inflight.empty() && !pending.empty() && req[pending.front()].kind == SGS_REQ_UPDATE) {
-      const uint32_t head = pending.front();
-      const sgs_request &r = req[head];
-      pending.pop_front();
-      sgs_completion &c = out[head];
-      c.start_s = since(t0);
-      c.status = sgs_apply_batch(e, r.ins_src, r.ins_dst, r.ins_w, r.n_ins, r.del_src, r.del_dst,
-                                 r.n_del, SGS_MEM_HOST);
-      if (c.status == SGS_OK) {
-        ++version;
-        sgs_engine_stats st;
-        if (sgs_get_engine_stats(e, &st) == SGS_OK) c.edges = st.last_batch_edges;
-      }
-      c.version = version;
-      c.batch = 1;
-      c.done_s = since(t0);
-      ++done;
+    if (inflight.empty() && update_at_head()) {
+      apply_head_update();
       continue;
     }
     if (worked) continue;

@@ -86,6 +86,7 @@ class Config(C.Structure):
         ("host_policy", C.c_uint32),
         ("pr_warm", C.c_uint32),
         ("repair", C.c_uint32),
+        ("serve_restarts", C.c_uint32),
     ]
 
 
@@ -177,6 +178,7 @@ class Completion(C.Structure):
         ("status", C.c_int), ("batch", C.c_uint32), ("version", C.c_uint64),
         ("start_s", C.c_double), ("done_s", C.c_double),
         ("summary", C.c_uint64 * 4), ("edges", C.c_uint64),
+        ("restarts", C.c_uint32), ("reserved", C.c_uint32),
     ]
 
 
@@ -487,7 +489,7 @@ class Engine:
                         # closed loop (not realtime): every request counts as
                         # arrived at the start
                         "latency_s": c.done_s - (arr[i].arrival_s if realtime else 0.0),
-                        "summary": list(c.summary), "edges": c.edges})
+                        "summary": list(c.summary), "edges": c.edges, "restarts": c.restarts})
         return res
 
     def autotune(self):

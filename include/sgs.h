@@ -146,6 +146,17 @@ typedef struct sgs_config {
                              from every reached vertex: same results, far
                              fewer edges read and counted; 0 (default): the
                              reference's re-push                            */
+  uint32_t serve_restarts; /* served loop (sgs_serve): how many times an
+                             update may preempt one BFS/SSSP/CC query in
+                             flight.  A preempting update is applied at the
+                             next round boundary and the queries in flight
+                             restart from their sources on the new snapshot
+                             (their results and versions are then that
+                             snapshot's); once a query in flight has used
+                             its restarts, the next update waits for the
+                             flight to drain.  0: updates always wait, so
+                             every BFS/SSSP/CC query sees exactly the updates
+                             that arrived before it.  Default 2            */
 } sgs_config;
 
 typedef struct sgs_query_stats {
@@ -500,11 +511,16 @@ typedef struct sgs_completion {
   uint32_t batch;           /* queries: lanes in flight when it joined (PR:
                                requests sharing the computation); 1 for an
                                update                                        */
-  uint64_t version;         /* updates applied before the query ran; for an
-                               update, its own position in the sequence     */
+  uint64_t version;         /* query: the snapshot its result reflects (the
+                               updates applied before its last run; PR: at
+                               least those before it arrived); an update:
+                               its own position in the sequence             */
   double start_s, done_s;   /* seconds from the start of the call            */
   uint64_t summary[4];      /* query: as sgs_query_summary                   */
-  uint64_t edges;           /* edges traversed for this request              */
+  uint64_t edges;           /* edges traversed for this request (a restarted
+                               query: its last run only)                     */
+  uint32_t restarts;        /* query: times an update restarted it           */
+  uint32_t reserved;
 } sgs_completion;
 SGS_API int sgs_serve(sgs_engine *e, const sgs_request *req, uint32_t n,
                       uint32_t slots, int realtime, sgs_completion *out);
