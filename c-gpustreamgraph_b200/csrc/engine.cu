@@ -232,6 +232,7 @@ struct sgs_engine {
   DBuf<unsigned int> b_err;
   DBuf<unsigned long long> b_stat;  // [0] demand d, [1] demand h, [2] tombs, [3] inval
   DBuf<unsigned long long> b_reclaim;  // slots reclaimed by block compaction: [0] out-, [1] in-store
+  DBuf<uint32_t> big_list, big_n;      // large blocks to compact (k_compact_large) and their count
   uint64_t reclaimed_total = 0;
   DBuf<uint64_t> wbase;
   DBuf<uint32_t> rl_vtx, rl_len;
@@ -652,7 +653,7 @@ struct sgs_engine {
       TombOp op{gi, t_dkeys.p, b_gstart.p, (uint32_t)nd};
       { ++n_launch; seg_map<<<grid_map(), RELAX_THREADS, 0, s>>>(fview(0, special(4)), fview(1, special(5)), op,
                                                    nullptr); }
-      { ++n_launch; k_compact_blocks<<<(uint32_t)nsm * 8, 256, 0, s>>>(gi, fview(0, special(4)), b_reclaim.p + 1); }
+      compact_blocks(gi, nd, b_reclaim.p + 1);
       CK(cudaGetLastError());
     }
     if (!ni || !nkept) return;
@@ -2044,6 +2045,7 @@ struct sgs_engine {
     for (DBuf<uint64_t> *b : {&b_dkeys, &b_dkeys_s, &t_dkeys}) b->ensure(cd);
     t_tmp.ensure(cm);
     b_flag.ensure(ci);
+    big_list.ensure(batch_cap(nd + 1));
     const size_t cr = batch_cap(ni + 1);
     rl_vtx.ensure(cr);
     rl_len.ensure(cr);
@@ -2063,6 +2065,19 @@ struct sgs_engine {
                                          eb, s));
     }
     cub_ensure(std::max(std::max(tb, t2), std::max(t3, t4)));
+  }
+
+  // Tombstone reclamation of the blocks touched by this snapshot's nd
+  // deletes (the frontier in buffer 0 / special(4)): small blocks a warp
+  // each, the large ones listed by that pass a CTA each.
+  void compact_blocks(const GraphView &gv, uint64_t nd, unsigned long long *reclaimed) {
+    big_list.ensure(batch_cap(nd + 1));  // at most one entry per delete group
+    big_n.ensure(1);
+    CK(cudaMemsetAsync(big_n.p, 0, sizeof(uint32_t), s));
+    { ++n_launch; k_compact_blocks<<<(uint32_t)nsm * 8, 256, 0, s>>>(gv, fview(0, special(4)), reclaimed,
+                                                                     big_list.p, big_n.p); }
+    { ++n_launch; k_compact_large<<<(uint32_t)nsm * 2, COMPACT_THREADS, 0, s>>>(gv, big_list.p, big_n.p,
+                                                                               reclaimed); }
   }
 
   void upload(DBuf<uint32_t> &dst, const uint32_t *src, uint64_t n, int mem) {
@@ -2496,7 +2511,7 @@ struct sgs_engine {
                                                    tombs); }
       // the touched blocks that now hold a sixteenth or more of dead slots are
       // compacted in place before the inserts append to them
-      { ++n_launch; k_compact_blocks<<<(uint32_t)nsm * 8, 256, 0, s>>>(g, fview(0, special(4)), b_reclaim.p); }
+      compact_blocks(g, nd, b_reclaim.p);
       CK(cudaGetLastError());
     }
     uint32_t nkept = 0;

@@ -569,8 +569,14 @@ __global__ void k_reloc_frontier(const unsigned long long *rl_count, const uint3
 // inserts append right after them.  Each compaction costs at most 17 times
 // the slots it reclaims, and no block walked by a relaxation keeps more than
 // a sixteenth of dead slots.  Input: the frontier of the touched blocks (one
-// entry per source); reclaimed slots are added to *reclaimed.
-__global__ void k_compact_blocks(GraphView g, FrontierView f, unsigned long long *reclaimed) {
+// entry per source); reclaimed slots are added to *reclaimed.  A block of
+// COMPACT_LARGE slots or more (the hubs, which lose edges in every snapshot
+// and cross the threshold together) is not walked by a warp, whose steps
+// each wait for one load: its vertex goes to `big` (count in big_n) for
+// k_compact_large, a CTA per block.
+constexpr uint32_t COMPACT_LARGE = 1024;
+__global__ void k_compact_blocks(GraphView g, FrontierView f, unsigned long long *reclaimed,
+                                 uint32_t *big, uint32_t *big_n) {
   const uint32_t n = (uint32_t)(__ldcg((const unsigned long long *)f.counter) >> CNT_SHIFT);
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -581,6 +587,10 @@ __global__ void k_compact_blocks(GraphView g, FrontierView f, unsigned long long
     const uint32_t sl = g.slots[v], lv = g.live[v];
     const uint32_t dead = sl - lv;
     if (dead == 0 || (uint64_t)dead * 16 < lv) continue;  // warp-uniform
+    if (sl >= COMPACT_LARGE) {
+      if (lane == 0) big[atomicAdd(big_n, 1u)] = v;
+      continue;
+    }
     const uint64_t o = g.off[v];
     const uint32_t *a = adj_wptr(g, o);
     const uint32_t *wt = ew ? wgt_wptr(g, o) : nullptr;
@@ -604,6 +614,89 @@ __global__ void k_compact_blocks(GraphView g, FrontierView f, unsigned long long
     }
   }
   if (lane == 0 && got) atomicAdd(reclaimed, got);
+}
+
+// In-place compaction of the large blocks listed by k_compact_blocks, one
+// CTA per block, in tiles of 4 * COMPACT_THREADS slots: every thread loads a
+// 16-B quad of ids (and weights), the CTA scans the live counts and writes
+// the live slots forward.  A tile's writes land at or below the positions it
+// read, all of which were read before the first barrier of the tile, and
+// below the next tile's first slot, so the next tile is loaded before the
+// current one is written (software pipeline).  Blocks start on a 4-slot
+// boundary and hold a multiple of 4 slots of capacity, so a quad read past
+// the used slots stays inside the block.
+constexpr int COMPACT_THREADS = 512;
+__global__ void __launch_bounds__(COMPACT_THREADS)
+    k_compact_large(GraphView g, const uint32_t *big, const uint32_t *big_n, unsigned long long *reclaimed) {
+  constexpr int NW = COMPACT_THREADS / 32;
+  constexpr uint32_t TILE = 4u * COMPACT_THREADS;
+  __shared__ uint32_t s_warp[NW];
+  __shared__ uint32_t s_tot;
+  const uint32_t n = __ldcg(big_n);
+  const bool ew = g.wmode == W_EXPLICIT;
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const uint4 none = make_uint4(SGS_TOMB, SGS_TOMB, SGS_TOMB, SGS_TOMB);
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const uint32_t v = __ldcg(&big[i]);
+    const uint32_t sl = g.slots[v];
+    const uint64_t o = g.off[v];
+    const uint32_t *a = adj_wptr(g, o);
+    const uint32_t *wt = ew ? wgt_wptr(g, o) : nullptr;
+    auto load = [&](uint32_t j, uint4 &ids, uint4 &ws) {
+      const uint32_t k0 = j + 4 * threadIdx.x;
+      ids = none;
+      ws = make_uint4(0, 0, 0, 0);
+      if (k0 < sl) {
+        ids = __ldcg(reinterpret_cast<const uint4 *>(a + k0));
+        if (ew) ws = __ldcg(reinterpret_cast<const uint4 *>(wt + k0));
+      }
+    };
+    uint4 ids, ws;
+    load(0, ids, ws);
+    uint32_t out = 0;  // CTA-uniform
+    for (uint32_t j = 0; j < sl; j += TILE) {
+      uint4 nids = none, nws = make_uint4(0, 0, 0, 0);
+      if (j + TILE < sl) load(j + TILE, nids, nws);
+      const uint32_t k0 = j + 4 * threadIdx.x;
+      uint32_t keep = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (k0 + k < sl && quad_at(ids, k) != SGS_TOMB) keep |= 1u << k;
+      const uint32_t c = __popc(keep);
+      uint32_t x = c;  // inclusive scan over the warp
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+        if (lane >= (uint32_t)d) x += y;
+      }
+      if (lane == 31) s_warp[wid] = x;
+      __syncthreads();
+      if (wid == 0) {
+        const uint32_t t = lane < (uint32_t)NW ? s_warp[lane] : 0u;
+        uint32_t u = t;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, u, d);
+          if (lane >= (uint32_t)d) u += y;
+        }
+        if (lane < (uint32_t)NW) s_warp[lane] = u - t;
+        if (lane == NW - 1) s_tot = u;
+      }
+      __syncthreads();
+      uint32_t pos = out + s_warp[wid] + x - c;
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (keep >> k & 1u) store_slot(g, o, pos++, quad_at(ids, k), ew, quad_at(ws, k));
+      out += s_tot;
+      __syncthreads();  // s_warp / s_tot are rewritten by the next tile
+      ids = nids;
+      ws = nws;
+    }
+    if (threadIdx.x == 0) {
+      g.slots[v] = out;
+      if (sl > out) atomicAdd(reclaimed, (unsigned long long)(sl - out));
+    }
+  }
 }
 
 struct RelocCopyOp {
