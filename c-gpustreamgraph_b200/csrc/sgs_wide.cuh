@@ -23,9 +23,6 @@
 
 namespace sgs {
 
-#ifndef SGS_WIDE_RESTRICT_BLOCKS
-#define SGS_WIDE_RESTRICT_BLOCKS 3
-#endif
 constexpr int WLANES = 64;
 constexpr int WCHUNK = 256;  // entries staged per chunk by wide_map
 // a window with more (edge, lane) pairs than this many per edge on average
@@ -508,7 +505,7 @@ __device__ __forceinline__ void wide_map_body(const GraphView &g, FrontierView i
 }
 
 template <class Op, bool H>
-__global__ void __launch_bounds__(RELAX_THREADS, Op::kRestrict ? SGS_WIDE_RESTRICT_BLOCKS : 3)
+__global__ void __launch_bounds__(RELAX_THREADS, 3)
     wide_map(GraphView g, FrontierView in, FrontierView out, Op op,
              const unsigned long long *m_in, unsigned long long *m_out, const uint32_t *prev_vtx,
              const unsigned long long *prev_cnt, unsigned long long *prev_mask,
