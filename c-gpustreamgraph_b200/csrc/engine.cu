@@ -925,6 +925,12 @@ struct sgs_engine {
     if (!n) return;
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, a, b));
+    account_n(kind, n, T, inst, per_slot, per_inst, ms, host);
+  }
+  // The same with the entry and slot counts given apart (a launch that ran
+  // several rounds over one frontier) and its time in ms.
+  void account_n(int kind, uint64_t n, uint64_t T, unsigned long long inst, double per_slot,
+                 double per_inst, double ms, unsigned long long host = 0) {
     sgs_kernel_stats &k = kst[kind];
     const double bytes = per_slot * (double)T + per_inst * (double)inst + 20.0 * (double)n;
     k.launches += 1;
@@ -1314,6 +1320,48 @@ struct sgs_engine {
     last_l1 = 0;
     PrPushOp op{g, q.pv.p, q.r.p};
     const unsigned long long pr_inst = (pr_in & EDGE_MASK);
+    // all rounds in one cooperative launch (k_pr_rounds, one host read) when
+    // the sweep's units fit one wave of it -- a graph small enough that the
+    // launches and host reads of the round loop, not the sweeps, set the
+    // time; a larger one keeps the multi-wave launches, which balance better
+    const void *fn = (const void *)k_pr_rounds;
+    const uint64_t units = ((pr_in & EDGE_MASK) + UNIT - 1) / UNIT;
+    if (pull && (cfg.persistent & 8u) && limit && units <= (uint64_t)coop_grid(fn)) {
+      d_rounds.ensure(1);
+      GraphView ga = g, gb = gi;
+      FrontierView f = fin;
+      double *x = q.x.p, *rp = q.r.p, *pv = q.pv.p, *l1b = l1buf;
+      double alpha = cfg.pr_alpha, tol = cfg.pr_tol;
+      uint32_t r0a = r0, lim = limit;
+      unsigned long long *es = edge_stat;
+      uint32_t *ro = d_rounds.p;
+      void *args[] = {&ga, &f, &gb, &x, &rp, &pv, &alpha, &tol, &l1b, &r0a, &lim, &es, &ro};
+      // no more CTAs than units (idle CTAs only lengthen the grid barriers)
+      const int grid = (int)std::max<uint64_t>(std::min<uint64_t>(units, (uint64_t)coop_grid(fn)), nsm);
+      if (ktiming) {
+        ensure_kev(2);
+        CK(cudaEventRecord(kev[0], s));
+      }
+      ++n_launch;
+      CK(cudaLaunchCooperativeKernel(fn, grid, RELAX_THREADS, args, 0, s));
+      if (ktiming) CK(cudaEventRecord(kev[1], s));
+      uint32_t ran = 0;
+      hl.resize(limit);
+      CK(cudaMemcpyAsync(&ran, d_rounds.p, sizeof(ran), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(hl.data(), l1buf + r0, sizeof(double) * limit, cudaMemcpyDeviceToHost, s));
+      sync();
+      if (ran > limit) fail(SGS_ERR_CUDA, "PageRank round kernel returned a bad round count");
+      if (ran) {
+        last_l1 = hl[ran - 1];
+        conv = last_l1 < cfg.pr_tol;
+      }
+      if (ktiming && ran) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, kev[0], kev[1]));
+        account_n(SGS_K_PR_PULL, (pr_in >> CNT_SHIFT) * ran, pr_inst * ran, pr_inst * ran, 4.0, 16.0, ms);
+      }
+      return ran;
+    }
     while (r < limit) {
       const uint32_t nb = std::min(rb, limit - r);
       if (ktiming) ensure_kev(2 * nb);
@@ -1909,7 +1957,7 @@ struct sgs_engine {
     for (uint32_t pers = 0; pers < 2; ++pers)
       for (uint32_t c : cps) {
         map_cps = c;
-        cfg.persistent = (keep_pers & 6u) | pers;
+        cfg.persistent = (keep_pers & ~1u) | pers;
         double t = 1e300;
         for (int rep = 0; rep < 2; ++rep) {  // the first run also warms up
           int ids[3];
@@ -1925,7 +1973,7 @@ struct sgs_engine {
         }
       }
     map_cps = bc;
-    cfg.persistent = (keep_pers & 6u) | bp;
+    cfg.persistent = (keep_pers & ~1u) | bp;
     (void)keep_cps;
     (void)keep_pers;
     out->ctas_per_sm = bc;
@@ -2801,8 +2849,9 @@ SGS_API void sgs_config_default(sgs_config *c) {
   c->slack_div = 8;
   c->arena_headroom = 0.30;
   c->group_size = 4;
-  c->persistent = 6;  // invalidation phases persistent (many small rounds); relaxation: round 0
-                      // (the snapshot's sweep) on the large grid, the rest persistent
+  c->persistent = 14;  // invalidation phases persistent (many small rounds); relaxation: round 0
+                      // (the snapshot's sweep) on the large grid, the rest persistent; PageRank
+                      // pull rounds in one launch
   c->pull = 1;  // PageRank sweeps as pulls; bit 1 (direction-optimizing BFS) is opt-in
   c->host_policy = 0;  // zero-copy reads of the host tier
   c->pr_warm = 1;

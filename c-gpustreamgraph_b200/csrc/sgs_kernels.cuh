@@ -332,12 +332,15 @@ __global__ void k_pr_warm_res(const double *x, double *r, uint32_t nv, double ba
 // Absorb: value += residual, residual = 0, push value alpha*res/outdeg
 // (CombineValueBuffer, hybrid_pr.cu:66-85).  Accumulates the L1 norm of the
 // absorbed residual into *l1.
-__global__ void k_pr_absorb(GraphView g, double *x, double *r, double *pv,
-                            double alpha, double *l1) {
+// Coherent: r was written earlier in the same launch by other CTAs (the
+// persistent round kernel), so it is read through L2.
+template <bool Coherent>
+__device__ __forceinline__ void pr_absorb_body(const GraphView &g, double *x, double *r, double *pv,
+                                               double alpha, double *l1) {
   double acc = 0.0;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < g.nv; v += stride) {
-    const double rv = r[v];
+    const double rv = Coherent ? __ldcg(r + v) : r[v];
     double p = 0.0;
     if (rv != 0.0) {
       r[v] = 0.0;
@@ -352,6 +355,39 @@ __global__ void k_pr_absorb(GraphView g, double *x, double *r, double *pv,
   __shared__ typename BR::TempStorage tmp;
   const double tot = BR(tmp).Sum(acc);
   if (threadIdx.x == 0 && tot != 0.0) atomicAdd(l1, tot);
+}
+
+__global__ void k_pr_absorb(GraphView g, double *x, double *r, double *pv,
+                            double alpha, double *l1) {
+  pr_absorb_body<false>(g, x, r, pv, alpha, l1);
+}
+
+// PageRank rounds r0, r0+1, ... (at most `limit`) of the pull form in one
+// cooperative launch: absorb, grid barrier, pull sweep over the dense
+// in-store frontier `fin`, grid barrier, then every thread reads the round's
+// absorbed L1 (complete after the barrier) and all stop together once it is
+// below `tol` -- the rounds of the launch-per-kernel loop, in the same
+// order, without a launch pair per round and a host read per few rounds
+// (which dominate when the graph sits in L2).  *rounds_out = rounds run.
+// r and pv are written by other CTAs within the launch and read through L2.
+__global__ void __launch_bounds__(RELAX_THREADS)
+    k_pr_rounds(GraphView g, FrontierView fin, GraphView gi, double *x, double *r, double *pv,
+                double alpha, double tol, double *l1buf, uint32_t r0, uint32_t limit,
+                unsigned long long *edge_stat, uint32_t *rounds_out) {
+  cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+  uint32_t k = 0;
+  while (k < limit) {
+    pr_absorb_body<true>(g, x, r, pv, alpha, l1buf + r0 + k);
+    __threadfence();
+    grid.sync();
+    pull_pr_body<true>(fin, gi, pv, r, edge_stat);
+    __threadfence();
+    grid.sync();
+    const double l1v = __ldcg(l1buf + r0 + k);
+    ++k;
+    if (l1v < tol) break;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *rounds_out = k;
 }
 
 // ---------------------------------------------------------------------------

@@ -98,9 +98,12 @@ __global__ void k_transpose_keys(const uint64_t *in, uint32_t n, const uint32_t 
 // and each entry is written once per CTA: a plain store when the CTA holds
 // all of its positions, an atomicAdd (r is zero from the absorb step) when it
 // is split between CTAs.  edge_stat counts the live slots read.
-__global__ void __launch_bounds__(RELAX_THREADS)
-    k_pull_pr(FrontierView in, GraphView gi, const double *pv, double *r,
-              unsigned long long *edge_stat) {
+// Coherent: pv was written earlier in the same launch (the persistent round
+// kernel k_pr_rounds), so it is read through L2 instead of the non-coherent
+// read-only path.
+template <bool Coherent>
+__device__ __forceinline__ void pull_pr_body(const FrontierView &in, const GraphView &gi, const double *pv,
+                                             double *r, unsigned long long *edge_stat) {
   constexpr int GC = CHUNK;
   __shared__ uint64_t s_eb[GC + 1];
   __shared__ uint32_t s_len[GC];
@@ -162,7 +165,7 @@ __global__ void __launch_bounds__(RELAX_THREADS)
             for (int k = 0; k < 4; ++k) {
               const uint32_t u = quad_at(ids, k);
               if (j0 + k < len && u != SGS_TOMB) {
-                part += __ldg(pv + u);
+                part += Coherent ? __ldcg(pv + u) : __ldg(pv + u);
                 ++counted;
               }
             }
@@ -197,6 +200,12 @@ __global__ void __launch_bounds__(RELAX_THREADS)
     const unsigned long long c = warp_sum((unsigned long long)counted);
     if (lane == 0 && c) atomicAdd(edge_stat, c);
   }
+}
+
+__global__ void __launch_bounds__(RELAX_THREADS)
+    k_pull_pr(FrontierView in, GraphView gi, const double *pv, double *r,
+              unsigned long long *edge_stat) {
+  pull_pr_body<false>(in, gi, pv, r, edge_stat);
 }
 
 // One bottom-up BFS round of a narrow group (S lanes, all running lanes

@@ -118,7 +118,9 @@ typedef struct sgs_config {
                              narrow group's relaxation phase runs round 0 --
                              a snapshot's sweep -- as a plain launch on the
                              large grid and its later rounds as one
-                             cooperative launch.  Default 6               */
+                             cooperative launch.  Bit 3: PageRank's pull
+                             rounds (absorb + sweep + convergence test) as
+                             one cooperative launch.  Default 14          */
   uint32_t pull;          /* bit 0 (default on): PageRank's all-vertex
                              sweeps as pulls over an in-edge (CSC) store
                              kept in HBM (built by transposing the graph

@@ -181,7 +181,7 @@ def test_autotune_picks_a_setting_and_keeps_results(gs):
         e.load_csr(nv, row, col, w)
         t = e.autotune()
         # the tuner chooses bit 0 and keeps the other bits of the default (6)
-        assert t["tried"] == 8 and t["ctas_per_sm"] in (4, 8, 16, 32) and t["persistent"] in (6, 7)
+        assert t["tried"] == 8 and t["ctas_per_sm"] in (4, 8, 16, 32) and t["persistent"] in (14, 15)
         assert t["best_ms"] > 0
         qs = e.add_queries(_specs(nv, 3, 3, 1, 8))
         e.apply_batch(i_s, i_d, iw, d_s, d_d)

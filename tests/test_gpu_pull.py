@@ -45,6 +45,36 @@ def test_pagerank_pull_and_push_agree(pull):
         assert (ks["pr_push"]["launches"] > 0) == (not pull)
 
 
+def test_pagerank_round_kernel_matches_launches():
+    """PageRank's pull rounds as one cooperative launch (persistent bit 3,
+    the default) or as a kernel pair per round: both within 1e-6 of the FP64
+    power iteration after every snapshot, and they stop after the same
+    rounds (up to one round: the residual sum's order differs)."""
+    nv, row, col = O.rmat_csr(14, 16, 6)
+    w = O.weights(nv, row, col, 2, 0)
+    rounds = {}
+    for pers in (6, 14):
+        with sgs.Engine(persistent=pers) as e:
+            e.load_csr(nv, row, col, w)
+            e.kernel_timing(True)
+            m = Mirror(nv, row, col, w)
+            q = e.add_query(sgs.PR)
+            check_query(q, m, sgs.W_EXPLICIT)
+            rs = [q.stats()["rounds"]]
+            for k in range(2):
+                b = _batch(m, 70 + k, 3000, 3000, 2)
+                e.apply_batch(*b)
+                m.apply(*b)
+                check_query(q, m, sgs.W_EXPLICIT)
+                assert q.stats()["converged"] == 1
+                rs.append(q.stats()["rounds"])
+            # one launch per convergence with the round kernel, two per round without
+            launches = e.kernel_stats()["pr_pull"]["launches"]
+            assert (launches == 3) if pers == 14 else (launches >= sum(rs))
+            rounds[pers] = rs
+    assert all(abs(a - b) <= 1 for a, b in zip(rounds[6], rounds[14]))
+
+
 def test_in_store_rebuild_and_host_tier():
     """No slack, no headroom: the in-store's relocations overflow and it is
     rebuilt from the updated graph; the out-store keeps most blocks in host
