@@ -38,6 +38,12 @@ def test_config_defaults_without_gpu():
     c = sgs.default_config()
     assert c.segments == 512 and c.max_rounds == 1000 and c.group_size == 4
     assert abs(c.pr_alpha - 0.85) < 1e-12
+    # the documented engine defaults: invalidation and post-sweep rounds and
+    # PageRank's pull rounds as cooperative launches; PageRank sweeps as
+    # pulls; the reference's re-push repair; warm PageRank starts; an update
+    # may restart a served query twice
+    assert c.persistent == 14 and c.pull == 1 and c.repair == 0 and c.pr_warm == 1
+    assert c.serve_restarts == 2 and c.host_policy == 0 and c.weight_mode == sgs.W_EXPLICIT
     assert sgs.lib().sgs_version().startswith(b"sgs-b200")
 
 
