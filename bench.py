@@ -1249,8 +1249,9 @@ def _basic_line(a, R, metric, value, ms, cfg, extra):
 
 
 def pagerank_arm(a, R):
-    """Plain incremental PageRank (by default the scale-16 configuration: 10k + 10k updates per snapshot): R-MAT
-    scale --pr-scale, snapshots of --pr-updates updates (50/50); one step =
+    """Plain incremental PageRank (by default R-MAT scale 16 with 10k + 10k
+    updates per snapshot): R-MAT scale --pr-scale, snapshots of --pr-updates
+    updates (50/50); one step =
     one snapshot (cancel + compensate + sweeps to the L1 tolerance).  value =
     edges traversed (active vertices' out-degrees summed over rounds) per
     second of device time; the static start is reported beside it."""
